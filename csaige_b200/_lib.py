@@ -1,0 +1,170 @@
+"""ctypes binding of libsaige_gpu.so (include/saige_gpu.h).
+
+The shared library is the product: there is no Python or CPU fallback.  If it
+is missing, importing this module raises with the command that builds it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libsaige_gpu.so"
+
+OK, EINVAL, ENOMEM, ECUDA, NOT_CONVERGED, TIMEOUT, SINGULAR, EBED, ENOTSUP = range(9)
+STATUS_NAMES = {
+    0: "SAIGE_OK",
+    1: "SAIGE_EINVAL",
+    2: "SAIGE_ENOMEM",
+    3: "SAIGE_ECUDA",
+    4: "SAIGE_NOT_CONVERGED",
+    5: "SAIGE_TIMEOUT",
+    6: "SAIGE_SINGULAR",
+    7: "SAIGE_EBED",
+    8: "SAIGE_ENOTSUP",
+}
+
+PREC_FP32, PREC_MIXED = 0, 1
+TRAIT_BINARY, TRAIT_QUANTITATIVE, TRAIT_SURVIVAL = 0, 1, 2
+SOLVE_SINGLE, SOLVE_BLOCK = 0, 1
+WARM_ZERO, WARM_PREVIOUS, WARM_LEARNED = 0, 1, 2
+
+
+class SaigeError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class PcgOptions(C.Structure):
+    _fields_ = [("tol", C.c_double), ("max_iter", C.c_int32), ("precision", C.c_int32)]
+
+
+class AiRemlConfigC(C.Structure):
+    _fields_ = [
+        ("max_iter", C.c_int32),
+        ("tol", C.c_double),
+        ("pcg_tol", C.c_double),
+        ("pcg_max_iter", C.c_int32),
+        ("n_random_vectors", C.c_int32),
+        ("seed", C.c_uint64),
+        ("precision", C.c_int32),
+        ("solve", C.c_int32),
+        ("warm_start", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class AiRemlSummaryC(C.Structure):
+    _fields_ = [
+        ("tau", C.c_double * 2),
+        ("iterations", C.c_int32),
+        ("converged", C.c_int32),
+        ("log_likelihood", C.c_double),
+        ("n_kv", C.c_int64),
+        ("n_kv_launches", C.c_int64),
+        ("pcg_iters", C.c_int64),
+        ("seconds", C.c_double),
+    ]
+
+
+class CohortSpecC(C.Structure):
+    _fields_ = [
+        ("seed", C.c_uint64),
+        ("n", C.c_int64),
+        ("m", C.c_int64),
+        ("sib_frac", C.c_double),
+        ("cousin_frac", C.c_double),
+        ("missing_rate", C.c_double),
+        ("maf_lo", C.c_double),
+        ("maf_hi", C.c_double),
+        ("trait", C.c_int32),
+        ("n_covar", C.c_int32),
+        ("prevalence", C.c_double),
+        ("h2", C.c_double),
+        ("n_causal", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+P = C.POINTER
+_d, _i64, _i32, _u8, _u64, _sz, _vp = (
+    P(C.c_double),
+    P(C.c_int64),
+    P(C.c_int32),
+    P(C.c_uint8),
+    C.c_uint64,
+    C.c_size_t,
+    C.c_void_p,
+)
+
+# name -> (restype, argtypes), exactly the declarations of include/saige_gpu.h
+SIGNATURES = {
+    "saige_last_error": (C.c_char_p, []),
+    "saige_version": (C.c_int32, []),
+    "saige_device_count": (C.c_int32, []),
+    "saige_bed_marker_stats": (
+        C.c_int32,
+        [_u8, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _d, _d, _i64],
+    ),
+    "saige_select_grm_markers": (
+        C.c_int32,
+        [_d, _d, _i64, C.c_int64, C.c_int64, C.c_double, C.c_double, _u64, _i64, _i64, _i64, _i64],
+    ),
+    "saige_grm_create_from_bed": (
+        C.c_int32,
+        [_u8, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _i64, C.c_int64, _d, C.c_int32, P(_vp)],
+    ),
+    "saige_grm_create_from_bed_dev": (
+        C.c_int32,
+        [_vp, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _i64, C.c_int64, _d, C.c_int32, P(_vp)],
+    ),
+    "saige_grm_create_from_dosages": (
+        C.c_int32,
+        [_d, C.c_int64, C.c_int64, _d, C.c_int32, P(_vp)],
+    ),
+    "saige_grm_destroy": (C.c_int32, [_vp]),
+    "saige_grm_dims": (C.c_int32, [_vp, _i64, _i64]),
+    "saige_grm_matvec": (C.c_int32, [_vp, _d, _d, C.c_int64, C.c_int32, C.c_int32]),
+    "saige_grm_matvec_dev": (
+        C.c_int32,
+        [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, _vp],
+    ),
+    "saige_pcg_solve": (
+        C.c_int32,
+        [_vp, _d, _d, _d, _d, _d, C.c_int64, C.c_int32, P(PcgOptions), _i32, _d, _u8],
+    ),
+    "saige_solve_mixed_model_pcg": (
+        C.c_int32,
+        [_vp, _d, _d, _d, _d, C.c_int64, P(PcgOptions), _i32, _d, _u8],
+    ),
+    "saige_ai_reml_config_default": (None, [P(AiRemlConfigC)]),
+    "saige_fit_ai_reml": (
+        C.c_int32,
+        [_vp, _d, _d, C.c_int64, C.c_int32, C.c_int32, P(AiRemlConfigC), P(AiRemlSummaryC),
+         _d, _d, _d, _d, _d],
+    ),
+    "saige_gen_bed": (C.c_int32, [P(CohortSpecC), _vp, C.c_int32]),
+    "saige_gen_pheno": (C.c_int32, [P(CohortSpecC), _d, _d]),
+}
+
+
+def load() -> C.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(
+            f"{LIB_PATH} is missing: build the sm_100a library first "
+            "(python -c 'import __graft_entry__ as g; g.build()')"
+        )
+    lib = C.CDLL(str(LIB_PATH))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+LIB = load()
+
+
+def check(code: int) -> None:
+    if code != OK:
+        raise SaigeError(code, LIB.saige_last_error().decode(errors="replace"))

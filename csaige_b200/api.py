@@ -1,0 +1,400 @@
+"""Host-side mirror of the saige-rs fit-null API over the sm_100a library.
+
+Names, argument meaning and error behaviour follow the saige-rs types they
+stand in for (paths relative to the frhl/CSAIGE tree):
+
+  OnTheFlyGrm         saige-core/src/glmm/pcg.rs:91-180
+  PcgSolver/PcgResult saige-linalg/src/decomposition.rs:167-298
+  solve_mixed_model_pcg, SaigePcgConfig   saige-core/src/glmm/pcg.rs:12-78
+  AiRemlConfig, AiRemlResult, fit_ai_reml saige-core/src/glmm/ai_reml.rs:20-427
+  TraitType           saige-core/src/glmm/link.rs:7-12
+  bed_marker_stats    saige-geno/src/plink.rs:237-267 + traits.rs:42-54
+  select_grm_markers  saige-cli/src/commands/fit_null.rs:209-259
+
+Every call goes through the C ABI of libsaige_gpu.so; nothing is computed in
+Python.  Where the reference panics (assert_eq! on dimensions) this module
+raises SaigeError(SAIGE_EINVAL).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import LIB, SaigeError, check
+
+PREC_FP32 = _lib.PREC_FP32
+PREC_MIXED = _lib.PREC_MIXED
+SOLVE_SINGLE = _lib.SOLVE_SINGLE
+SOLVE_BLOCK = _lib.SOLVE_BLOCK
+WARM_ZERO = _lib.WARM_ZERO
+WARM_PREVIOUS = _lib.WARM_PREVIOUS
+WARM_LEARNED = _lib.WARM_LEARNED
+
+
+class TraitType(enum.IntEnum):
+    Binary = _lib.TRAIT_BINARY
+    Quantitative = _lib.TRAIT_QUANTITATIVE
+    Survival = _lib.TRAIT_SURVIVAL
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _i64ptr(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def _f64(a, n: Optional[int] = None) -> np.ndarray:
+    out = np.ascontiguousarray(np.asarray(a, dtype=np.float64))
+    if n is not None and out.size != n:
+        raise SaigeError(_lib.EINVAL, f"expected {n} values, got {out.size}")
+    return out
+
+
+def device_count() -> int:
+    return int(LIB.saige_device_count())
+
+
+def version() -> int:
+    return int(LIB.saige_version())
+
+
+# ---------------------------------------------------------------------------
+# genotype input
+# ---------------------------------------------------------------------------
+def _bed_array(bed) -> np.ndarray:
+    if isinstance(bed, (bytes, bytearray, memoryview)):
+        return np.frombuffer(bed, dtype=np.uint8)
+    return np.ascontiguousarray(np.asarray(bed, dtype=np.uint8))
+
+
+def bed_marker_stats(bed, n_fam: int, m_tot: int, sample_idx: Optional[Sequence[int]] = None):
+    """(af, mac, n_valid) per marker over the sample subset, integer-exact on the GPU."""
+    b = _bed_array(bed)
+    sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
+    n = n_fam if sidx is None else sidx.size
+    af = np.empty(m_tot)
+    mac = np.empty(m_tot)
+    nv = np.empty(m_tot, dtype=np.int64)
+    check(
+        LIB.saige_bed_marker_stats(
+            b.ctypes.data_as(C.POINTER(C.c_uint8)), b.size, n_fam, m_tot, _i64ptr(sidx), n,
+            _dptr(af), _dptr(mac), _i64ptr(nv)
+        )
+    )
+    return af, mac, nv
+
+
+def select_grm_markers(af, mac, n_valid, n: int, min_maf: float = 0.01,
+                       max_missing: float = 0.15, seed: int = 12345):
+    """(grm_idx, vr_idx): QC plus the variance-ratio marker split of fit-null."""
+    af = _f64(af)
+    mac = _f64(mac, af.size)
+    nv = np.ascontiguousarray(n_valid, dtype=np.int64)
+    m = af.size
+    g = np.empty(max(m, 1), dtype=np.int64)
+    v = np.empty(max(m, 1), dtype=np.int64)
+    mg = C.c_int64()
+    mv = C.c_int64()
+    check(
+        LIB.saige_select_grm_markers(
+            _dptr(af), _dptr(mac), _i64ptr(nv), m, n, min_maf, max_missing, seed, _i64ptr(g),
+            C.byref(mg), _i64ptr(v), C.byref(mv)
+        )
+    )
+    return g[: mg.value].copy(), v[: mv.value].copy()
+
+
+# ---------------------------------------------------------------------------
+# GRM operator
+# ---------------------------------------------------------------------------
+class OnTheFlyGrm:
+    """K v = Z (Z' v) / M over 2-bit genotypes resident in HBM."""
+
+    def __init__(self, handle: C.c_void_p, precision: int = PREC_FP32):
+        self._h = handle
+        n = C.c_int64()
+        m = C.c_int64()
+        check(LIB.saige_grm_dims(self._h, C.byref(n), C.byref(m)))
+        self.n_samples = n.value
+        self.n_markers = m.value
+        self.precision = precision
+
+    @classmethod
+    def new(cls, dosages, allele_freqs, device: int = -1, precision: int = PREC_FP32):
+        """OnTheFlyGrm::new(dosages, allele_freqs): m dosage vectors of n hard calls."""
+        d = np.asarray(dosages, dtype=np.float64)
+        if d.ndim != 2:
+            raise SaigeError(_lib.EINVAL, "dosages must be m x n")
+        m, n = d.shape
+        d = np.ascontiguousarray(d)
+        af = _f64(allele_freqs, m)
+        h = C.c_void_p()
+        check(LIB.saige_grm_create_from_dosages(_dptr(d), n, m, _dptr(af), device, C.byref(h)))
+        return cls(h, precision)
+
+    @classmethod
+    def from_bed(cls, bed, n_fam: int, m_tot: int, marker_idx, allele_freqs,
+                 sample_idx: Optional[Sequence[int]] = None, device: int = -1,
+                 precision: int = PREC_FP32):
+        b = _bed_array(bed)
+        midx = np.ascontiguousarray(marker_idx, dtype=np.int64)
+        af = _f64(allele_freqs, midx.size)
+        sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
+        n = n_fam if sidx is None else sidx.size
+        h = C.c_void_p()
+        check(
+            LIB.saige_grm_create_from_bed(
+                b.ctypes.data_as(C.POINTER(C.c_uint8)), b.size, n_fam, m_tot, _i64ptr(sidx), n,
+                _i64ptr(midx), midx.size, _dptr(af), device, C.byref(h)
+            )
+        )
+        return cls(h, precision)
+
+    @classmethod
+    def from_bed_dev(cls, bed_ptr: int, bed_len: int, n_fam: int, m_tot: int, marker_idx,
+                     allele_freqs, sample_idx=None, device: int = -1,
+                     precision: int = PREC_FP32):
+        midx = np.ascontiguousarray(marker_idx, dtype=np.int64)
+        af = _f64(allele_freqs, midx.size)
+        sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
+        n = n_fam if sidx is None else sidx.size
+        h = C.c_void_p()
+        check(
+            LIB.saige_grm_create_from_bed_dev(
+                C.c_void_p(bed_ptr), bed_len, n_fam, m_tot, _i64ptr(sidx), n, _i64ptr(midx),
+                midx.size, _dptr(af), device, C.byref(h)
+            )
+        )
+        return cls(h, precision)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            LIB.saige_grm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def mat_vec(self, v, precision: Optional[int] = None) -> np.ndarray:
+        """K v for one vector (n,) or a block (nrhs, n)."""
+        a = _f64(v)
+        one = a.ndim == 1
+        a = a.reshape(1, -1) if one else a
+        if a.shape[1] != self.n_samples:
+            raise SaigeError(_lib.EINVAL, f"v.len() = {a.shape[1]} != n_samples = {self.n_samples}")
+        out = np.empty_like(a)
+        prec = self.precision if precision is None else precision
+        check(LIB.saige_grm_matvec(self._h, _dptr(a), _dptr(out), self.n_samples, a.shape[0], prec))
+        return out[0] if one else out
+
+    def mat_vec_dev(self, v_ptr: int, out_ptr: int, nrhs: int = 1,
+                    precision: Optional[int] = None, stream: int = 0) -> None:
+        prec = self.precision if precision is None else precision
+        check(LIB.saige_grm_matvec_dev(self._h, C.c_void_p(v_ptr), C.c_void_p(out_ptr),
+                                       self.n_samples, nrhs, prec, C.c_void_p(stream or None)))
+
+    def __call__(self, v):
+        return self.mat_vec(v)
+
+
+# ---------------------------------------------------------------------------
+# PCG
+# ---------------------------------------------------------------------------
+@dataclass
+class PcgResult:
+    x: np.ndarray
+    iterations: int
+    residual: float
+    converged: bool
+
+
+class PcgSolver:
+    """PcgSolver { tol, max_iter } on the fit-null operator of a GRM handle."""
+
+    def __init__(self, tol: float = 1e-5, max_iter: int = 500):
+        self.tol = tol
+        self.max_iter = max_iter
+
+    def solve(self, grm: OnTheFlyGrm, w, tau, b, x0=None, precision: Optional[int] = None):
+        """Solve (tau0 W^-1 + tau1 K) x = b; b is (n,) or a block (nrhs, n).
+
+        A block returns one PcgResult per column."""
+        n = grm.n_samples
+        bb = _f64(b)
+        one = bb.ndim == 1
+        bb = bb.reshape(1, -1) if one else bb
+        q = bb.shape[0]
+        if bb.shape[1] != n:
+            raise SaigeError(_lib.EINVAL, "b has the wrong length")
+        wv = _f64(w, n)
+        t = _f64(tau, 2)
+        xx = np.empty_like(bb)
+        x0a = None if x0 is None else _f64(x0, q * n).reshape(q, n)
+        it = np.zeros(q, dtype=np.int32)
+        rs = np.zeros(q)
+        cv = np.zeros(q, dtype=np.uint8)
+        opt = _lib.PcgOptions(self.tol, self.max_iter,
+                              grm.precision if precision is None else precision)
+        check(LIB.saige_pcg_solve(grm._h, _dptr(wv), _dptr(t), _dptr(bb),
+                                  None if x0a is None else _dptr(x0a), _dptr(xx), n, q,
+                                  C.byref(opt), it.ctypes.data_as(C.POINTER(C.c_int32)),
+                                  _dptr(rs), cv.ctypes.data_as(C.POINTER(C.c_uint8))))
+        res = [PcgResult(xx[c].copy(), int(it[c]), float(rs[c]), bool(cv[c])) for c in range(q)]
+        return res[0] if one else res
+
+
+@dataclass
+class SaigePcgConfig:
+    tol: float = 1e-5
+    max_iter: int = 500
+
+
+def solve_mixed_model_pcg(tau, w, grm: OnTheFlyGrm, b, config: SaigePcgConfig = SaigePcgConfig(),
+                          precision: Optional[int] = None) -> PcgResult:
+    """(tau_e W + tau_g GRM) x = b, the score-test convention of pcg.rs:37-78."""
+    n = grm.n_samples
+    bb = _f64(b, n)
+    wv = _f64(w, n)
+    t = _f64(tau, 2)
+    x = np.empty(n)
+    it = C.c_int32()
+    rs = C.c_double()
+    cv = C.c_uint8()
+    opt = _lib.PcgOptions(config.tol, config.max_iter,
+                          grm.precision if precision is None else precision)
+    check(LIB.saige_solve_mixed_model_pcg(grm._h, _dptr(t), _dptr(wv), _dptr(bb), _dptr(x), n,
+                                          C.byref(opt), C.byref(it), C.byref(rs), C.byref(cv)))
+    return PcgResult(x, it.value, rs.value, bool(cv.value))
+
+
+# ---------------------------------------------------------------------------
+# AI-REML
+# ---------------------------------------------------------------------------
+@dataclass
+class AiRemlConfig:
+    max_iter: int = 30
+    tol: float = 0.02
+    pcg_tol: float = 1e-5
+    pcg_max_iter: int = 500
+    n_random_vectors: int = 30
+    use_sparse_grm: bool = False  # parsed by the reference, never read (ai_reml.rs:33)
+    seed: int = 12345
+    precision: int = PREC_FP32
+    solve: int = SOLVE_SINGLE
+    warm_start: int = WARM_ZERO
+
+
+@dataclass
+class AiRemlResult:
+    tau: np.ndarray
+    iterations: int
+    converged: bool
+    mu: np.ndarray
+    working_weights: np.ndarray
+    residuals: np.ndarray
+    eta: np.ndarray
+    alpha: np.ndarray
+    log_likelihood: float
+    n_kv: int = 0
+    n_kv_launches: int = 0
+    pcg_iters: int = 0
+    seconds: float = 0.0
+    tau_trace: np.ndarray = field(default_factory=lambda: np.zeros((0, 2)))
+
+
+def _design(x, n: int) -> tuple[np.ndarray, int]:
+    a = np.asarray(x, dtype=np.float64)
+    if a.ndim == 1:
+        a = a.reshape(n, -1, order="F")
+    if a.shape[0] != n:
+        raise SaigeError(_lib.EINVAL, f"x.nrows() = {a.shape[0]} != n = {n}")
+    return np.asfortranarray(a).ravel(order="F").copy(), a.shape[1]
+
+
+def fit_ai_reml(y, x, grm: OnTheFlyGrm, trait_type: TraitType,
+                config: AiRemlConfig = AiRemlConfig()) -> AiRemlResult:
+    """fit_ai_reml(y, x, |v| grm.mat_vec(v), trait_type, config).  x is n x p."""
+    yy = _f64(y)
+    n = yy.size
+    if n != grm.n_samples:
+        raise SaigeError(_lib.EINVAL, "y.len() != n_samples")
+    xc, p = _design(x, n)
+    cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
+                             config.n_random_vectors, config.seed, config.precision, config.solve,
+                             config.warm_start, 0)
+    out = _lib.AiRemlSummaryC()
+    alpha = np.zeros(p)
+    mu = np.zeros(n)
+    eta = np.zeros(n)
+    w = np.zeros(n)
+    trace = np.full(2 * max(config.max_iter, 1), np.nan)
+    check(LIB.saige_fit_ai_reml(grm._h, _dptr(yy), _dptr(xc), n, p, int(trait_type),
+                                C.byref(cfg), C.byref(out), _dptr(alpha), _dptr(mu), _dptr(eta),
+                                _dptr(w), _dptr(trace)))
+    it = out.iterations
+    return AiRemlResult(
+        tau=np.array([out.tau[0], out.tau[1]]), iterations=it, converged=bool(out.converged),
+        mu=mu, working_weights=w, residuals=yy - mu, eta=eta, alpha=alpha,
+        log_likelihood=out.log_likelihood, n_kv=out.n_kv, n_kv_launches=out.n_kv_launches,
+        pcg_iters=out.pcg_iters, seconds=out.seconds,
+        tau_trace=trace[: 2 * it].reshape(-1, 2))
+
+
+# ---------------------------------------------------------------------------
+# synthetic cohorts
+# ---------------------------------------------------------------------------
+@dataclass
+class CohortSpec:
+    seed: int = 12345
+    n: int = 2000
+    m: int = 5000
+    sib_frac: float = 0.10
+    cousin_frac: float = 0.0
+    missing_rate: float = 0.01
+    maf_lo: float = 0.01
+    maf_hi: float = 0.5
+    trait: int = _lib.TRAIT_BINARY
+    n_covar: int = 2
+    prevalence: float = 0.10
+    h2: float = 0.2
+    n_causal: int = 500
+
+    def c(self) -> _lib.CohortSpecC:
+        return _lib.CohortSpecC(self.seed, self.n, self.m, self.sib_frac, self.cousin_frac,
+                                self.missing_rate, self.maf_lo, self.maf_hi, self.trait,
+                                self.n_covar, self.prevalence, self.h2, self.n_causal, 0)
+
+    @property
+    def bed_len(self) -> int:
+        return 3 + self.m * ((self.n + 3) // 4)
+
+
+def gen_bed(spec: CohortSpec) -> np.ndarray:
+    out = np.empty(spec.bed_len, dtype=np.uint8)
+    s = spec.c()
+    check(LIB.saige_gen_bed(C.byref(s), out.ctypes.data_as(C.c_void_p), 0))
+    return out
+
+
+def gen_bed_dev(spec: CohortSpec, dev_ptr: int) -> None:
+    s = spec.c()
+    check(LIB.saige_gen_bed(C.byref(s), C.c_void_p(dev_ptr), 1))
+
+
+def gen_pheno(spec: CohortSpec) -> tuple[np.ndarray, np.ndarray]:
+    """(y, x) with x n x (1 + n_covar), intercept first."""
+    y = np.empty(spec.n)
+    x = np.empty(spec.n * (1 + spec.n_covar))
+    s = spec.c()
+    check(LIB.saige_gen_pheno(C.byref(s), _dptr(y), _dptr(x)))
+    return y, x.reshape(1 + spec.n_covar, spec.n).T.copy()

@@ -1,0 +1,440 @@
+// AI-REML fit of the null GLMM on the GPU: fit_ai_reml and fit_glm_irls of
+// saige-core/src/glmm/ai_reml.rs:86-482.  N-vectors stay in HBM; the p x p
+// Cholesky solves (p <= 64) and the tau update run on the host in FP64.
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "engine.cuh"
+#include "rng.hpp"
+
+namespace saige {
+
+namespace {
+
+// decomposition.rs:35-61 (row-major p x p); false when not positive definite.
+bool cholesky(const std::vector<double>& a, int p, std::vector<double>& l) {
+  l.assign((size_t)p * p, 0.0);
+  for (int j = 0; j < p; ++j) {
+    double sum = 0.0;
+    for (int k = 0; k < j; ++k) sum += l[j * p + k] * l[j * p + k];
+    const double diag = a[j * p + j] - sum;
+    if (diag <= 0.0) return false;
+    l[j * p + j] = sqrt(diag);
+    for (int i = j + 1; i < p; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < j; ++k) s += l[i * p + k] * l[j * p + k];
+      l[i * p + j] = (a[i * p + j] - s) / l[j * p + j];
+    }
+  }
+  return true;
+}
+
+// decomposition.rs:64-89
+void chol_solve(const std::vector<double>& l, int p, const double* b, double* x) {
+  std::vector<double> y((size_t)p);
+  for (int i = 0; i < p; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < i; ++j) s += l[i * p + j] * y[j];
+    y[i] = (b[i] - s) / l[i * p + i];
+  }
+  for (int i = p - 1; i >= 0; --i) {
+    double s = 0.0;
+    for (int j = i + 1; j < p; ++j) s += l[j * p + i] * x[j];
+    x[i] = (y[i] - s) / l[i * p + i];
+  }
+}
+
+struct Fit {
+  saige_grm* h;
+  cudaStream_t st;
+  int64_t n, ld;
+  int p, nrv, q;
+  const saige_ai_reml_config* cfg;
+  DevBuf mem;
+  // device vectors
+  double *y, *x, *eta, *mu, *w, *wmax, *d, *ytil;
+  double *rhs, *sol;      // n_pad x q each: [ytil | X | U], [Sinv ytil | Sinv X | Sinv U]
+  double *ku, *pu, *tmpq; // n_pad x nrv
+  double *py, *kpy, *pk, *invw_py, *pw, *pk_raw, *pw_raw;
+  double *dsmall;         // small device scratch (coefficients, dot results)
+  double *partial;
+  int64_t pcg_iters = 0;
+  bool have_prev = false, have_prev_pk = false, have_prev_pw = false;
+};
+
+Status dots(Fit& f, const double* a, int pa, const double* b, int qb, const double* wv,
+            std::vector<double>& out) {
+  double* dout = f.dsmall;
+  SG_CUDA(cross_dots(a, pa, b, qb, wv, f.n, f.ld, f.partial, dout, f.st));
+  out.resize((size_t)pa * qb);
+  SG_CUDA(cudaMemcpyAsync(out.data(), dout, out.size() * 8, cudaMemcpyDeviceToHost, f.st));
+  SG_CUDA(cudaStreamSynchronize(f.st));
+  return Status();
+}
+
+Status coldots(Fit& f, const double* a, const double* b, int q, std::vector<double>& out) {
+  double* dout = f.dsmall;
+  SG_CUDA(col_dots(a, b, f.n, f.ld, q, f.partial, dout, f.st));
+  out.resize((size_t)q);
+  SG_CUDA(cudaMemcpyAsync(out.data(), dout, out.size() * 8, cudaMemcpyDeviceToHost, f.st));
+  SG_CUDA(cudaStreamSynchronize(f.st));
+  return Status();
+}
+
+// PCG of Sigma = tau0 W^-1 + tau1 K on q columns of b into x (x0 optional).
+Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const double tau[2]) {
+  PcgRun run;
+  run.b = b;
+  run.x0 = x0;
+  run.wv = f.wmax;
+  run.d = f.d;
+  run.tau0 = tau[0];
+  run.tau1 = tau[1];
+  run.q = q;
+  run.tol = f.cfg->pcg_tol;
+  run.max_iter = f.cfg->pcg_max_iter;
+  run.precision = f.cfg->precision;
+  run.x = x;
+  SG_TRY(pcg_run(f.h, run, f.st));
+  f.pcg_iters += run.total_iters;
+  return Status();
+}
+
+// P-projection (ai_reml.rs:242-251) of q solved columns sol (in place):
+// sol -= SinvX C^-1 (SinvX' u).
+Status p_project(Fit& f, double* sol, const double* u, int q, const std::vector<double>& l) {
+  std::vector<double> t;
+  SG_TRY(dots(f, f.sol + f.ld, f.p, u, q, nullptr, t));  // p x q
+  std::vector<double> coef((size_t)f.p * q), col((size_t)f.p), corr((size_t)f.p);
+  for (int c = 0; c < q; ++c) {
+    for (int j = 0; j < f.p; ++j) col[(size_t)j] = t[(size_t)j * q + c];
+    chol_solve(l, f.p, col.data(), corr.data());
+    for (int j = 0; j < f.p; ++j) coef[(size_t)j * q + c] = corr[(size_t)j];
+  }
+  SG_CUDA(cudaMemcpyAsync(f.dsmall, coef.data(), coef.size() * 8, cudaMemcpyHostToDevice, f.st));
+  SG_CUDA(sub_combo(sol, q, f.sol + f.ld, f.p, f.dsmall, f.n, f.ld, f.st));
+  return Status();
+}
+
+Status copy_cols(Fit& f, const double* src, double* dst, int q) {
+  SG_CUDA(cudaMemcpyAsync(dst, src, (size_t)f.ld * q * 8, cudaMemcpyDeviceToDevice, f.st));
+  return Status();
+}
+
+}  // namespace
+
+}  // namespace saige
+
+using namespace saige;
+
+#define SG_API extern "C" __attribute__((visibility("default")))
+
+SG_API void saige_ai_reml_config_default(saige_ai_reml_config* c) {
+  if (!c) return;
+  c->max_iter = 30;
+  c->tol = 0.02;
+  c->pcg_tol = 1e-5;
+  c->pcg_max_iter = 500;
+  c->n_random_vectors = 30;
+  c->seed = 12345;
+  c->precision = SAIGE_PREC_FP32;
+  c->solve = SAIGE_SOLVE_SINGLE;
+  c->warm_start = SAIGE_WARM_ZERO;
+  c->reserved = 0;
+}
+
+static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n, int32_t p,
+                       int32_t trait, const saige_ai_reml_config* cfg, saige_ai_reml_summary* out,
+                       double* alpha_out, double* mu_out, double* eta_out, double* w_out,
+                       double* tau_trace) {
+  Fit f;
+  f.h = h;
+  f.st = h->stream;
+  f.n = n;
+  f.ld = h->n_pad;
+  f.p = p;
+  f.nrv = cfg->n_random_vectors;
+  f.q = 1 + p + f.nrv;
+  f.cfg = cfg;
+  const int64_t ld = f.ld;
+  const size_t nvec = 8 + 2 * (size_t)f.q + 3 * (size_t)f.nrv + 7;
+  const size_t small = (size_t)(p * f.q + p * p + 4 * f.q + 64) * 8;
+  const size_t part = (size_t)red_blocks(n) * (size_t)std::max(p * f.q, 3 * f.q) * 8;
+  SG_TRY(f.mem.reserve(nvec * ld * 8 + small + part));
+  double* base = f.mem.as<double>();
+  SG_CUDA(cudaMemsetAsync(base, 0, nvec * ld * 8, f.st));
+  auto take = [&](size_t cols) {
+    double* r = base;
+    base += cols * ld;
+    return r;
+  };
+  f.y = take(1); f.x = take((size_t)p); f.eta = take(1); f.mu = take(1); f.w = take(1);
+  f.wmax = take(1); f.d = take(1); f.ytil = take(1);
+  f.rhs = take((size_t)f.q); f.sol = take((size_t)f.q);
+  f.ku = take((size_t)f.nrv); f.pu = take((size_t)f.nrv); f.tmpq = take((size_t)f.nrv);
+  f.py = take(1); f.kpy = take(1); f.pk = take(1); f.invw_py = take(1); f.pw = take(1);
+  f.pk_raw = take(1); f.pw_raw = take(1);
+  f.dsmall = base;
+  f.partial = base + small / 8;
+
+  cudaEvent_t e0, e1;
+  SG_CUDA(cudaEventCreate(&e0));
+  SG_CUDA(cudaEventCreate(&e1));
+  SG_CUDA(cudaEventRecord(e0, f.st));
+  const int64_t kv0 = h->n_kv, kl0 = h->n_kv_launches;
+
+  SG_CUDA(cudaMemcpyAsync(f.y, y, (size_t)n * 8, cudaMemcpyHostToDevice, f.st));
+  SG_CUDA(cudaMemcpy2DAsync(f.x, (size_t)ld * 8, x, (size_t)n * 8, (size_t)n * 8, (size_t)p,
+                            cudaMemcpyHostToDevice, f.st));
+
+  // ---- GLM IRLS initialisation (ai_reml.rs:431-482) --------------------
+  std::vector<double> alpha((size_t)p, 0.0), anew((size_t)p), l, xtwx, xtwz;
+  SG_CUDA(init_mu(f.y, trait, f.mu, f.eta, n, f.st));
+  for (int it = 0; it < 25; ++it) {
+    SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, f.ytil, n, f.st));
+    SG_TRY(dots(f, f.x, p, f.x, p, f.w, xtwx));
+    SG_TRY(dots(f, f.x, p, f.ytil, 1, f.w, xtwz));
+    // symmetric fill as dense.rs:227-245 (j <= k computed, mirrored)
+    for (int j = 0; j < p; ++j)
+      for (int k = j + 1; k < p; ++k) xtwx[(size_t)k * p + j] = xtwx[(size_t)j * p + k];
+    if (!cholesky(xtwx, p, l)) {
+      for (int i = 0; i < p; ++i) xtwx[(size_t)i * p + i] += 1e-6;
+      if (!cholesky(xtwx, p, l)) return fail(SAIGE_SINGULAR, "Matrix is not positive definite (IRLS)");
+    }
+    chol_solve(l, p, xtwz.data(), anew.data());
+    SG_CUDA(cudaMemcpyAsync(f.dsmall, anew.data(), (size_t)p * 8, cudaMemcpyHostToDevice, f.st));
+    SG_CUDA(eta_mu(f.x, p, f.dsmall, trait, f.eta, f.mu, n, ld, f.st));
+    double change = 0.0;
+    for (int j = 0; j < p; ++j) change += fabs(anew[(size_t)j] - alpha[(size_t)j]);
+    alpha = anew;
+    if (change < 1e-8) break;
+  }
+  SG_CUDA(cudaMemcpyAsync(f.dsmall, alpha.data(), (size_t)p * 8, cudaMemcpyHostToDevice, f.st));
+  SG_CUDA(eta_mu(f.x, p, f.dsmall, trait, f.eta, f.mu, n, ld, f.st));
+
+  // ---- probes (ai_reml.rs:121-130), fixed for the whole fit ------------
+  {
+    std::vector<uint8_t> signs((size_t)f.nrv * n);
+    ChaCha8 rng(cfg->seed);
+    for (size_t k = 0; k < signs.size(); ++k) signs[k] = rng.gen_bool() ? 1 : 0;
+    DevBuf ds;
+    SG_TRY(ds.reserve(signs.size()));
+    SG_CUDA(cudaMemcpyAsync(ds.ptr, signs.data(), signs.size(), cudaMemcpyHostToDevice, f.st));
+    double* u = f.rhs + (size_t)(1 + p) * ld;
+    SG_CUDA(expand_signs(ds.as<uint8_t>(), u, n, ld, f.nrv, f.st));
+    SG_CUDA(cudaStreamSynchronize(f.st));
+  }
+  double* U = f.rhs + (size_t)(1 + p) * ld;
+  SG_CUDA(cudaMemcpy2DAsync(f.rhs + ld, (size_t)ld * 8, f.x, (size_t)ld * 8, (size_t)ld * 8,
+                            (size_t)p, cudaMemcpyDeviceToDevice, f.st));
+  // K u is the same every iteration (K and the probes are fixed): one block product.
+  SG_TRY(grm_product(h, U, f.ku, f.nrv, nullptr, cfg->precision, f.st));
+
+  const bool fix_tau_e = trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL;
+  double tau[2] = {1.0, 0.0};
+  int converged = 0, n_iter = 0;
+  const bool warm = cfg->warm_start != SAIGE_WARM_ZERO;
+  double* SinvY = f.sol;
+  double* SinvX = f.sol + ld;
+  double* SinvU = f.sol + (size_t)(1 + p) * ld;
+  DevBuf prev;
+  if (warm) SG_TRY(prev.reserve((size_t)ld * f.q * 8));
+
+  for (int iter = 0; iter < cfg->max_iter; ++iter) {
+    n_iter = iter + 1;
+    SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, f.ytil, n, f.st));
+    SG_CUDA(sigma_diag(f.w, tau[0], tau[1], f.wmax, f.d, n, f.st));
+    SG_CUDA(cudaMemcpyAsync(f.rhs, f.ytil, (size_t)ld * 8, cudaMemcpyDeviceToDevice, f.st));
+    if (warm && f.have_prev)
+      SG_CUDA(cudaMemcpyAsync(prev.ptr, f.sol, (size_t)ld * f.q * 8, cudaMemcpyDeviceToDevice, f.st));
+    const double* x0 = (warm && f.have_prev) ? prev.as<double>() : nullptr;
+    if (cfg->solve == SAIGE_SOLVE_BLOCK) {
+      SG_TRY(solve(f, f.rhs, f.sol, x0, f.q, tau));
+    } else {
+      // one solve per right-hand side, in the reference's order
+      for (int c = 0; c < f.q; ++c)
+        SG_TRY(solve(f, f.rhs + (size_t)c * ld, f.sol + (size_t)c * ld,
+                     x0 ? x0 + (size_t)c * ld : nullptr, 1, tau));
+    }
+    f.have_prev = true;
+
+    // X' Sigma^-1 X and X' Sigma^-1 y (ai_reml.rs:189-205)
+    std::vector<double> dxs, dxy;
+    SG_TRY(dots(f, f.x, p, SinvX, p, nullptr, dxs));  // dxs[j*p+k] = X_j . SinvX_k
+    SG_TRY(dots(f, f.x, p, SinvY, 1, nullptr, dxy));
+    std::vector<double> cmat((size_t)p * p);
+    for (int j = 0; j < p; ++j)
+      for (int k = j; k < p; ++k) {
+        const double v = dxs[(size_t)k * p + j];  // x.col(k) . sigma_inv_x[j]
+        cmat[(size_t)j * p + k] = v;
+        cmat[(size_t)k * p + j] = v;
+      }
+    if (!cholesky(cmat, p, l)) break;  // ai_reml.rs:207-213
+    chol_solve(l, p, dxy.data(), alpha.data());
+    SG_CUDA(cudaMemcpyAsync(f.dsmall, alpha.data(), (size_t)p * 8, cudaMemcpyHostToDevice, f.st));
+    SG_CUDA(eta_mu(f.x, p, f.dsmall, trait, f.eta, f.mu, n, ld, f.st));
+
+    // P y = Sinv y - SinvX alpha; YPAPY = Py' K Py (ai_reml.rs:221-232)
+    SG_TRY(copy_cols(f, SinvY, f.py, 1));
+    SG_CUDA(sub_combo(f.py, 1, SinvX, p, f.dsmall, n, ld, f.st));
+    SG_TRY(grm_product(h, f.py, f.kpy, 1, nullptr, cfg->precision, f.st));
+    std::vector<double> r1;
+    SG_TRY(coldots(f, f.py, f.kpy, 1, r1));
+    const double ypapy = r1[0];
+
+    // Hutchinson trace of P K (ai_reml.rs:237-258)
+    SG_TRY(copy_cols(f, SinvU, f.pu, f.nrv));
+    SG_TRY(p_project(f, f.pu, U, f.nrv, l));
+    std::vector<double> tr;
+    SG_TRY(coldots(f, f.ku, f.pu, f.nrv, tr));
+    double trace_sum = 0.0;
+    for (int k = 0; k < f.nrv; ++k) trace_sum += tr[(size_t)k];
+    const double trace_grm = trace_sum / (double)f.nrv;
+    const double score_g = ypapy - trace_grm;
+
+    // AI = (K P y)' P (K P y) (ai_reml.rs:263-273)
+    // warm start from the previous iteration's unprojected solution
+    if (warm && f.have_prev_pk) SG_TRY(copy_cols(f, f.pk_raw, f.pw, 1));
+    SG_TRY(solve(f, f.kpy, f.pk_raw, (warm && f.have_prev_pk) ? f.pw : nullptr, 1, tau));
+    f.have_prev_pk = true;
+    SG_TRY(copy_cols(f, f.pk_raw, f.pk, 1));
+    SG_TRY(p_project(f, f.pk, f.kpy, 1, l));
+    SG_TRY(coldots(f, f.kpy, f.pk, 1, r1));
+    const double ai_11 = r1[0];
+
+    double score_e = 0.0, ai_00 = 0.0, ai_01 = 0.0;
+    if (!fix_tau_e) {
+      // trace of P W^-1 (ai_reml.rs:281-299): the probe solves repeat the ones above
+      for (int k = 0; k < f.nrv; ++k)
+        SG_CUDA(div_w(U + (size_t)k * ld, f.w, f.tmpq + (size_t)k * ld, n, f.st));
+      SG_TRY(coldots(f, f.tmpq, f.pu, f.nrv, tr));
+      double tw = 0.0;
+      for (int k = 0; k < f.nrv; ++k) tw += tr[(size_t)k];
+      const double trace_w = tw / (double)f.nrv;
+      SG_CUDA(div_w(f.py, f.w, f.invw_py, n, f.st));
+      SG_TRY(coldots(f, f.py, f.invw_py, 1, r1));
+      score_e = r1[0] - trace_w;
+      if (warm && f.have_prev_pw) SG_TRY(copy_cols(f, f.pw_raw, f.tmpq, 1));
+      SG_TRY(solve(f, f.invw_py, f.pw_raw, (warm && f.have_prev_pw) ? f.tmpq : nullptr, 1, tau));
+      f.have_prev_pw = true;
+      SG_TRY(copy_cols(f, f.pw_raw, f.pw, 1));
+      SG_TRY(p_project(f, f.pw, f.invw_py, 1, l));
+      SG_TRY(coldots(f, f.invw_py, f.pw, 1, r1));
+      ai_00 = r1[0];
+      SG_TRY(coldots(f, f.invw_py, f.pk, 1, r1));
+      ai_01 = r1[0];
+    }
+
+    // tau update (ai_reml.rs:329-369)
+    double tn[2], max_change;
+    if (fix_tau_e) {
+      if (fabs(ai_11) < 1e-30) break;
+      const double d1 = score_g / ai_11;
+      double step = 1.0;
+      double tg = tau[1] + step * d1;
+      while (tg < 0.0 && step > 1e-10) {
+        step *= 0.5;
+        tg = tau[1] + step * d1;
+      }
+      tg = tg > 1e-10 ? tg : 1e-10;
+      max_change = fabs(tg - tau[1]) / (fabs(tg) + fabs(tau[1]) + cfg->tol);
+      tn[0] = 1.0;
+      tn[1] = tg;
+    } else {
+      const double det = ai_00 * ai_11 - ai_01 * ai_01;
+      if (fabs(det) < 1e-30) break;
+      const double d0 = (ai_11 * score_e - ai_01 * score_g) / det;
+      const double d1 = (-ai_01 * score_e + ai_00 * score_g) / det;
+      double step = 1.0;
+      double t0 = tau[0] + step * d0, t1 = tau[1] + step * d1;
+      while ((t0 < 0.0 || t1 < 0.0) && step > 1e-10) {
+        step *= 0.5;
+        t0 = tau[0] + step * d0;
+        t1 = tau[1] + step * d1;
+      }
+      tn[0] = t0 > 1e-10 ? t0 : 1e-10;
+      tn[1] = t1 > 1e-10 ? t1 : 1e-10;
+      const double c0 = fabs(tn[0] - tau[0]) / (fabs(tn[0]) + fabs(tau[0]) + cfg->tol);
+      const double c1 = fabs(tn[1] - tau[1]) / (fabs(tn[1]) + fabs(tau[1]) + cfg->tol);
+      max_change = c0 > c1 ? c0 : c1;
+    }
+    tau[0] = tn[0];
+    tau[1] = tn[1];
+    if (tau_trace) {
+      tau_trace[2 * iter] = tau[0];
+      tau_trace[2 * iter + 1] = tau[1];
+    }
+    if (max_change < cfg->tol) {
+      converged = 1;
+      break;
+    }
+  }
+
+  // final W, log-likelihood (ai_reml.rs:393-414)
+  SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, nullptr, n, f.st));
+  SG_CUDA(cudaEventRecord(e1, f.st));
+  std::vector<double> mu((size_t)n), yh(y, y + n);
+  SG_CUDA(cudaMemcpyAsync(mu.data(), f.mu, (size_t)n * 8, cudaMemcpyDeviceToHost, f.st));
+  if (eta_out) SG_CUDA(cudaMemcpyAsync(eta_out, f.eta, (size_t)n * 8, cudaMemcpyDeviceToHost, f.st));
+  if (w_out) SG_CUDA(cudaMemcpyAsync(w_out, f.w, (size_t)n * 8, cudaMemcpyDeviceToHost, f.st));
+  SG_CUDA(cudaStreamSynchronize(f.st));
+  double ll = 0.0;
+  if (trait == SAIGE_TRAIT_QUANTITATIVE) {
+    double ss = 0.0;
+    for (int64_t i = 0; i < n; ++i) ss += (yh[(size_t)i] - mu[(size_t)i]) * (yh[(size_t)i] - mu[(size_t)i]);
+    ll = -0.5 * (double)n * log(2.0 * M_PI * tau[0]) - 0.5 * ss / tau[0];
+  } else {
+    for (int64_t i = 0; i < n; ++i) {
+      double mi = mu[(size_t)i];
+      mi = mi < 1e-15 ? 1e-15 : (mi > 1.0 - 1e-15 ? 1.0 - 1e-15 : mi);
+      ll += yh[(size_t)i] * log(mi) + (1.0 - yh[(size_t)i]) * log(1.0 - mi);
+    }
+  }
+  float ms = 0.f;
+  SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (mu_out) memcpy(mu_out, mu.data(), (size_t)n * 8);
+  if (alpha_out) memcpy(alpha_out, alpha.data(), (size_t)p * 8);
+  out->tau[0] = tau[0];
+  out->tau[1] = tau[1];
+  out->iterations = n_iter;
+  out->converged = converged;
+  out->log_likelihood = ll;
+  out->n_kv = h->n_kv - kv0;
+  out->n_kv_launches = h->n_kv_launches - kl0;
+  out->pcg_iters = f.pcg_iters;
+  out->seconds = ms * 1e-3;
+  return Status();
+}
+
+SG_API int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x, int64_t n,
+                                 int32_t p, int32_t trait, const saige_ai_reml_config* cfg,
+                                 saige_ai_reml_summary* out, double* alpha, double* mu,
+                                 double* eta, double* w, double* tau_trace) {
+  try {
+    set_error("");
+    if (!h || !y || !x || !out) return fail(SAIGE_EINVAL, "null argument").code;
+    if (n != h->n) return fail(SAIGE_EINVAL, "y.len() != n_samples").code;
+    if (p <= 0 || p > 64) return fail(SAIGE_EINVAL, "p must be in 1..64").code;
+    if (trait < 0 || trait > 2) return fail(SAIGE_EINVAL, "unknown trait type").code;
+    saige_ai_reml_config c;
+    if (cfg) c = *cfg;
+    else saige_ai_reml_config_default(&c);
+    if (c.n_random_vectors <= 0) return fail(SAIGE_EINVAL, "n_random_vectors must be positive").code;
+    if (c.max_iter < 0) return fail(SAIGE_EINVAL, "max_iter must be >= 0").code;
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    Status s = fit_impl(h, y, x, n, p, trait, &c, out, alpha, mu, eta, w, tau_trace);
+    if (prev >= 0) cudaSetDevice(prev);
+    return s.code;
+  } catch (const std::bad_alloc&) {
+    return fail(SAIGE_ENOMEM, "host allocation failed").code;
+  } catch (...) {
+    return fail(SAIGE_EINVAL, "unexpected C++ exception").code;
+  }
+}

@@ -1,0 +1,757 @@
+// GRM handle lifecycle, GRM product dispatch, PCG driver and the C ABI.
+#include <math.h>
+#include <stdarg.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "engine.cuh"
+#include "kernels.cuh"
+#include "kernels_tc.cuh"
+#include "rng.hpp"
+
+namespace saige {
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+const char* last_error() { return g_err.c_str(); }
+
+Status fail(int32_t code, const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return Status(code);
+}
+
+Status DevBuf::reserve(size_t want) {
+  if (want <= bytes) return Status();
+  release();
+  if (want == 0) return Status();
+  cudaError_t e = cudaMalloc(&ptr, want);
+  if (e != cudaSuccess) {
+    ptr = nullptr;
+    bytes = 0;
+    (void)cudaGetLastError();
+    return fail(SAIGE_ENOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+  }
+  bytes = want;
+  return Status();
+}
+
+void DevBuf::release() {
+  if (ptr) cudaFree(ptr);
+  ptr = nullptr;
+  bytes = 0;
+}
+
+// ---------------------------------------------------------------------------
+// device selection
+// ---------------------------------------------------------------------------
+static Status pick_device(int32_t want, int* dev) {
+  int count = 0;
+  cudaError_t e = cudaGetDeviceCount(&count);
+  if (e != cudaSuccess || count == 0) {
+    (void)cudaGetLastError();
+    return fail(SAIGE_ECUDA, "no CUDA device available (%s)",
+                e == cudaSuccess ? "count = 0" : cudaGetErrorString(e));
+  }
+  int d = want;
+  if (d < 0) SG_CUDA(cudaGetDevice(&d));
+  if (d >= count) return fail(SAIGE_EINVAL, "device %d out of range (%d devices)", d, count);
+  cudaDeviceProp prop;
+  SG_CUDA(cudaGetDeviceProperties(&prop, d));
+  if (prop.major != 10 || prop.minor != 0)
+    return fail(SAIGE_ECUDA, "device %d is sm_%d%d; this library is built for sm_100a only", d,
+                prop.major, prop.minor);
+  SG_CUDA(cudaSetDevice(d));
+  *dev = d;
+  return Status();
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != d) cudaSetDevice(d);
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
+// ---------------------------------------------------------------------------
+// per-marker metadata (pcg.rs:101-122 arithmetic, done on the host in f64)
+// ---------------------------------------------------------------------------
+static void marker_meta(const double* af, int64_t m, int64_t m_pad, std::vector<float4>& zl,
+                        std::vector<double>& tp, std::vector<double>& is) {
+  zl.assign((size_t)m_pad, make_float4(0.f, 0.f, 0.f, 0.f));
+  tp.assign((size_t)m_pad, 0.0);
+  is.assign((size_t)m_pad, 0.0);
+  for (int64_t j = 0; j < m; ++j) {
+    const double p = af[j];
+    const double denom = sqrt(2.0 * p * (1.0 - p));
+    if (!(denom > 1e-10)) continue;  // OnTheFlyGrm leaves the column at 0
+    const double mean = 2.0 * p;
+    // codes 00 -> 2, 01 -> missing (mean, so exactly 0), 10 -> 1, 11 -> 0
+    zl[j] = make_float4((float)((2.0 - mean) / denom), 0.0f, (float)((1.0 - mean) / denom),
+                        (float)((0.0 - mean) / denom));
+    tp[j] = mean;
+    is[j] = 1.0 / denom;
+  }
+}
+
+static Status grm_alloc(saige_grm* h, int64_t n, int64_t m) {
+  h->n = n;
+  h->n_pad = round_up(std::max<int64_t>(n, 1), kSamplePad);
+  h->wpr = h->n_pad / 16;
+  h->m = m;
+  h->m_pad = round_up(std::max<int64_t>(m, 1), kMarkerPad);
+  SG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  SG_CUDA(cudaMalloc(&h->geno, (size_t)h->m_pad * h->wpr * 4));
+  SG_CUDA(cudaMalloc(&h->zlut, (size_t)h->m_pad * sizeof(float4)));
+  SG_CUDA(cudaMalloc(&h->two_p, (size_t)h->m_pad * sizeof(double)));
+  SG_CUDA(cudaMalloc(&h->inv_s, (size_t)h->m_pad * sizeof(double)));
+  // padding rows: all codes missing
+  SG_CUDA(cudaMemsetAsync(h->geno + (size_t)m * h->wpr, 0x55,
+                          (size_t)(h->m_pad - m) * h->wpr * 4, h->stream));
+  h->n_splits = fp32_z_splits(h->n_pad, h->m_pad);
+  return Status();
+}
+
+static Status grm_upload_meta(saige_grm* h, const double* af) {
+  std::vector<float4> zl;
+  std::vector<double> tp, is;
+  marker_meta(af, h->m, h->m_pad, zl, tp, is);
+  SG_CUDA(cudaMemcpy(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice));
+  SG_CUDA(cudaMemcpy(h->two_p, tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice));
+  SG_CUDA(cudaMemcpy(h->inv_s, is.data(), is.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return Status();
+}
+
+static void grm_free(saige_grm* h) {
+  if (!h) return;
+  cudaSetDevice(h->device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  tc_destroy(h);
+  h->v32.release();
+  h->u32.release();
+  h->ypart.release();
+  h->ws_vec.release();
+  h->ws_red.release();
+  h->ws_cols.release();
+  h->ws_io.release();
+  if (h->geno) cudaFree(h->geno);
+  if (h->zlut) cudaFree(h->zlut);
+  if (h->two_p) cudaFree(h->two_p);
+  if (h->inv_s) cudaFree(h->inv_s);
+  if (h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+static Status check_bed_header(const uint8_t* hdr, size_t bed_len, int64_t n_fam, int64_t m_tot) {
+  if (bed_len < 3) return fail(SAIGE_EBED, "Bed file too small");
+  if (hdr[0] != 0x6C || hdr[1] != 0x1B) return fail(SAIGE_EBED, "Invalid PLINK bed file magic number");
+  if (hdr[2] != 0x01)
+    return fail(SAIGE_EBED, "Only SNP-major bed files are supported (mode byte = 0x01)");
+  const int64_t bpm = (n_fam + 3) / 4;
+  if ((int64_t)bed_len < 3 + bpm * m_tot)
+    return fail(SAIGE_EBED, "Bed file too small: expected at least %lld bytes, got %zu",
+                (long long)(3 + bpm * m_tot), bed_len);
+  return Status();
+}
+
+static Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam,
+                           std::vector<int32_t>& out, bool& identity) {
+  identity = true;
+  if (n <= 0) return fail(SAIGE_EINVAL, "n must be positive");
+  if (n_fam > INT32_MAX) return fail(SAIGE_EINVAL, "n_fam exceeds 2^31-1");
+  if (!sidx) {
+    if (n != n_fam) return fail(SAIGE_EINVAL, "n (%lld) != n_fam (%lld) without sample_idx",
+                                (long long)n, (long long)n_fam);
+    return Status();
+  }
+  out.resize((size_t)n);
+  for (int64_t k = 0; k < n; ++k) {
+    if (sidx[k] < 0 || sidx[k] >= n_fam)
+      return fail(SAIGE_EINVAL, "sample_idx[%lld] = %lld out of range", (long long)k,
+                  (long long)sidx[k]);
+    out[(size_t)k] = (int32_t)sidx[k];
+    if (sidx[k] != k) identity = false;
+  }
+  if (n != n_fam) identity = false;
+  return Status();
+}
+
+// Gather rows of a device-resident .bed into the handle (or count only).
+static Status bed_gather_dev(const uint8_t* bed_dev, int64_t n_fam, const std::vector<int64_t>& rows,
+                             const std::vector<int32_t>& sidx, bool identity, int64_t n,
+                             uint32_t* geno_out, int64_t wpr, int64_t* counts_dev,
+                             cudaStream_t st) {
+  DevBuf d_rows, d_sidx;
+  SG_TRY(d_rows.reserve(rows.size() * sizeof(int64_t)));
+  SG_CUDA(cudaMemcpyAsync(d_rows.ptr, rows.data(), rows.size() * sizeof(int64_t),
+                          cudaMemcpyHostToDevice, st));
+  const int32_t* sp = nullptr;
+  if (!identity) {
+    SG_TRY(d_sidx.reserve(sidx.size() * sizeof(int32_t)));
+    SG_CUDA(cudaMemcpyAsync(d_sidx.ptr, sidx.data(), sidx.size() * sizeof(int32_t),
+                            cudaMemcpyHostToDevice, st));
+    sp = d_sidx.as<int32_t>();
+  }
+  SG_CUDA(launch_bed_gather(bed_dev, (n_fam + 3) / 4, d_rows.as<int64_t>(), (int64_t)rows.size(),
+                            sp, n, geno_out, wpr, counts_dev, st));
+  SG_CUDA(cudaStreamSynchronize(st));
+  return Status();
+}
+
+// ---------------------------------------------------------------------------
+// GRM product
+// ---------------------------------------------------------------------------
+static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
+                               const int32_t* active, cudaStream_t st) {
+  SG_TRY(h->v32.reserve((size_t)h->n_pad * sizeof(float)));
+  SG_TRY(h->u32.reserve((size_t)h->m_pad * sizeof(float)));
+  SG_TRY(h->ypart.reserve((size_t)h->n_splits * h->n_pad * sizeof(float)));
+  const float scale = 1.0f / (float)h->m;
+  for (int c = 0; c < q; ++c) {
+    if (active && active[c] != kColActive) continue;
+    const double* vc = v + (int64_t)c * h->n_pad;
+    double* oc = kp + (int64_t)c * h->n_pad;
+    SG_CUDA(launch_to_f32(vc, h->n, h->n_pad, h->v32.as<float>(), st));
+    SG_CUDA(launch_fp32_zt(h->geno, h->wpr, h->zlut, h->m_pad, h->v32.as<float>(),
+                           h->u32.as<float>(), st));
+    SG_CUDA(launch_fp32_z(h->geno, h->wpr, h->zlut, h->m_pad, h->u32.as<float>(),
+                          h->ypart.as<float>(), h->n_splits, st));
+    SG_CUDA(launch_fp32_finish(h->ypart.as<float>(), h->n_splits, h->n_pad, h->n, scale, oc, st));
+    h->n_kv += 1;
+    h->n_kv_launches += 1;
+  }
+  return Status();
+}
+
+Status grm_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
+                   int precision, cudaStream_t st) {
+  if (h->m == 0) {
+    // pcg.rs:132-134: no markers -> zero vector
+    for (int c = 0; c < q; ++c)
+      if (!active || active[c] == kColActive)
+        SG_CUDA(cudaMemsetAsync(kp + (int64_t)c * h->n_pad, 0, (size_t)h->n_pad * 8, st));
+    return Status();
+  }
+  if (precision == SAIGE_PREC_FP32) return grm_product_fp32(h, v, kp, q, active, st);
+  if (precision == SAIGE_PREC_MIXED) return tc_product(h, v, kp, q, active, st);
+  return fail(SAIGE_EINVAL, "unknown precision %d", precision);
+}
+
+// ---------------------------------------------------------------------------
+// PCG driver
+// ---------------------------------------------------------------------------
+Status pcg_scratch(saige_grm* h, int q, PcgScratch& s) {
+  const int64_t ld = h->n_pad;
+  const int nb = red_blocks(h->n);
+  SG_TRY(h->ws_vec.reserve((size_t)5 * ld * q * sizeof(double)));
+  SG_TRY(h->ws_red.reserve((size_t)nb * 3 * q * sizeof(double) + 64));
+  SG_TRY(h->ws_cols.reserve((size_t)q * (8 * sizeof(double) + 2 * sizeof(int32_t)) + 256));
+  double* base = h->ws_vec.as<double>();
+  s.r = base;
+  s.z = base + (int64_t)1 * ld * q;
+  s.p = base + (int64_t)2 * ld * q;
+  s.ap = base + (int64_t)3 * ld * q;
+  s.kp = base + (int64_t)4 * ld * q;
+  s.partial = h->ws_red.as<double>();
+  double* cb = h->ws_cols.as<double>();
+  s.cols.rz = cb;
+  s.cols.rr = cb + q;
+  s.cols.pap = cb + 2 * q;
+  s.cols.tol_abs = cb + 3 * q;
+  s.small = cb + 4 * q;  // 4q doubles
+  int32_t* ib = reinterpret_cast<int32_t*>(cb + 8 * q);
+  s.cols.state = ib;
+  s.cols.iters = ib + q;
+  return Status();
+}
+
+Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
+  const int q = run.q;
+  const int64_t n = h->n, ld = h->n_pad;
+  PcgScratch s;
+  SG_TRY(pcg_scratch(h, q, s));
+  std::vector<int32_t> state((size_t)q, kColActive);
+  const double* ax0 = nullptr;
+  if (run.x0) {
+    // r = b - A x0 (decomposition.rs:225-227)
+    SG_CUDA(cudaMemsetAsync(s.cols.state, 0, (size_t)q * sizeof(int32_t), st));
+    SG_TRY(grm_product(h, run.x0, s.kp, q, nullptr, run.precision, st));
+    if (run.w_inverse)
+      SG_CUDA(pcg_apply(run.x0, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
+                        s.partial, st));
+    else
+      SG_CUDA(pcg_apply_w(run.x0, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
+                          s.partial, st));
+    ax0 = s.ap;
+  }
+  SG_CUDA(pcg_start(run.b, run.x0, ax0, run.d, run.x, s.r, s.z, s.p, n, ld, q, run.tol, s.cols,
+                    s.partial, s.small, st));
+  if (run.max_iter <= 0) {
+    // the loop body never runs; converged is the initial test
+    SG_CUDA(cudaMemcpyAsync(state.data(), s.cols.state, (size_t)q * 4, cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+  } else {
+    for (;;) {
+      SG_CUDA(cudaMemcpyAsync(state.data(), s.cols.state, (size_t)q * 4, cudaMemcpyDeviceToHost,
+                              st));
+      SG_CUDA(cudaStreamSynchronize(st));
+      bool any = false;
+      for (int c = 0; c < q; ++c) any |= state[(size_t)c] == kColActive;
+      if (!any) break;
+      SG_TRY(grm_product(h, s.p, s.kp, q, state.data(), run.precision, st));
+      if (run.w_inverse)
+        SG_CUDA(pcg_apply(s.p, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
+                          s.partial, st));
+      else
+        SG_CUDA(pcg_apply_w(s.p, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
+                            s.partial, st));
+      SG_CUDA(pcg_step(run.x, s.r, s.z, s.p, s.ap, run.d, n, ld, q, run.max_iter, s.cols,
+                       s.partial, s.small, st));
+    }
+  }
+  std::vector<double> rr((size_t)q);
+  run.iters.assign((size_t)q, 0);
+  run.state = state;
+  SG_CUDA(cudaMemcpyAsync(run.iters.data(), s.cols.iters, (size_t)q * 4, cudaMemcpyDeviceToHost, st));
+  SG_CUDA(cudaMemcpyAsync(rr.data(), s.cols.rr, (size_t)q * 8, cudaMemcpyDeviceToHost, st));
+  SG_CUDA(cudaStreamSynchronize(st));
+  run.resid.resize((size_t)q);
+  run.total_iters = 0;
+  for (int c = 0; c < q; ++c) {
+    run.resid[(size_t)c] = sqrt(rr[(size_t)c]);
+    if (run.max_iter <= 0 && state[(size_t)c] == kColActive) run.state[(size_t)c] = kColMaxIter;
+    run.total_iters += run.iters[(size_t)c];
+  }
+  return Status();
+}
+
+}  // namespace saige
+
+using namespace saige;
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+#define SG_API extern "C" __attribute__((visibility("default")))
+
+#define SG_GUARD_BEGIN try {
+#define SG_GUARD_END                                                          \
+  }                                                                           \
+  catch (const std::bad_alloc&) {                                             \
+    return fail(SAIGE_ENOMEM, "host allocation failed").code;                 \
+  }                                                                           \
+  catch (...) {                                                               \
+    return fail(SAIGE_EINVAL, "unexpected C++ exception").code;               \
+  }
+
+SG_API const char* saige_last_error(void) { return last_error(); }
+
+SG_API int32_t saige_version(void) { return 1 * 10000 + 0 * 100 + 0; }
+
+SG_API int32_t saige_device_count(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    (void)cudaGetLastError();
+    return 0;
+  }
+  int usable = 0;
+  for (int d = 0; d < count; ++d) {
+    cudaDeviceProp p;
+    if (cudaGetDeviceProperties(&p, d) == cudaSuccess && p.major == 10 && p.minor == 0) ++usable;
+  }
+  return usable;
+}
+
+SG_API int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                      int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                      double* af, double* mac, int64_t* n_valid) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!bed || !af || !mac || !n_valid || m_tot < 0) return fail(SAIGE_EINVAL, "null argument").code;
+  Status s = check_bed_header(bed, bed_len, n_fam, m_tot);
+  if (!s.ok()) return s.code;
+  std::vector<int32_t> sidx;
+  bool identity;
+  s = check_subset(sample_idx, n, n_fam, sidx, identity);
+  if (!s.ok()) return s.code;
+  int dev;
+  s = pick_device(-1, &dev);
+  if (!s.ok()) return s.code;
+  const int64_t bpm = (n_fam + 3) / 4;
+  const size_t used = (size_t)(3 + bpm * m_tot);
+  cudaStream_t st;
+  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+    return fail(SAIGE_ECUDA, "stream creation failed").code;
+  DevBuf d_bed, d_cnt;
+  auto body = [&]() -> Status {
+    SG_TRY(d_bed.reserve(used));
+    SG_TRY(d_cnt.reserve((size_t)std::max<int64_t>(m_tot, 1) * 2 * sizeof(int64_t)));
+    SG_CUDA(cudaMemcpyAsync(d_bed.ptr, bed, used, cudaMemcpyHostToDevice, st));
+    std::vector<int64_t> rows((size_t)m_tot);
+    for (int64_t j = 0; j < m_tot; ++j) rows[(size_t)j] = j;
+    if (m_tot > 0)
+      SG_TRY(bed_gather_dev(d_bed.as<uint8_t>(), n_fam, rows, sidx, identity, n, nullptr, 0,
+                            d_cnt.as<int64_t>(), st));
+    std::vector<int64_t> cnt((size_t)m_tot * 2);
+    if (m_tot > 0) {
+      SG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
+    }
+    for (int64_t j = 0; j < m_tot; ++j) {
+      const int64_t alt = cnt[(size_t)(2 * j)], miss = cnt[(size_t)(2 * j + 1)];
+      const int64_t nv = n - miss;
+      // traits.rs:42-54, the same f64 operations on the same exact integers
+      const double sum = (double)alt;
+      af[j] = nv > 0 ? sum / (2.0 * (double)nv) : 0.0;
+      const double other = 2.0 * (double)nv - sum;
+      mac[j] = sum < other ? sum : other;
+      n_valid[j] = nv;
+    }
+    return Status();
+  };
+  s = body();
+  d_bed.release();
+  d_cnt.release();
+  cudaStreamDestroy(st);
+  return s.code;
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_select_grm_markers(const double* af, const double* mac,
+                                        const int64_t* n_valid, int64_t m_tot, int64_t n,
+                                        double min_maf, double max_missing, uint64_t seed,
+                                        int64_t* grm_idx, int64_t* m_grm, int64_t* vr_idx,
+                                        int64_t* m_vr) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!af || !mac || !n_valid || !grm_idx || !m_grm || !vr_idx || !m_vr || n <= 0)
+    return fail(SAIGE_EINVAL, "null argument or n <= 0").code;
+  // fit_null.rs:209-222
+  std::vector<int64_t> pass;
+  pass.reserve((size_t)m_tot);
+  for (int64_t j = 0; j < m_tot; ++j) {
+    const double missing_rate = 1.0 - ((double)n_valid[j] / (double)n);
+    if (af[j] >= min_maf && af[j] <= 1.0 - min_maf && missing_rate <= max_missing)
+      pass.push_back(j);
+  }
+  *m_grm = 0;
+  *m_vr = 0;
+  if (pass.empty())
+    return fail(SAIGE_EINVAL, "no marker passes QC (gen_range(0..0) in the reference)").code;
+  // fit_null.rs:234-243
+  ChaCha8 rng(seed);
+  std::vector<uint64_t> cand(1000);
+  for (auto& c : cand) c = rng.gen_range(0, (uint64_t)pass.size());
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  std::vector<uint8_t> vr(pass.size(), 0);
+  for (uint64_t c : cand)
+    if (mac[pass[(size_t)c]] >= 20.0) vr[(size_t)c] = 1;
+  int64_t g = 0, v = 0;
+  for (size_t i = 0; i < pass.size(); ++i) {
+    if (vr[i]) vr_idx[v++] = pass[i];
+    else grm_idx[g++] = pass[i];
+  }
+  *m_grm = g;
+  *m_vr = v;
+  return SAIGE_OK;
+  SG_GUARD_END
+}
+
+static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t bed_len,
+                                    int64_t n_fam, int64_t m_tot, const int64_t* sample_idx,
+                                    int64_t n, const int64_t* marker_idx, int64_t m,
+                                    const double* allele_freqs, int32_t device, saige_grm** out) {
+  if (!bed || !out || (m > 0 && (!marker_idx || !allele_freqs)) || m < 0)
+    return fail(SAIGE_EINVAL, "null argument").code;
+  *out = nullptr;
+  std::vector<uint8_t> hdr(3, 0);
+  int dev;
+  Status s = pick_device(device, &dev);
+  if (!s.ok()) return s.code;
+  if (on_device) {
+    if (bed_len >= 3 && cudaMemcpy(hdr.data(), bed, 3, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(SAIGE_ECUDA, "reading the bed header from device memory failed").code;
+  } else if (bed_len >= 3) {
+    memcpy(hdr.data(), bed, 3);
+  }
+  s = check_bed_header(hdr.data(), bed_len, n_fam, m_tot);
+  if (!s.ok()) return s.code;
+  std::vector<int32_t> sidx;
+  bool identity;
+  s = check_subset(sample_idx, n, n_fam, sidx, identity);
+  if (!s.ok()) return s.code;
+  std::vector<int64_t> rows((size_t)m);
+  for (int64_t r = 0; r < m; ++r) {
+    if (marker_idx[r] < 0 || marker_idx[r] >= m_tot)
+      return fail(SAIGE_EINVAL, "marker_idx[%lld] out of range", (long long)r).code;
+    rows[(size_t)r] = marker_idx[r];
+  }
+  saige_grm* h = new saige_grm();
+  h->device = dev;
+  auto body = [&]() -> Status {
+    SG_TRY(grm_alloc(h, n, m));
+    SG_TRY(grm_upload_meta(h, allele_freqs));
+    if (m > 0) {
+      const int64_t bpm = (n_fam + 3) / 4;
+      const size_t used = (size_t)(3 + bpm * m_tot);
+      DevBuf d_bed;
+      const uint8_t* src = bed;
+      if (!on_device) {
+        SG_TRY(d_bed.reserve(used));
+        SG_CUDA(cudaMemcpyAsync(d_bed.ptr, bed, used, cudaMemcpyHostToDevice, h->stream));
+        src = d_bed.as<uint8_t>();
+      }
+      SG_TRY(bed_gather_dev(src, n_fam, rows, sidx, identity, n, h->geno, h->wpr, nullptr,
+                            h->stream));
+    }
+    SG_CUDA(cudaStreamSynchronize(h->stream));
+    return Status();
+  };
+  s = body();
+  if (!s.ok()) {
+    grm_free(h);
+    return s.code;
+  }
+  *out = h;
+  return SAIGE_OK;
+}
+
+SG_API int32_t saige_grm_create_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                         int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                         const int64_t* marker_idx, int64_t m,
+                                         const double* allele_freqs, int32_t device,
+                                         saige_grm** out) {
+  SG_GUARD_BEGIN
+  set_error("");
+  return create_from_bed_impl(bed, false, bed_len, n_fam, m_tot, sample_idx, n, marker_idx, m,
+                              allele_freqs, device, out);
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_create_from_bed_dev(const uint8_t* bed_dev, size_t bed_len,
+                                             int64_t n_fam, int64_t m_tot,
+                                             const int64_t* sample_idx, int64_t n,
+                                             const int64_t* marker_idx, int64_t m,
+                                             const double* allele_freqs, int32_t device,
+                                             saige_grm** out) {
+  SG_GUARD_BEGIN
+  set_error("");
+  return create_from_bed_impl(bed_dev, true, bed_len, n_fam, m_tot, sample_idx, n, marker_idx, m,
+                              allele_freqs, device, out);
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_create_from_dosages(const double* dosages, int64_t n, int64_t m,
+                                             const double* allele_freqs, int32_t device,
+                                             saige_grm** out) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!out || n <= 0 || m < 0 || (m > 0 && (!dosages || !allele_freqs)))
+    return fail(SAIGE_EINVAL, "null argument or bad dimension").code;
+  // Encode hard calls as a .bed image and reuse the packed path.
+  const int64_t bpm = (n + 3) / 4;
+  std::vector<uint8_t> bed((size_t)(3 + bpm * m), 0);
+  bed[0] = 0x6C;
+  bed[1] = 0x1B;
+  bed[2] = 0x01;
+  for (int64_t j = 0; j < m; ++j) {
+    uint8_t* row = bed.data() + 3 + j * bpm;
+    for (int64_t i = 0; i < n; ++i) {
+      const double g = dosages[j * n + i];
+      uint32_t code;
+      if (isnan(g)) code = 1;
+      else if (g == 2.0) code = 0;
+      else if (g == 1.0) code = 2;
+      else if (g == 0.0) code = 3;
+      else
+        return fail(SAIGE_EINVAL, "dosage[%lld][%lld] = %g is not a hard call (0, 1, 2 or NaN)",
+                    (long long)j, (long long)i, g)
+            .code;
+      row[i >> 2] |= (uint8_t)(code << ((i & 3) * 2));
+    }
+  }
+  std::vector<int64_t> rows((size_t)m);
+  for (int64_t j = 0; j < m; ++j) rows[(size_t)j] = j;
+  return create_from_bed_impl(bed.data(), false, bed.size(), n, m, nullptr, n, rows.data(), m,
+                              allele_freqs, device, out);
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_destroy(saige_grm* h) {
+  SG_GUARD_BEGIN
+  grm_free(h);
+  return SAIGE_OK;
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_dims(const saige_grm* h, int64_t* n, int64_t* m) {
+  if (!h) return fail(SAIGE_EINVAL, "null handle").code;
+  if (n) *n = h->n;
+  if (m) *m = h->m;
+  return SAIGE_OK;
+}
+
+// Copy a host block (n x q, vector-major) into a padded device block.
+static Status upload_block(saige_grm* h, const double* src, double* dst, int q, cudaStream_t st) {
+  SG_CUDA(cudaMemcpy2DAsync(dst, (size_t)h->n_pad * 8, src, (size_t)h->n * 8, (size_t)h->n * 8, q,
+                            cudaMemcpyHostToDevice, st));
+  SG_CUDA(zero_pad(dst, h->n, h->n_pad, q, st));
+  return Status();
+}
+static Status download_block(saige_grm* h, const double* src, double* dst, int q, cudaStream_t st) {
+  SG_CUDA(cudaMemcpy2DAsync(dst, (size_t)h->n * 8, src, (size_t)h->n_pad * 8, (size_t)h->n * 8, q,
+                            cudaMemcpyDeviceToHost, st));
+  return Status();
+}
+static Status devcopy_block(saige_grm* h, const double* src, int64_t sld, double* dst, int64_t dld,
+                            int q, cudaStream_t st) {
+  SG_CUDA(cudaMemcpy2DAsync(dst, (size_t)dld * 8, src, (size_t)sld * 8, (size_t)h->n * 8, q,
+                            cudaMemcpyDeviceToDevice, st));
+  return Status();
+}
+
+SG_API int32_t saige_grm_matvec(saige_grm* h, const double* v, double* out, int64_t n,
+                                int32_t nrhs, int32_t precision) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!h || !v || !out) return fail(SAIGE_EINVAL, "null argument").code;
+  if (n != h->n) return fail(SAIGE_EINVAL, "v.len() = %lld != n_samples = %lld", (long long)n,
+                             (long long)h->n).code;  // pcg.rs:129
+  if (nrhs <= 0) return fail(SAIGE_EINVAL, "nrhs must be positive").code;
+  std::lock_guard<std::recursive_mutex> lk(h->mu);
+  DeviceGuard dg(h->device);
+  auto body = [&]() -> Status {
+    const size_t blk = (size_t)h->n_pad * nrhs * sizeof(double);
+    SG_TRY(h->ws_io.reserve(2 * blk));
+    double* dv = h->ws_io.as<double>();
+    double* dk = dv + (size_t)h->n_pad * nrhs;
+    SG_TRY(upload_block(h, v, dv, nrhs, h->stream));
+    SG_TRY(grm_product(h, dv, dk, nrhs, nullptr, precision, h->stream));
+    SG_TRY(download_block(h, dk, out, nrhs, h->stream));
+    SG_CUDA(cudaStreamSynchronize(h->stream));
+    return Status();
+  };
+  return body().code;
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_matvec_dev(saige_grm* h, const double* v_dev, double* out_dev, int64_t n,
+                                    int32_t nrhs, int32_t precision, void* stream) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!h || !v_dev || !out_dev) return fail(SAIGE_EINVAL, "null argument").code;
+  if (n != h->n) return fail(SAIGE_EINVAL, "n mismatch").code;
+  if (nrhs <= 0) return fail(SAIGE_EINVAL, "nrhs must be positive").code;
+  std::lock_guard<std::recursive_mutex> lk(h->mu);
+  DeviceGuard dg(h->device);
+  cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
+  auto body = [&]() -> Status {
+    const size_t blk = (size_t)h->n_pad * nrhs * sizeof(double);
+    SG_TRY(h->ws_io.reserve(2 * blk));
+    double* dv = h->ws_io.as<double>();
+    double* dk = dv + (size_t)h->n_pad * nrhs;
+    SG_TRY(devcopy_block(h, v_dev, h->n, dv, h->n_pad, nrhs, st));
+    SG_CUDA(zero_pad(dv, h->n, h->n_pad, nrhs, st));
+    SG_TRY(grm_product(h, dv, dk, nrhs, nullptr, precision, st));
+    SG_TRY(devcopy_block(h, dk, h->n_pad, out_dev, h->n, nrhs, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    return Status();
+  };
+  return body().code;
+  SG_GUARD_END
+}
+
+static int32_t pcg_entry(saige_grm* h, const double* w, const double tau[2], const double* b,
+                         const double* x0, double* x, int64_t n, int32_t nrhs,
+                         const saige_pcg_options* opt, int32_t* iters, double* resid,
+                         uint8_t* converged, bool w_inverse) {
+  if (!h || !w || !tau || !b || !x) return fail(SAIGE_EINVAL, "null argument").code;
+  if (n != h->n) return fail(SAIGE_EINVAL, "n mismatch (%lld vs %lld)", (long long)n,
+                             (long long)h->n).code;
+  if (nrhs <= 0) return fail(SAIGE_EINVAL, "nrhs must be positive").code;
+  saige_pcg_options o = {1e-5, 500, SAIGE_PREC_FP32};
+  if (opt) o = *opt;
+  std::lock_guard<std::recursive_mutex> lk(h->mu);
+  DeviceGuard dg(h->device);
+  cudaStream_t st = h->stream;
+  auto body = [&]() -> Status {
+    const int64_t ld = h->n_pad;
+    const size_t blk = (size_t)ld * nrhs;
+    // io: b, x0, x (blocks) + wv, d (vectors)
+    SG_TRY(h->ws_io.reserve((3 * blk + 3 * (size_t)ld) * sizeof(double)));
+    double* db = h->ws_io.as<double>();
+    double* dx0 = db + blk;
+    double* dx = dx0 + blk;
+    double* dw = dx + blk;
+    double* dwv = dw + ld;
+    double* dd = dwv + ld;
+    SG_TRY(upload_block(h, b, db, nrhs, st));
+    if (x0) SG_TRY(upload_block(h, x0, dx0, nrhs, st));
+    SG_TRY(upload_block(h, w, dw, 1, st));
+    if (w_inverse) {
+      SG_CUDA(sigma_diag(dw, tau[0], tau[1], dwv, dd, h->n, st));
+    } else {
+      SG_CUDA(sigma_diag_w(dw, tau[0], tau[1], dd, h->n, st));
+      SG_CUDA(cudaMemcpyAsync(dwv, dw, (size_t)ld * 8, cudaMemcpyDeviceToDevice, st));
+    }
+    PcgRun run;
+    run.b = db;
+    run.x0 = x0 ? dx0 : nullptr;
+    run.wv = dwv;
+    run.d = dd;
+    run.tau0 = tau[0];
+    run.tau1 = tau[1];
+    run.w_inverse = w_inverse;
+    run.q = nrhs;
+    run.tol = o.tol;
+    run.max_iter = o.max_iter;
+    run.precision = o.precision;
+    run.x = dx;
+    SG_TRY(pcg_run(h, run, st));
+    SG_TRY(download_block(h, dx, x, nrhs, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    for (int c = 0; c < nrhs; ++c) {
+      if (iters) iters[c] = run.iters[(size_t)c];
+      if (resid) resid[c] = run.resid[(size_t)c];
+      if (converged) converged[c] = run.state[(size_t)c] == kColConverged ? 1 : 0;
+    }
+    return Status();
+  };
+  return body().code;
+}
+
+SG_API int32_t saige_pcg_solve(saige_grm* h, const double* w, const double tau[2], const double* b,
+                               const double* x0, double* x, int64_t n, int32_t nrhs,
+                               const saige_pcg_options* opt, int32_t* iters, double* resid,
+                               uint8_t* converged) {
+  SG_GUARD_BEGIN
+  set_error("");
+  return pcg_entry(h, w, tau, b, x0, x, n, nrhs, opt, iters, resid, converged, true);
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_solve_mixed_model_pcg(saige_grm* h, const double tau[2], const double* w,
+                                           const double* b, double* x, int64_t n,
+                                           const saige_pcg_options* opt, int32_t* iters,
+                                           double* resid, uint8_t* converged) {
+  SG_GUARD_BEGIN
+  set_error("");
+  return pcg_entry(h, w, tau, b, nullptr, x, n, 1, opt, iters, resid, converged, false);
+  SG_GUARD_END
+}

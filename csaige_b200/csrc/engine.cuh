@@ -1,0 +1,88 @@
+// Internal engine of the fit-null library: the GRM handle, the GRM product
+// dispatch and the PCG driver shared by the C ABI and the AI-REML loop.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <vector>
+
+#include "common.cuh"
+#include "kernels_vec.cuh"
+
+namespace saige {
+
+// Growable device buffer.
+struct DevBuf {
+  void* ptr = nullptr;
+  size_t bytes = 0;
+  Status reserve(size_t want);
+  void release();
+  template <class T> T* as() const { return static_cast<T*>(ptr); }
+  ~DevBuf() { release(); }
+};
+
+struct TcPlan;  // tensor-core path state (kernels_tc.cu)
+
+}  // namespace saige
+
+struct saige_grm {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::recursive_mutex mu;
+  int64_t n = 0, n_pad = 0, wpr = 0;  // samples, padded samples, 32-bit words per row
+  int64_t m = 0, m_pad = 0;           // markers, padded markers
+  uint32_t* geno = nullptr;           // m_pad x wpr packed 2-bit codes
+  float4* zlut = nullptr;             // per marker: f32 z for codes 00,01,10,11
+  double* two_p = nullptr;            // per marker 2p (0 for padding)
+  double* inv_s = nullptr;            // per marker 1/sqrt(2p(1-p)) (0 when degenerate / padding)
+  // FP32 product workspace
+  saige::DevBuf v32, u32, ypart;
+  int n_splits = 1;
+  // tensor-core product state
+  saige::TcPlan* tc = nullptr;
+  // generic workspaces
+  saige::DevBuf ws_vec, ws_red, ws_cols, ws_io;
+  // statistics
+  int64_t n_kv = 0, n_kv_launches = 0;
+};
+
+namespace saige {
+
+// Kv for q columns of v (ld = h->n_pad, padding rows zero) into kp.
+// active (host, length q, may be NULL) selects columns; others are skipped.
+Status grm_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
+                   int precision, cudaStream_t st);
+
+struct PcgRun {
+  // inputs (device, ld = n_pad)
+  const double* b = nullptr;
+  const double* x0 = nullptr;
+  const double* wv = nullptr;  // wmax (fit-null form) or w (score-test form)
+  const double* d = nullptr;   // Jacobi diagonal
+  double tau0 = 1.0, tau1 = 0.0;
+  bool w_inverse = true;       // fit-null operator tau0 v/w + tau1 K v
+  int q = 1;
+  double tol = 1e-5;
+  int max_iter = 500;
+  int precision = SAIGE_PREC_FP32;
+  // outputs
+  double* x = nullptr;         // device n_pad x q
+  std::vector<int32_t> iters, state;
+  std::vector<double> resid;
+  int64_t total_iters = 0;
+};
+
+// Block PCG with per-column masks (decomposition.rs:212-298 per column).
+Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st);
+
+// Device scratch carved from the handle's workspaces.
+struct PcgScratch {
+  double *r, *z, *p, *ap, *kp;
+  double* partial;
+  double* small;  // >= 4*q
+  PcgCols cols;
+};
+Status pcg_scratch(saige_grm* h, int q, PcgScratch& s);
+
+}  // namespace saige

@@ -1,0 +1,128 @@
+// K1: gather the sample subset out of raw PLINK .bed rows, repack it into
+// 128-byte-aligned 2-bit rows, and count alleles and missing calls exactly.
+//
+// Replaces PlinkReader::read_marker_raw / read_marker (saige-geno/src/
+// plink.rs:182-194, 237-249) and MarkerData::compute_af's sums
+// (saige-geno/src/traits.rs:42-54): the counts are integers from popc over
+// the code bit planes, so af = alt / (2 n_valid) computed from them on the
+// host is bit-identical to the reference's f64 sum of 0/1/2 dosages.
+#include "common.cuh"
+#include "kernels.cuh"
+
+namespace saige {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int64_t kSmemRowMax = 200 * 1024;  // stage raw rows up to this size in shared memory
+
+// Counts over a word of 16 codes; valid = even bits of the real samples.
+__device__ __forceinline__ void count_word(uint32_t w, uint32_t valid, long long& alt,
+                                           long long& miss) {
+  const uint32_t lo = w & 0x55555555u;
+  const uint32_t hi = (w >> 1) & 0x55555555u;
+  const uint32_t hom_a1 = ~lo & ~hi & valid;  // 00 -> 2 copies of A1
+  const uint32_t het = ~lo & hi & valid;      // 10 -> 1 copy
+  const uint32_t mis = lo & ~hi & valid;      // 01 -> missing
+  alt += 2 * __popc(hom_a1) + __popc(het);
+  miss += __popc(mis);
+}
+
+__device__ __forceinline__ long long warp_sum_ll(long long v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+template <bool kIdentity>
+__global__ void __launch_bounds__(kThreads)
+    bed_gather_kernel(const uint8_t* __restrict__ bed, int64_t bpm,
+                      const int64_t* __restrict__ src_rows, const int32_t* __restrict__ sidx,
+                      int64_t n, uint32_t* __restrict__ out, int64_t wpr,
+                      int64_t* __restrict__ counts, int use_smem) {
+  extern __shared__ uint8_t row_s[];
+  __shared__ long long red[2][kThreads / 32];
+  const int64_t r = blockIdx.x;
+  const uint8_t* row = bed + 3 + src_rows[r] * bpm;
+  const uint8_t* src = row;
+  if (use_smem) {
+    for (int64_t b = threadIdx.x; b < bpm; b += blockDim.x) row_s[b] = row[b];
+    __syncthreads();
+    src = row_s;
+  }
+  long long alt = 0, miss = 0;
+  const int64_t n_words_real = (n + 15) / 16;
+  const int64_t n_words = out ? wpr : n_words_real;
+  for (int64_t j = threadIdx.x; j < n_words; j += blockDim.x) {
+    uint32_t w = 0x55555555u;  // padding: all codes 01 (missing -> z = 0)
+    if (j < n_words_real) {
+      const int64_t k0 = j * 16;
+      const int kn = (n - k0) < 16 ? (int)(n - k0) : 16;
+      uint32_t word = 0;
+      if (kIdentity) {
+        // bytes 4j .. 4j+3 of the raw row hold exactly these samples
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+          const int64_t bi = 4 * j + b;
+          const uint32_t byte = bi < bpm ? (uint32_t)src[bi] : 0u;
+          word |= byte << (8 * b);
+        }
+      } else {
+        for (int k = 0; k < kn; ++k) {
+          const int32_t s = sidx[k0 + k];
+          const uint32_t code = (src[s >> 2] >> ((s & 3) * 2)) & 3u;
+          word |= code << (2 * k);
+        }
+      }
+      const uint32_t keep = kn >= 16 ? 0xFFFFFFFFu : ((1u << (2 * kn)) - 1u);
+      count_word(word, keep & 0x55555555u, alt, miss);
+      w = (word & keep) | (0x55555555u & ~keep);
+    }
+    if (out) out[r * wpr + j] = w;
+  }
+  if (!counts) return;
+  alt = warp_sum_ll(alt);
+  miss = warp_sum_ll(miss);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) {
+    red[0][wid] = alt;
+    red[1][wid] = miss;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long a = 0, mm = 0;
+    for (int k = 0; k < kThreads / 32; ++k) {
+      a += red[0][k];
+      mm += red[1][k];
+    }
+    counts[2 * r] = a;
+    counts[2 * r + 1] = mm;
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_bed_gather(const uint8_t* bed, int64_t bpm, const int64_t* src_rows,
+                              int64_t n_rows, const int32_t* sample_idx, int64_t n,
+                              uint32_t* geno_out, int64_t words_per_row, int64_t* counts,
+                              cudaStream_t st) {
+  if (n_rows <= 0) return cudaSuccess;
+  const int use_smem = bpm <= kSmemRowMax ? 1 : 0;
+  const size_t smem = use_smem ? (size_t)round_up(bpm, 16) : 0;
+  if (sample_idx) {
+    auto k = bed_gather_kernel<false>;
+    if (smem > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e != cudaSuccess) return e;
+    }
+    k<<<(unsigned)n_rows, kThreads, smem, st>>>(bed, bpm, src_rows, sample_idx, n, geno_out,
+                                                words_per_row, counts, use_smem);
+  } else {
+    // identity subset: no staging needed, bytes are read in order
+    bed_gather_kernel<true><<<(unsigned)n_rows, kThreads, 0, st>>>(
+        bed, bpm, src_rows, nullptr, n, geno_out, words_per_row, counts, 0);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace saige

@@ -1,0 +1,260 @@
+/*
+ * saige_gpu.h — C ABI of the B200 (sm_100a) fit-null GRM-product library.
+ *
+ * The library replaces the saige-rs fit-null hot path: the on-the-fly GRM
+ * product K.v = Z (Z' v) / M computed straight from 2-bit PLINK genotypes,
+ * the PCG solves of the Sigma = tau0 W^-1 + tau1 K operator, and the AI-REML
+ * loop that drives them.  Every entry point below names the saige-rs
+ * interface it stands in for (paths relative to the frhl/CSAIGE tree).
+ *
+ * Conventions
+ *  - extern "C", plain pointers and sizes; no C++ exception crosses the ABI.
+ *  - Every function returns an int32_t status (SAIGE_OK = 0).  On failure a
+ *    message is available from saige_last_error() (thread-local).
+ *  - Host-buffer entry points copy in and out; *_dev entry points take device
+ *    pointers on the handle's device and run on the given stream (NULL = the
+ *    handle's own stream) and return after the work is complete.
+ *  - A handle owns its device memory and one CUDA stream.  Calls on one handle
+ *    are serialised by an internal mutex, so concurrent callers (the rayon
+ *    probe solves of ai_reml.rs:237-240) are safe.
+ *  - Matrices are column-major (DenseMatrix, saige-linalg/src/dense.rs:15-39);
+ *    a block of nrhs vectors of length n is n*nrhs doubles, vector-major.
+ *  - There is no CPU fallback: when no sm_100 device is usable, calls that
+ *    need one return SAIGE_ECUDA.
+ */
+#ifndef SAIGE_GPU_H
+#define SAIGE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  saige-rs reports dimension mismatches by panicking
+ * (assert_eq!, pcg.rs:129), PCG non-convergence as a flag, and Cholesky or
+ * bed-format failures as anyhow errors; here all are codes. */
+#define SAIGE_OK 0
+#define SAIGE_EINVAL 1        /* bad argument / dimension mismatch          */
+#define SAIGE_ENOMEM 2        /* device or host allocation failed           */
+#define SAIGE_ECUDA 3         /* CUDA error or no usable sm_100 device      */
+#define SAIGE_NOT_CONVERGED 4 /* iteration limit reached (results valid)    */
+#define SAIGE_TIMEOUT 5       /* a bounded device wait ran out              */
+#define SAIGE_SINGULAR 6      /* Cholesky / AI matrix failure               */
+#define SAIGE_EBED 7          /* malformed .bed (magic, mode or size)       */
+#define SAIGE_ENOTSUP 8       /* unsupported option                         */
+
+/* Arithmetic of the GRM product.
+ *  FP32:  the saige-rs arithmetic (pcg.rs:128-180): z = ((g-2p)/s) rounded to
+ *         f32, v rounded to f32, f32 products and sums (CUDA cores).
+ *  MIXED: v quantised per column to 24-bit fixed point, split into three
+ *         int8 limbs; genotypes 0/1/2 and the missing-call indicator are exact
+ *         int8 tensor-core operands (tcgen05.mma kind::i8, s32 accumulate),
+ *         standardisation and limb recombination in FP64. */
+#define SAIGE_PREC_FP32 0
+#define SAIGE_PREC_MIXED 1
+
+/* TraitType, saige-core/src/glmm/link.rs:7-12. */
+#define SAIGE_TRAIT_BINARY 0
+#define SAIGE_TRAIT_QUANTITATIVE 1
+#define SAIGE_TRAIT_SURVIVAL 2
+
+typedef struct saige_grm saige_grm;
+
+/* Last error message of the calling thread ("" when none). */
+const char* saige_last_error(void);
+
+/* ABI version: major*10000 + minor*100 + patch. */
+int32_t saige_version(void);
+
+/* Number of usable sm_100 devices (0 when none). */
+int32_t saige_device_count(void);
+
+/* ---------------------------------------------------------------------
+ * Genotype input
+ * ------------------------------------------------------------------- */
+
+/* Per-marker allele frequency, minor allele count and non-missing count
+ * over the sample subset, computed integer-exact on the GPU.
+ * Replaces the PlinkReader::read_marker + MarkerData::compute_af loop
+ * (saige-geno/src/plink.rs:237-267, saige-geno/src/traits.rs:42-54) with the
+ * bed checks of plink.rs:80-98.  bed is the whole .bed file in host memory
+ * (3-byte header included); sample_idx (length n, NULL = identity) holds
+ * .fam row indices in the order wanted (set_sample_subset, plink.rs:223-235).
+ * af/mac/n_valid have length m_tot and are bit-identical to compute_af. */
+int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                               const int64_t* sample_idx, int64_t n, double* af, double* mac,
+                               int64_t* n_valid);
+
+/* Marker QC and the variance-ratio / GRM marker split of fit-null
+ * (saige-cli/src/commands/fit_null.rs:209-259): keep af in
+ * [min_maf, 1-min_maf] and missing rate <= max_missing; draw 1000 indices
+ * with ChaCha8Rng::seed_from_u64(seed).gen_range(0..n_pass), sort, dedup,
+ * keep MAC >= 20 for the VR pool, the rest form the GRM.  grm_idx / vr_idx
+ * (capacity m_tot) receive original marker indices in increasing order.
+ * Returns SAIGE_EINVAL when no marker passes QC. */
+int32_t saige_select_grm_markers(const double* af, const double* mac, const int64_t* n_valid,
+                                 int64_t m_tot, int64_t n, double min_maf, double max_missing,
+                                 uint64_t seed, int64_t* grm_idx, int64_t* m_grm, int64_t* vr_idx,
+                                 int64_t* m_vr);
+
+/* ---------------------------------------------------------------------
+ * GRM operator (OnTheFlyGrm, saige-core/src/glmm/pcg.rs:91-180)
+ * ------------------------------------------------------------------- */
+
+/* OnTheFlyGrm::new (pcg.rs:101-122) from the packed bed: the markers
+ * marker_idx[0..m) (rows of the .bed) over the sample subset, with the allele
+ * frequencies the reference passes (grm_afs, fit_null.rs:257).  Genotypes
+ * stay 2-bit packed in HBM (gathered to the subset order, padded); no dense
+ * Z is materialised.  device < 0 selects the current device. */
+int32_t saige_grm_create_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                  int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                  const int64_t* marker_idx, int64_t m,
+                                  const double* allele_freqs, int32_t device, saige_grm** out);
+
+/* Same as saige_grm_create_from_bed, with the .bed already in device memory
+ * (bed_dev points at the 3-byte header). */
+int32_t saige_grm_create_from_bed_dev(const uint8_t* bed_dev, size_t bed_len, int64_t n_fam,
+                                      int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                      const int64_t* marker_idx, int64_t m,
+                                      const double* allele_freqs, int32_t device,
+                                      saige_grm** out);
+
+/* OnTheFlyGrm::new with the reference's own argument (pcg.rs:101): m dosage
+ * vectors of length n (marker-major, m*n doubles, NaN = missing) and their
+ * allele frequencies.  Dosages must be 0, 1, 2 or NaN (hard calls). */
+int32_t saige_grm_create_from_dosages(const double* dosages, int64_t n, int64_t m,
+                                      const double* allele_freqs, int32_t device,
+                                      saige_grm** out);
+
+int32_t saige_grm_destroy(saige_grm* h);
+
+/* n samples, m markers of the operator. */
+int32_t saige_grm_dims(const saige_grm* h, int64_t* n, int64_t* m);
+
+/* OnTheFlyGrm::mat_vec (pcg.rs:128-180) for nrhs vectors at once:
+ * out[:,r] = K v[:,r].  v and out are n*nrhs doubles (host memory). */
+int32_t saige_grm_matvec(saige_grm* h, const double* v, double* out, int64_t n, int32_t nrhs,
+                         int32_t precision);
+
+/* Device-pointer form of saige_grm_matvec. */
+int32_t saige_grm_matvec_dev(saige_grm* h, const double* v_dev, double* out_dev, int64_t n,
+                             int32_t nrhs, int32_t precision, void* stream);
+
+/* ---------------------------------------------------------------------
+ * PCG solves
+ * ------------------------------------------------------------------- */
+
+typedef struct {
+  double tol;        /* PcgSolver::tol (decomposition.rs:173-187), default 1e-5 */
+  int32_t max_iter;  /* PcgSolver::max_iter, default 500                        */
+  int32_t precision; /* SAIGE_PREC_*                                            */
+} saige_pcg_options;
+
+/* PcgSolver::solve (saige-linalg/src/decomposition.rs:212-298) on the
+ * fit-null operator Sigma v = tau0 v / max(w,1e-30) + tau1 K v with the
+ * Jacobi preconditioner 1/(tau0/max(w,1e-30) + tau1) (ai_reml.rs:142-164).
+ * nrhs > 1 runs one block PCG whose columns each follow the single-vector
+ * recurrence and stop on their own test ||r|| < tol*max(||b||,1).
+ * x0 (nullable) is the warm start; x receives the solutions; iters, resid
+ * and converged (each length nrhs, nullable) the per-column PcgResult.
+ * Returns SAIGE_OK even when a column did not converge (as the reference,
+ * which only sets converged = false). */
+int32_t saige_pcg_solve(saige_grm* h, const double* w, const double tau[2], const double* b,
+                        const double* x0, double* x, int64_t n, int32_t nrhs,
+                        const saige_pcg_options* opt, int32_t* iters, double* resid,
+                        uint8_t* converged);
+
+/* solve_mixed_model_pcg (saige-core/src/glmm/pcg.rs:37-78): the score-test
+ * convention Sigma v = tau0 w v + tau1 K v with preconditioner
+ * 1/(tau0 w + tau1) (unchanged when |diag| <= 1e-30), single vector. */
+int32_t saige_solve_mixed_model_pcg(saige_grm* h, const double tau[2], const double* w,
+                                    const double* b, double* x, int64_t n,
+                                    const saige_pcg_options* opt, int32_t* iters, double* resid,
+                                    uint8_t* converged);
+
+/* ---------------------------------------------------------------------
+ * AI-REML (fit_ai_reml, saige-core/src/glmm/ai_reml.rs:86-427)
+ * ------------------------------------------------------------------- */
+
+/* Solve strategies beyond the reference's (the reference is
+ * SAIGE_SOLVE_SINGLE with SAIGE_WARM_ZERO). */
+#define SAIGE_SOLVE_SINGLE 0 /* one PCG per right-hand side, as ai_reml.rs     */
+#define SAIGE_SOLVE_BLOCK 1  /* y, X columns and probes in one block PCG        */
+
+#define SAIGE_WARM_ZERO 0     /* x0 = 0 (the reference)                        */
+#define SAIGE_WARM_PREVIOUS 1 /* previous AI-REML iteration's solution         */
+#define SAIGE_WARM_LEARNED 2  /* MLP-predicted start, previous as fallback      */
+
+typedef struct {
+  int32_t max_iter;         /* AiRemlConfig::max_iter (ai_reml.rs:22-51), 30     */
+  double tol;               /* tau tolerance, 0.02 (fit-null CLI passes --tol)   */
+  double pcg_tol;           /* 1e-5                                              */
+  int32_t pcg_max_iter;     /* 500                                               */
+  int32_t n_random_vectors; /* 30                                                */
+  uint64_t seed;            /* 12345                                             */
+  int32_t precision;        /* SAIGE_PREC_*                                      */
+  int32_t solve;            /* SAIGE_SOLVE_*                                     */
+  int32_t warm_start;       /* SAIGE_WARM_*                                      */
+  int32_t reserved;
+} saige_ai_reml_config;
+
+typedef struct {
+  double tau[2];
+  int32_t iterations;
+  int32_t converged;
+  double log_likelihood;
+  int64_t n_kv;            /* GRM products (columns) performed               */
+  int64_t n_kv_launches;   /* GRM product launches (a block counts once)     */
+  int64_t pcg_iters;       /* sum over solves of PCG iterations              */
+  double seconds;          /* device wall time of the fit                    */
+} saige_ai_reml_summary;
+
+/* Fill cfg with AiRemlConfig::default() (ai_reml.rs:39-51) and the
+ * reference's solve strategy. */
+void saige_ai_reml_config_default(saige_ai_reml_config* cfg);
+
+/* fit_ai_reml: y (n), x (n x p column-major, intercept included), trait
+ * SAIGE_TRAIT_*.  alpha (p), mu/eta/w (n) and tau_trace (2*max_iter: tau
+ * after each iteration) are optional outputs.  Returns SAIGE_SINGULAR when
+ * the initial IRLS Cholesky fails (the reference's only error path);
+ * non-convergence is reported in out->converged. */
+int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x, int64_t n, int32_t p,
+                          int32_t trait, const saige_ai_reml_config* cfg,
+                          saige_ai_reml_summary* out, double* alpha, double* mu, double* eta,
+                          double* w, double* tau_trace);
+
+/* ---------------------------------------------------------------------
+ * Synthetic cohorts (seeded; no counterpart in the reference — test and
+ * benchmark input).  Deterministic functions of the spec: the host and the
+ * device generator produce identical bytes.
+ * ------------------------------------------------------------------- */
+typedef struct {
+  uint64_t seed;
+  int64_t n;            /* samples                                            */
+  int64_t m;            /* markers                                            */
+  double sib_frac;      /* fraction of samples in sibling pairs               */
+  double cousin_frac;   /* fraction of samples in first-cousin pairs          */
+  double missing_rate;  /* MCAR missing-call rate                             */
+  double maf_lo, maf_hi;/* allele frequency ~ U(maf_lo, maf_hi)               */
+  int32_t trait;        /* SAIGE_TRAIT_BINARY or SAIGE_TRAIT_QUANTITATIVE     */
+  int32_t n_covar;      /* covariates (intercept not counted)                 */
+  double prevalence;    /* binary: target case fraction                       */
+  double h2;            /* heritability of the polygenic score                */
+  int32_t n_causal;     /* causal markers for the polygenic score             */
+  int32_t reserved;
+} saige_cohort_spec;
+
+/* Writes the .bed bytes (3-byte header + m * ceil(n/4)) into bed_out, which
+ * is device memory when on_device != 0. */
+int32_t saige_gen_bed(const saige_cohort_spec* spec, uint8_t* bed_out, int32_t on_device);
+
+/* Phenotype y (n) and design x (n x (1+n_covar), column-major, column 0 the
+ * intercept). */
+int32_t saige_gen_pheno(const saige_cohort_spec* spec, double* y, double* x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SAIGE_GPU_H */

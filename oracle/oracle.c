@@ -1,0 +1,836 @@
+/*
+ * CPU oracle for the saige-rs fit-null GRM-product path — TEST INFRASTRUCTURE ONLY.
+ * See oracle.h for what pins it.  Built with -ffp-contract=off so that no
+ * multiply-add is fused, which is what rustc emits for the reference.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* ===================================================================== */
+/* PLINK .bed decode                                                      */
+/* ===================================================================== */
+
+/* saige-geno/src/plink.rs:170-179: 2-bit code, low bits first;
+ * 00 -> 2 (hom A1), 01 -> missing, 10 -> 1 (het), 11 -> 0 (hom A2). */
+double orc_decode_genotype(uint8_t byte, int offset) {
+  int bits = (byte >> (offset * 2)) & 3;
+  switch (bits) {
+    case 0: return 2.0;
+    case 1: return NAN;
+    case 2: return 1.0;
+    default: return 0.0;
+  }
+}
+
+/* plink.rs:182-194 (raw row) and :237-247 (sample-subset gather). */
+void orc_read_marker(const uint8_t* bed, int64_t bytes_per_marker, int64_t n_fam, int64_t marker,
+                     const int64_t* sample_idx, int64_t n, double* dosages_out) {
+  const uint8_t* row = bed + 3 + marker * bytes_per_marker;
+  for (int64_t k = 0; k < n; ++k) {
+    int64_t s = sample_idx ? sample_idx[k] : k;
+    (void)n_fam;
+    dosages_out[k] = orc_decode_genotype(row[s / 4], (int)(s % 4));
+  }
+}
+
+/* saige-geno/src/traits.rs:42-54. */
+void orc_compute_af(const double* dosages, int64_t n, double* af, double* mac, int64_t* n_valid) {
+  double sum = 0.0;
+  int64_t cnt = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    double d = dosages[i];
+    if (!isnan(d)) {
+      sum += d;
+      cnt += 1;
+    }
+  }
+  *af = cnt > 0 ? sum / (2.0 * (double)cnt) : 0.0;
+  double other = 2.0 * (double)cnt - sum;
+  *mac = sum < other ? sum : other;
+  *n_valid = cnt;
+}
+
+/* The read_marker + compute_af loop of fit_null.rs:209-211, with the bed
+ * size checks of plink.rs:80-98.  Returns 0, or -1 on a malformed bed. */
+int orc_marker_stats(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                     const int64_t* sample_idx, int64_t n, double* af, double* mac,
+                     int64_t* n_valid) {
+  if (bed_len < 3) return -1;
+  if (bed[0] != 0x6C || bed[1] != 0x1B) return -1;
+  if (bed[2] != 0x01) return -1;
+  int64_t bpm = (n_fam + 3) / 4;
+  if ((int64_t)bed_len < 3 + bpm * m_tot) return -1;
+  for (int64_t k = 0; k < n; ++k)
+    if (sample_idx && (sample_idx[k] < 0 || sample_idx[k] >= n_fam)) return -1;
+#pragma omp parallel
+  {
+    double* dos = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(static)
+    for (int64_t m = 0; m < m_tot; ++m) {
+      orc_read_marker(bed, bpm, n_fam, m, sample_idx, n, dos);
+      orc_compute_af(dos, n, &af[m], &mac[m], &n_valid[m]);
+    }
+    free(dos);
+  }
+  return 0;
+}
+
+/* ===================================================================== */
+/* ChaCha (Bernstein's published specification) + rand 0.8.5 mappings    */
+/* ===================================================================== */
+
+static inline uint32_t rotl32(uint32_t x, int k) { return (x << k) | (x >> (32 - k)); }
+
+#define QR(a, b, c, d)            \
+  do {                            \
+    a += b; d ^= a; d = rotl32(d, 16); \
+    c += d; b ^= c; b = rotl32(b, 12); \
+    a += b; d ^= a; d = rotl32(d, 8);  \
+    c += d; b ^= c; b = rotl32(b, 7);  \
+  } while (0)
+
+/* One 64-byte block: constants "expand 32-byte k", 8 key words, a 64-bit
+ * block counter in words 12-13 and a 64-bit stream id in words 14-15 (the
+ * layout rand_chacha uses).  rounds = 8 for ChaCha8, 20 for ChaCha20. */
+void orc_chacha_block(const uint32_t key[8], uint64_t counter, uint64_t stream, int rounds,
+                      uint32_t out[16]) {
+  uint32_t s[16];
+  s[0] = 0x61707865u; s[1] = 0x3320646eu; s[2] = 0x79622d32u; s[3] = 0x6b206574u;
+  for (int i = 0; i < 8; ++i) s[4 + i] = key[i];
+  s[12] = (uint32_t)counter; s[13] = (uint32_t)(counter >> 32);
+  s[14] = (uint32_t)stream;  s[15] = (uint32_t)(stream >> 32);
+  uint32_t x[16];
+  memcpy(x, s, sizeof x);
+  for (int r = 0; r < rounds; r += 2) {
+    QR(x[0], x[4], x[8], x[12]);
+    QR(x[1], x[5], x[9], x[13]);
+    QR(x[2], x[6], x[10], x[14]);
+    QR(x[3], x[7], x[11], x[15]);
+    QR(x[0], x[5], x[10], x[15]);
+    QR(x[1], x[6], x[11], x[12]);
+    QR(x[2], x[7], x[8], x[13]);
+    QR(x[3], x[4], x[9], x[14]);
+  }
+  for (int i = 0; i < 16; ++i) out[i] = x[i] + s[i];
+}
+
+void orc_chacha_from_seed(orc_chacha_rng* r, const uint8_t seed[32], int rounds) {
+  for (int i = 0; i < 8; ++i)
+    r->key[i] = (uint32_t)seed[4 * i] | ((uint32_t)seed[4 * i + 1] << 8) |
+                ((uint32_t)seed[4 * i + 2] << 16) | ((uint32_t)seed[4 * i + 3] << 24);
+  r->counter = 0;
+  r->stream = 0;
+  r->idx = 64;
+  r->rounds = rounds;
+}
+
+/* rand_core 0.6.4 SeedableRng::seed_from_u64: the 32-byte seed is filled
+ * with successive PCG32 (XSH-RR) outputs, little-endian. */
+void orc_chacha_seed_from_u64(orc_chacha_rng* r, uint64_t state, int rounds) {
+  const uint64_t MUL = 6364136223846793005ull;
+  const uint64_t INC = 11634580027462260723ull;
+  uint8_t seed[32];
+  for (int c = 0; c < 8; ++c) {
+    state = state * MUL + INC;
+    uint32_t xorshifted = (uint32_t)(((state >> 18) ^ state) >> 27);
+    uint32_t rot = (uint32_t)(state >> 59);
+    uint32_t x = (xorshifted >> rot) | (xorshifted << ((32 - rot) & 31));
+    seed[4 * c] = (uint8_t)x; seed[4 * c + 1] = (uint8_t)(x >> 8);
+    seed[4 * c + 2] = (uint8_t)(x >> 16); seed[4 * c + 3] = (uint8_t)(x >> 24);
+  }
+  orc_chacha_from_seed(r, seed, rounds);
+}
+
+static void orc_refill(orc_chacha_rng* r) {
+  for (int b = 0; b < 4; ++b) orc_chacha_block(r->key, r->counter + b, r->stream, r->rounds, r->buf + 16 * b);
+  r->counter += 4;
+  r->idx = 0;
+}
+
+/* rand_core BlockRng: a contiguous stream of u32 words. */
+uint32_t orc_rng_next_u32(orc_chacha_rng* r) {
+  if (r->idx >= 64) orc_refill(r);
+  return r->buf[r->idx++];
+}
+
+/* BlockRng::next_u64: two consecutive words, low word first (also across a
+ * buffer refill). */
+uint64_t orc_rng_next_u64(orc_chacha_rng* r) {
+  uint64_t lo = orc_rng_next_u32(r);
+  uint64_t hi = orc_rng_next_u32(r);
+  return (hi << 32) | lo;
+}
+
+/* rand 0.8.5 Standard for bool: the sign bit of one u32. */
+int orc_rng_gen_bool(orc_chacha_rng* r) { return (int32_t)orc_rng_next_u32(r) < 0; }
+
+/* rand 0.8.5 UniformInt<u64/usize>::sample_single(low, high): widening
+ * multiply with the "conservative zone" rejection test. */
+uint64_t orc_rng_gen_range_u64(orc_chacha_rng* r, uint64_t low, uint64_t high) {
+  uint64_t range = high - 1 - low + 1;
+  if (range == 0) return orc_rng_next_u64(r);
+  int lz = __builtin_clzll(range);
+  uint64_t zone = (range << lz) - 1;
+  for (;;) {
+    uint64_t v = orc_rng_next_u64(r);
+    unsigned __int128 prod = (unsigned __int128)v * (unsigned __int128)range;
+    uint64_t hi = (uint64_t)(prod >> 64);
+    uint64_t lo = (uint64_t)prod;
+    if (lo <= zone) return low + hi;
+  }
+}
+
+/* ai_reml.rs:121-130: n_vec Rademacher vectors from one ChaCha8 stream,
+ * vector-major.  out is n_vec x n. */
+void orc_rademacher_probes(uint64_t seed, int n_vec, int64_t n, double* out) {
+  orc_chacha_rng r;
+  orc_chacha_seed_from_u64(&r, seed, 8);
+  for (int k = 0; k < n_vec; ++k)
+    for (int64_t i = 0; i < n; ++i) out[(int64_t)k * n + i] = orc_rng_gen_bool(&r) ? 1.0 : -1.0;
+}
+
+/* ===================================================================== */
+/* QC + VR/GRM split (saige-cli/src/commands/fit_null.rs:209-259)          */
+/* ===================================================================== */
+
+static int cmp_u64(const void* a, const void* b) {
+  uint64_t x = *(const uint64_t*)a, y = *(const uint64_t*)b;
+  return x < y ? -1 : (x > y ? 1 : 0);
+}
+
+/* Returns 0, or -1 when no marker passes QC (the reference panics in
+ * gen_range(0..0)).  grm_idx / vr_idx receive original marker indices. */
+int orc_select_markers(const double* af, const double* mac, const int64_t* n_valid, int64_t m_tot,
+                       int64_t n, double min_maf, double max_missing, uint64_t seed,
+                       int64_t* grm_idx, int64_t* m_grm, int64_t* vr_idx, int64_t* m_vr,
+                       int64_t* n_pass_out) {
+  int64_t* pass = (int64_t*)malloc(sizeof(int64_t) * (size_t)(m_tot > 0 ? m_tot : 1));
+  int64_t n_pass = 0;
+  for (int64_t m = 0; m < m_tot; ++m) {
+    double missing_rate = 1.0 - ((double)n_valid[m] / (double)n);
+    if (af[m] >= min_maf && af[m] <= 1.0 - min_maf && missing_rate <= max_missing)
+      pass[n_pass++] = m;
+  }
+  *n_pass_out = n_pass;
+  if (n_pass == 0) {
+    free(pass);
+    *m_grm = 0;
+    *m_vr = 0;
+    return -1;
+  }
+  orc_chacha_rng r;
+  orc_chacha_seed_from_u64(&r, seed, 8);
+  uint64_t cand[1000];
+  for (int k = 0; k < 1000; ++k) cand[k] = orc_rng_gen_range_u64(&r, 0, (uint64_t)n_pass);
+  qsort(cand, 1000, sizeof(uint64_t), cmp_u64);
+  unsigned char* is_vr = (unsigned char*)calloc((size_t)n_pass, 1);
+  uint64_t prev = UINT64_MAX;
+  for (int k = 0; k < 1000; ++k) {
+    if (cand[k] == prev) continue;
+    prev = cand[k];
+    if (mac[pass[cand[k]]] >= 20.0) is_vr[cand[k]] = 1;
+  }
+  int64_t g = 0, v = 0;
+  for (int64_t i = 0; i < n_pass; ++i) {
+    if (is_vr[i]) vr_idx[v++] = pass[i];
+    else grm_idx[g++] = pass[i];
+  }
+  *m_grm = g;
+  *m_vr = v;
+  free(is_vr);
+  free(pass);
+  return 0;
+}
+
+/* ===================================================================== */
+/* On-the-fly GRM (saige-core/src/glmm/pcg.rs:91-180)                     */
+/* ===================================================================== */
+
+/* pcg.rs:101-122: z = (g - 2p)/sqrt(2p(1-p)) in f64, missing -> mean -> 0,
+ * a column of zeros when the denominator is <= 1e-10.  mode 1 rounds to
+ * f32 as the reference stores it.  z_out is m x n (marker-major). */
+void orc_grm_standardize(const double* dosages, const double* af, int64_t n, int64_t m, int mode,
+                         double* z_out) {
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < m; ++j) {
+    double denom = sqrt(2.0 * af[j] * (1.0 - af[j]));
+    double* zj = z_out + j * n;
+    if (denom > 1e-10) {
+      double mean = 2.0 * af[j];
+      for (int64_t i = 0; i < n; ++i) {
+        double g = dosages[j * n + i];
+        if (isnan(g)) g = mean;
+        double z = (g - mean) / denom;
+        zj[i] = mode == 1 ? (double)(float)z : z;
+      }
+    } else {
+      for (int64_t i = 0; i < n; ++i) zj[i] = 0.0;
+    }
+  }
+}
+
+/* pcg.rs:128-180.  mode 1 = the f32 arithmetic and the single-thread
+ * sequential order (one rayon chunk: fold over markers, then x(1/M) in f32). */
+void orc_grm_matvec(const double* z, int64_t n, int64_t m, const double* v, double* out, int mode) {
+  if (m == 0) {
+    for (int64_t i = 0; i < n; ++i) out[i] = 0.0;
+    return;
+  }
+  if (mode == 1) {
+    float* v32 = (float*)malloc(sizeof(float) * (size_t)n);
+    float* acc = (float*)calloc((size_t)n, sizeof(float));
+    float* z32 = (float*)malloc(sizeof(float) * (size_t)n);
+    for (int64_t i = 0; i < n; ++i) v32[i] = (float)v[i];
+    for (int64_t j = 0; j < m; ++j) {
+      for (int64_t i = 0; i < n; ++i) z32[i] = (float)z[j * n + i];
+      float dot = 0.0f;
+      for (int64_t i = 0; i < n; ++i) dot += z32[i] * v32[i];
+      for (int64_t i = 0; i < n; ++i) acc[i] += z32[i] * dot;
+    }
+    float scale = 1.0f / (float)m;
+    for (int64_t i = 0; i < n; ++i) out[i] = (double)(acc[i] * scale);
+    free(v32); free(acc); free(z32);
+    return;
+  }
+  double* dots = (double*)malloc(sizeof(double) * (size_t)m);
+#pragma omp parallel for schedule(static)
+  for (int64_t j = 0; j < m; ++j) {
+    const double* zj = z + j * n;
+    double d = 0.0;
+    for (int64_t i = 0; i < n; ++i) d += zj[i] * v[i];
+    dots[j] = d;
+  }
+  double scale = 1.0 / (double)m;
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    double a = 0.0;
+    for (int64_t j = 0; j < m; ++j) a += z[j * n + i] * dots[j];
+    out[i] = a * scale;
+  }
+  free(dots);
+}
+
+/* grm/dense.rs:115-186 semantics: K = Z'Z/M, n x n row-major, FP64. */
+void orc_grm_explicit(const double* z, int64_t n, int64_t m, double* k_out) {
+  double scale = m > 0 ? 1.0 / (double)m : 0.0;
+#pragma omp parallel for schedule(dynamic, 4)
+  for (int64_t a = 0; a < n; ++a) {
+    for (int64_t b = a; b < n; ++b) {
+      double s = 0.0;
+      for (int64_t j = 0; j < m; ++j) s += z[j * n + a] * z[j * n + b];
+      k_out[a * n + b] = s * scale;
+      k_out[b * n + a] = s * scale;
+    }
+  }
+}
+
+/* ===================================================================== */
+/* Dense linear algebra (saige-linalg/src/decomposition.rs)               */
+/* ===================================================================== */
+
+/* decomposition.rs:35-61; a and l are p x p row-major.  -1 = not PD. */
+int orc_cholesky(const double* a, int p, double* l) {
+  for (int i = 0; i < p * p; ++i) l[i] = 0.0;
+  for (int j = 0; j < p; ++j) {
+    double sum = 0.0;
+    for (int k = 0; k < j; ++k) sum += l[j * p + k] * l[j * p + k];
+    double diag = a[j * p + j] - sum;
+    if (diag <= 0.0) return -1;
+    l[j * p + j] = sqrt(diag);
+    for (int i = j + 1; i < p; ++i) {
+      double s = 0.0;
+      for (int k = 0; k < j; ++k) s += l[i * p + k] * l[j * p + k];
+      l[i * p + j] = (a[i * p + j] - s) / l[j * p + j];
+    }
+  }
+  return 0;
+}
+
+/* decomposition.rs:64-89. */
+void orc_chol_solve(const double* l, int p, const double* b, double* x) {
+  double y[64];
+  for (int i = 0; i < p; ++i) {
+    double s = 0.0;
+    for (int j = 0; j < i; ++j) s += l[i * p + j] * y[j];
+    y[i] = (b[i] - s) / l[i * p + i];
+  }
+  for (int i = p - 1; i >= 0; --i) {
+    double s = 0.0;
+    for (int j = i + 1; j < p; ++j) s += l[j * p + i] * x[j];
+    x[i] = (y[i] - s) / l[i * p + i];
+  }
+}
+
+typedef void (*orc_op_fn)(void* ctx, const double* v, double* out);
+
+/* decomposition.rs:212-298, verbatim control flow: x0 (or 0), r = b - A x,
+ * tol_abs = tol * max(||b||, 1), test ||r|| before each product, give up
+ * when |p'Ap| < 1e-30.  Returns 1 when converged. */
+static int orc_pcg_core(orc_op_fn op, void* op_ctx, orc_op_fn pre, void* pre_ctx, int64_t n,
+                        const double* b, const double* x0, double tol, int max_iter, double* x,
+                        int* iters, double* resid) {
+  double* r = (double*)malloc(sizeof(double) * (size_t)n);
+  double* z = (double*)malloc(sizeof(double) * (size_t)n);
+  double* p = (double*)malloc(sizeof(double) * (size_t)n);
+  double* ap = (double*)malloc(sizeof(double) * (size_t)n);
+  for (int64_t i = 0; i < n; ++i) x[i] = x0 ? x0[i] : 0.0;
+  op(op_ctx, x, ap);
+  for (int64_t i = 0; i < n; ++i) r[i] = b[i] - ap[i];
+  pre(pre_ctx, r, z);
+  for (int64_t i = 0; i < n; ++i) p[i] = z[i];
+  double rz = 0.0;
+  for (int64_t i = 0; i < n; ++i) rz += r[i] * z[i];
+  double bn = 0.0;
+  for (int64_t i = 0; i < n; ++i) bn += b[i] * b[i];
+  bn = sqrt(bn);
+  double tol_abs = tol * (bn > 1.0 ? bn : 1.0);
+  int conv = 0;
+  int it;
+  double rn = 0.0;
+  for (it = 0; it < max_iter; ++it) {
+    rn = 0.0;
+    for (int64_t i = 0; i < n; ++i) rn += r[i] * r[i];
+    rn = sqrt(rn);
+    if (rn < tol_abs) { conv = 1; break; }
+    op(op_ctx, p, ap);
+    double pap = 0.0;
+    for (int64_t i = 0; i < n; ++i) pap += p[i] * ap[i];
+    if (fabs(pap) < 1e-30) { conv = 0; goto done; }
+    double alpha = rz / pap;
+    for (int64_t i = 0; i < n; ++i) x[i] += alpha * p[i];
+    for (int64_t i = 0; i < n; ++i) r[i] -= alpha * ap[i];
+    pre(pre_ctx, r, z);
+    double rz_new = 0.0;
+    for (int64_t i = 0; i < n; ++i) rz_new += r[i] * z[i];
+    double beta = rz_new / rz;
+    rz = rz_new;
+    for (int64_t i = 0; i < n; ++i) p[i] = z[i] + beta * p[i];
+  }
+  if (!conv) {
+    rn = 0.0;
+    for (int64_t i = 0; i < n; ++i) rn += r[i] * r[i];
+    rn = sqrt(rn);
+    conv = rn < tol_abs;
+    it = max_iter;
+  }
+done:
+  *iters = it;
+  *resid = rn;
+  free(r); free(z); free(p); free(ap);
+  return conv;
+}
+
+typedef struct { const double* a; int n; } dense_ctx;
+static void dense_op(void* c, const double* v, double* out) {
+  dense_ctx* d = (dense_ctx*)c;
+  for (int i = 0; i < d->n; ++i) out[i] = 0.0;
+  /* DenseMatrix::mat_vec (dense.rs:102-113): column sweep */
+  for (int j = 0; j < d->n; ++j)
+    for (int i = 0; i < d->n; ++i) out[i] += d->a[i * d->n + j] * v[j];
+}
+static void dense_diag_pre(void* c, const double* v, double* out) {
+  dense_ctx* d = (dense_ctx*)c;
+  for (int i = 0; i < d->n; ++i) {
+    double di = d->a[i * d->n + i];
+    out[i] = fabs(di) > 1e-30 ? v[i] / di : v[i];
+  }
+}
+
+/* decomposition.rs:301-315 (solve_dense: Jacobi on diag(A)).  Returns 1 when
+ * converged; a is n x n row-major. */
+int orc_pcg_dense(const double* a, int n, const double* b, double tol, int max_iter, double* x,
+                  int* iters, double* resid) {
+  dense_ctx c = {a, n};
+  return orc_pcg_core(dense_op, &c, dense_diag_pre, &c, n, b, NULL, tol, max_iter, x, iters, resid);
+}
+
+/* ===================================================================== */
+/* Link and family (saige-core/src/glmm/link.rs:29-100, family.rs:23-90)  */
+/* ===================================================================== */
+
+double orc_link(int t, double mu) {
+  if (t == ORC_BINARY) return log(mu / (1.0 - mu));
+  if (t == ORC_QUANTITATIVE) return mu;
+  return log(-log(1.0 - mu));
+}
+double orc_inv_link(int t, double eta) {
+  if (t == ORC_BINARY) return 1.0 / (1.0 + exp(-eta));
+  if (t == ORC_QUANTITATIVE) return eta;
+  return 1.0 - exp(-exp(eta));
+}
+/* family.rs:82-90: clamp to [1e-10, 1-1e-10] for binary/survival. */
+double orc_update_mu(int t, double eta) {
+  double mu = orc_inv_link(t, eta);
+  if (t == ORC_QUANTITATIVE) return mu;
+  if (mu < 1e-10) mu = 1e-10;
+  if (mu > 1.0 - 1e-10) mu = 1.0 - 1e-10;
+  return mu;
+}
+/* family.rs:55-66 with link.rs variance(). */
+double orc_working_weight(int t, double mu) {
+  double v = t == ORC_QUANTITATIVE ? 1.0 : mu * (1.0 - mu);
+  return v > 1e-30 ? v : 1e-30;
+}
+/* family.rs:23-40. */
+double orc_initialize_mu(int t, double y) {
+  if (t == ORC_BINARY) return (y + 0.5) / 2.0;
+  if (t == ORC_QUANTITATIVE) return y;
+  double m = (y + 0.5) / 2.0;
+  if (m < 0.01) m = 0.01;
+  if (m > 0.99) m = 0.99;
+  return m;
+}
+
+/* ===================================================================== */
+/* GLM IRLS (ai_reml.rs:431-482)                                          */
+/* ===================================================================== */
+
+/* x is n x p column-major (DenseMatrix::from_col_major). */
+int orc_fit_glm_irls(const double* y, const double* x, int64_t n, int p, int t, int max_iter,
+                     double* alpha) {
+  double* mu = (double*)malloc(sizeof(double) * (size_t)n);
+  double* eta = (double*)malloc(sizeof(double) * (size_t)n);
+  double* w = (double*)malloc(sizeof(double) * (size_t)n);
+  double* zz = (double*)malloc(sizeof(double) * (size_t)n);
+  double xtwx[64 * 64], l[64 * 64], xtwz[64], anew[64];
+  int rc = 0;
+  for (int64_t i = 0; i < n; ++i) {
+    mu[i] = orc_initialize_mu(t, y[i]);
+    eta[i] = orc_link(t, mu[i]);
+  }
+  for (int j = 0; j < p; ++j) alpha[j] = 0.0;
+  for (int it = 0; it < max_iter; ++it) {
+    for (int64_t i = 0; i < n; ++i) {
+      w[i] = orc_working_weight(t, mu[i]);
+      double wm = w[i] > 1e-30 ? w[i] : 1e-30;
+      zz[i] = eta[i] + (y[i] - mu[i]) / wm;
+    }
+    /* dense.rs:227-263 */
+    for (int j = 0; j < p; ++j)
+      for (int k = j; k < p; ++k) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += x[j * n + i] * w[i] * x[k * n + i];
+        xtwx[j * p + k] = s;
+        xtwx[k * p + j] = s;
+      }
+    for (int j = 0; j < p; ++j) {
+      double s = 0.0;
+      for (int64_t i = 0; i < n; ++i) s += x[j * n + i] * w[i] * zz[i];
+      xtwz[j] = s;
+    }
+    if (orc_cholesky(xtwx, p, l) != 0) {
+      for (int i = 0; i < p; ++i) xtwx[i * p + i] += 1e-6;
+      if (orc_cholesky(xtwx, p, l) != 0) { rc = -1; break; }
+    }
+    orc_chol_solve(l, p, xtwz, anew);
+    /* DenseMatrix::mat_vec: column sweep */
+    for (int64_t i = 0; i < n; ++i) eta[i] = 0.0;
+    for (int j = 0; j < p; ++j)
+      for (int64_t i = 0; i < n; ++i) eta[i] += x[j * n + i] * anew[j];
+    for (int64_t i = 0; i < n; ++i) mu[i] = orc_update_mu(t, eta[i]);
+    double change = 0.0;
+    for (int j = 0; j < p; ++j) change += fabs(anew[j] - alpha[j]);
+    for (int j = 0; j < p; ++j) alpha[j] = anew[j];
+    if (change < 1e-8) break;
+  }
+  free(mu); free(eta); free(w); free(zz);
+  return rc;
+}
+
+/* ===================================================================== */
+/* AI-REML (ai_reml.rs:86-427)                                            */
+/* ===================================================================== */
+
+typedef struct {
+  int kind;
+  const double* grm;
+  int64_t n, m;
+  int kmode;
+  int64_t n_kv;
+} grm_ctx;
+
+static void grm_apply(grm_ctx* g, const double* v, double* out) {
+  g->n_kv += 1;
+  if (g->kind == ORC_K_IDENTITY) {
+    for (int64_t i = 0; i < g->n; ++i) out[i] = v[i];
+  } else if (g->kind == ORC_K_OTF) {
+    orc_grm_matvec(g->grm, g->n, g->m, v, out, g->kmode);
+  } else {
+    int64_t n = g->n;
+#pragma omp parallel for schedule(static)
+    for (int64_t a = 0; a < n; ++a) {
+      double s = 0.0;
+      const double* row = g->grm + a * n;
+      for (int64_t b = 0; b < n; ++b) s += row[b] * v[b];
+      out[a] = s;
+    }
+  }
+}
+
+typedef struct {
+  grm_ctx* g;
+  const double* w;
+  double tau0, tau1;
+  double* tmp;
+} sigma_ctx;
+
+/* ai_reml.rs:142-149 */
+static void sigma_op(void* c, const double* v, double* out) {
+  sigma_ctx* s = (sigma_ctx*)c;
+  grm_apply(s->g, v, s->tmp);
+  for (int64_t i = 0; i < s->g->n; ++i) {
+    double wi = s->w[i] > 1e-30 ? s->w[i] : 1e-30;
+    out[i] = s->tau0 * v[i] / wi + s->tau1 * s->tmp[i];
+  }
+}
+/* ai_reml.rs:152-164 */
+static void sigma_pre(void* c, const double* v, double* out) {
+  sigma_ctx* s = (sigma_ctx*)c;
+  for (int64_t i = 0; i < s->g->n; ++i) {
+    double wi = s->w[i] > 1e-30 ? s->w[i] : 1e-30;
+    double diag = s->tau0 / wi + s->tau1;
+    out[i] = fabs(diag) > 1e-30 ? v[i] / diag : v[i];
+  }
+}
+
+int orc_pcg_sigma(const double* y_unused, int kind, const double* grm, int64_t n, int64_t m,
+                  int kmode, const double* w, const double tau[2], const double* b,
+                  const double* x0, double tol, int max_iter, double* x, int* iters,
+                  double* resid, int* converged) {
+  (void)y_unused;
+  grm_ctx g = {kind, grm, n, m, kmode, 0};
+  double* tmp = (double*)malloc(sizeof(double) * (size_t)n);
+  sigma_ctx s = {&g, w, tau[0], tau[1], tmp};
+  *converged = orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, b, x0, tol, max_iter, x, iters, resid);
+  free(tmp);
+  return 0;
+}
+
+static double dotv(const double* a, const double* b, int64_t n) {
+  double s = 0.0;
+  for (int64_t i = 0; i < n; ++i) s += a[i] * b[i];
+  return s;
+}
+
+/* P-projection of a Sigma^-1 solve (ai_reml.rs:242-251):
+ * pu = sinv_u - SinvX C^-1 (SinvX' u). */
+static void p_project(double* pu, const double* u, const double* sinvx, const double* l, int p,
+                      int64_t n) {
+  double t[64], corr[64];
+  for (int j = 0; j < p; ++j) t[j] = dotv(sinvx + (int64_t)j * n, u, n);
+  orc_chol_solve(l, p, t, corr);
+  for (int j = 0; j < p; ++j)
+    for (int64_t i = 0; i < n; ++i) pu[i] -= sinvx[(int64_t)j * n + i] * corr[j];
+}
+
+int orc_fit_ai_reml(const double* y, const double* x, int64_t n, int p, int t, int kind,
+                    const double* grm, int64_t m, int kmode, const orc_ai_reml_config* cfg,
+                    orc_ai_reml_summary* out, double* tau_trace, double* alpha_out,
+                    double* mu_out, double* eta_out, double* w_out) {
+  if (p > 64) return -2;
+  int fix_tau_e = (t == ORC_BINARY || t == ORC_SURVIVAL);
+  double tau[2] = {1.0, 0.0};
+  double alpha[64];
+  if (orc_fit_glm_irls(y, x, n, p, t, 25, alpha) != 0) return -1;
+
+  size_t nb = sizeof(double) * (size_t)n;
+  double* eta = (double*)malloc(nb);
+  double* mu = (double*)malloc(nb);
+  double* w = (double*)malloc(nb);
+  double* ytil = (double*)malloc(nb);
+  double* sinvy = (double*)malloc(nb);
+  double* sinvx = (double*)malloc(nb * (size_t)p);
+  double* xcol = (double*)malloc(nb);
+  double* py = (double*)malloc(nb);
+  double* kpy = (double*)malloc(nb);
+  double* su = (double*)malloc(nb);
+  double* ku = (double*)malloc(nb);
+  double* pk = (double*)malloc(nb);
+  double* invw_py = (double*)malloc(nb);
+  double* tmp = (double*)malloc(nb);
+  int nrv = cfg->n_random_vectors;
+  double* probes = (double*)malloc(nb * (size_t)(nrv > 0 ? nrv : 1));
+  orc_rademacher_probes(cfg->seed, nrv, n, probes);
+
+  for (int64_t i = 0; i < n; ++i) {
+    double e = 0.0;
+    for (int j = 0; j < p; ++j) e += x[(int64_t)j * n + i] * alpha[j];
+    eta[i] = e;
+    mu[i] = orc_update_mu(t, e);
+  }
+
+  grm_ctx g = {kind, grm, n, m, kmode, 0};
+  int64_t pcg_total = 0;
+  int converged = 0, n_iter = 0;
+  double l[64 * 64], c[64 * 64];
+
+  for (int iter = 0; iter < cfg->max_iter; ++iter) {
+    n_iter = iter + 1;
+    for (int64_t i = 0; i < n; ++i) w[i] = orc_working_weight(t, mu[i]);
+    sigma_ctx s = {&g, w, tau[0], tau[1], tmp};
+    for (int64_t i = 0; i < n; ++i) {
+      double wi = w[i] > 1e-30 ? w[i] : 1e-30;
+      ytil[i] = eta[i] + (y[i] - mu[i]) / wi;
+    }
+    int it;
+    double rs;
+    orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, ytil, NULL, cfg->pcg_tol, cfg->pcg_max_iter,
+                 sinvy, &it, &rs);
+    pcg_total += it;
+    for (int j = 0; j < p; ++j) {
+      for (int64_t i = 0; i < n; ++i) xcol[i] = x[(int64_t)j * n + i];
+      orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, xcol, NULL, cfg->pcg_tol, cfg->pcg_max_iter,
+                   sinvx + (int64_t)j * n, &it, &rs);
+      pcg_total += it;
+    }
+    /* ai_reml.rs:189-200: C[j,k] = X[:,k] . SinvX[:,j] */
+    for (int j = 0; j < p; ++j)
+      for (int k = j; k < p; ++k) {
+        double d = dotv(x + (int64_t)k * n, sinvx + (int64_t)j * n, n);
+        c[j * p + k] = d;
+        c[k * p + j] = d;
+      }
+    double xsy[64];
+    for (int j = 0; j < p; ++j) xsy[j] = dotv(x + (int64_t)j * n, sinvy, n);
+    if (orc_cholesky(c, p, l) != 0) break;
+    orc_chol_solve(l, p, xsy, alpha);
+    for (int64_t i = 0; i < n; ++i) {
+      double e = 0.0;
+      for (int j = 0; j < p; ++j) e += x[(int64_t)j * n + i] * alpha[j];
+      eta[i] = e;
+      mu[i] = orc_update_mu(t, e);
+    }
+    /* ai_reml.rs:221-232 */
+    for (int64_t i = 0; i < n; ++i) py[i] = sinvy[i];
+    for (int j = 0; j < p; ++j)
+      for (int64_t i = 0; i < n; ++i) py[i] -= sinvx[(int64_t)j * n + i] * alpha[j];
+    grm_apply(&g, py, kpy);
+    double ypapy = dotv(py, kpy, n);
+    /* ai_reml.rs:237-258: Hutchinson trace of P K */
+    double trace_sum = 0.0;
+    for (int k = 0; k < nrv; ++k) {
+      const double* u = probes + (int64_t)k * n;
+      orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, u, NULL, cfg->pcg_tol, cfg->pcg_max_iter, su,
+                   &it, &rs);
+      pcg_total += it;
+      p_project(su, u, sinvx, l, p, n);
+      grm_apply(&g, u, ku);
+      trace_sum += dotv(ku, su, n);
+    }
+    double trace_grm = trace_sum / (double)nrv;
+    double score_g = ypapy - trace_grm;
+    /* ai_reml.rs:263-273 */
+    orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, kpy, NULL, cfg->pcg_tol, cfg->pcg_max_iter, pk,
+                 &it, &rs);
+    pcg_total += it;
+    p_project(pk, kpy, sinvx, l, p, n);
+    double ai_11 = dotv(kpy, pk, n);
+    double score_e = 0.0, ai_00 = 0.0, ai_01 = 0.0;
+    if (!fix_tau_e) {
+      /* ai_reml.rs:281-317 */
+      double tw = 0.0;
+      for (int k = 0; k < nrv; ++k) {
+        const double* u = probes + (int64_t)k * n;
+        orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, u, NULL, cfg->pcg_tol, cfg->pcg_max_iter, su,
+                     &it, &rs);
+        pcg_total += it;
+        p_project(su, u, sinvx, l, p, n);
+        double d = 0.0;
+        for (int64_t i = 0; i < n; ++i) {
+          double wi = w[i] > 1e-30 ? w[i] : 1e-30;
+          d += (u[i] / wi) * su[i];
+        }
+        tw += d;
+      }
+      double trace_w = tw / (double)nrv;
+      for (int64_t i = 0; i < n; ++i) {
+        double wi = w[i] > 1e-30 ? w[i] : 1e-30;
+        invw_py[i] = py[i] / wi;
+      }
+      double ypa0py = dotv(py, invw_py, n);
+      score_e = ypa0py - trace_w;
+      orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, invw_py, NULL, cfg->pcg_tol,
+                   cfg->pcg_max_iter, su, &it, &rs);
+      pcg_total += it;
+      p_project(su, invw_py, sinvx, l, p, n);
+      ai_00 = dotv(invw_py, su, n);
+      ai_01 = dotv(invw_py, pk, n);
+    }
+    double tau_new[2], max_change;
+    if (fix_tau_e) {
+      if (fabs(ai_11) < 1e-30) break;
+      double d1 = score_g / ai_11;
+      double step = 1.0;
+      double tg = tau[1] + step * d1;
+      while (tg < 0.0 && step > 1e-10) {
+        step *= 0.5;
+        tg = tau[1] + step * d1;
+      }
+      if (tg < 1e-10) tg = 1e-10;
+      max_change = fabs(tg - tau[1]) / (fabs(tg) + fabs(tau[1]) + cfg->tol);
+      tau_new[0] = 1.0;
+      tau_new[1] = tg;
+    } else {
+      double det = ai_00 * ai_11 - ai_01 * ai_01;
+      if (fabs(det) < 1e-30) break;
+      double d0 = (ai_11 * score_e - ai_01 * score_g) / det;
+      double d1 = (-ai_01 * score_e + ai_00 * score_g) / det;
+      double step = 1.0;
+      double t0 = tau[0] + step * d0, t1 = tau[1] + step * d1;
+      while ((t0 < 0.0 || t1 < 0.0) && step > 1e-10) {
+        step *= 0.5;
+        t0 = tau[0] + step * d0;
+        t1 = tau[1] + step * d1;
+      }
+      tau_new[0] = t0 > 1e-10 ? t0 : 1e-10;
+      tau_new[1] = t1 > 1e-10 ? t1 : 1e-10;
+      double c0 = fabs(tau_new[0] - tau[0]) / (fabs(tau_new[0]) + fabs(tau[0]) + cfg->tol);
+      double c1 = fabs(tau_new[1] - tau[1]) / (fabs(tau_new[1]) + fabs(tau[1]) + cfg->tol);
+      max_change = c0 > c1 ? c0 : c1;
+    }
+    tau[0] = tau_new[0];
+    tau[1] = tau_new[1];
+    if (tau_trace) {
+      tau_trace[2 * iter] = tau[0];
+      tau_trace[2 * iter + 1] = tau[1];
+    }
+    if (max_change < cfg->tol) {
+      converged = 1;
+      break;
+    }
+  }
+  for (int64_t i = 0; i < n; ++i) w[i] = orc_working_weight(t, mu[i]);
+  double ll = 0.0;
+  if (t == ORC_QUANTITATIVE) {
+    double ss = 0.0;
+    for (int64_t i = 0; i < n; ++i) ss += (y[i] - mu[i]) * (y[i] - mu[i]);
+    ll = -0.5 * (double)n * log(2.0 * M_PI * tau[0]) - 0.5 * ss / tau[0];
+  } else {
+    for (int64_t i = 0; i < n; ++i) {
+      double mi = mu[i];
+      if (mi < 1e-15) mi = 1e-15;
+      if (mi > 1.0 - 1e-15) mi = 1.0 - 1e-15;
+      ll += y[i] * log(mi) + (1.0 - y[i]) * log(1.0 - mi);
+    }
+  }
+  out->tau[0] = tau[0];
+  out->tau[1] = tau[1];
+  out->iterations = n_iter;
+  out->converged = converged;
+  out->log_likelihood = ll;
+  out->n_kv = g.n_kv;
+  out->pcg_iters = pcg_total;
+  if (alpha_out) for (int j = 0; j < p; ++j) alpha_out[j] = alpha[j];
+  if (mu_out) memcpy(mu_out, mu, nb);
+  if (eta_out) memcpy(eta_out, eta, nb);
+  if (w_out) memcpy(w_out, w, nb);
+  free(eta); free(mu); free(w); free(ytil); free(sinvy); free(sinvx); free(xcol); free(py);
+  free(kpy); free(su); free(ku); free(pk); free(invw_py); free(tmp); free(probes);
+  return 0;
+}
