@@ -4,6 +4,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <cstdlib>
 #include <vector>
 
 #include "engine.cuh"
@@ -159,23 +160,35 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   f.q = 1 + p + f.nrv;
   f.cfg = cfg;
   const int64_t ld = f.ld;
-  const size_t nvec = 8 + 2 * (size_t)f.q + 3 * (size_t)f.nrv + 7;
+  // column layout of the fit workspace (each column is ld doubles)
+  const size_t q = (size_t)f.q, nrv = (size_t)f.nrv, pp = (size_t)p;
+  const size_t cols[] = {1, pp, 1, 1, 1, 1, 1, 1,  // y, x, eta, mu, w, wmax, d, ytil
+                         q, q,                     // rhs, sol
+                         nrv, nrv, nrv,            // ku, pu, tmpq
+                         1, 1, 1, 1, 1, 1, 1};     // py, kpy, pk, invw_py, pw, pk_raw, pw_raw
+  size_t nvec = 0;
+  for (size_t c : cols) nvec += c;
   const size_t small = (size_t)(p * f.q + p * p + 4 * f.q + 64) * 8;
   const size_t part = (size_t)red_blocks(n) * (size_t)std::max(p * f.q, 3 * f.q) * 8;
   SG_TRY(f.mem.reserve(nvec * ld * 8 + small + part));
   double* base = f.mem.as<double>();
+  double* const vec_end = base + nvec * ld;
   SG_CUDA(cudaMemsetAsync(base, 0, nvec * ld * 8, f.st));
-  auto take = [&](size_t cols) {
+  size_t ci = 0;
+  auto take = [&](size_t ncol) {
+    if (ci >= sizeof(cols) / sizeof(cols[0]) || cols[ci] != ncol) std::abort();
+    ++ci;
     double* r = base;
-    base += cols * ld;
+    base += ncol * ld;
     return r;
   };
-  f.y = take(1); f.x = take((size_t)p); f.eta = take(1); f.mu = take(1); f.w = take(1);
+  f.y = take(1); f.x = take(pp); f.eta = take(1); f.mu = take(1); f.w = take(1);
   f.wmax = take(1); f.d = take(1); f.ytil = take(1);
-  f.rhs = take((size_t)f.q); f.sol = take((size_t)f.q);
-  f.ku = take((size_t)f.nrv); f.pu = take((size_t)f.nrv); f.tmpq = take((size_t)f.nrv);
+  f.rhs = take(q); f.sol = take(q);
+  f.ku = take(nrv); f.pu = take(nrv); f.tmpq = take(nrv);
   f.py = take(1); f.kpy = take(1); f.pk = take(1); f.invw_py = take(1); f.pw = take(1);
   f.pk_raw = take(1); f.pw_raw = take(1);
+  if (base != vec_end || ci != sizeof(cols) / sizeof(cols[0])) std::abort();
   f.dsmall = base;
   f.partial = base + small / 8;
 
