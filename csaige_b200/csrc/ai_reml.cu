@@ -98,6 +98,7 @@ Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const 
   run.max_iter = f.cfg->pcg_max_iter;
   run.precision = f.cfg->precision;
   run.x = x;
+  run.force_step = x0 != nullptr;
   SG_TRY(pcg_run(f.h, run, f.st));
   f.pcg_iters += run.total_iters;
   return Status();

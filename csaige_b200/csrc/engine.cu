@@ -299,8 +299,8 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
                           s.partial, st));
     ax0 = s.ap;
   }
-  SG_CUDA(pcg_start(run.b, run.x0, ax0, run.d, run.x, s.r, s.z, s.p, n, ld, q, run.tol, s.cols,
-                    s.partial, s.small, st));
+  SG_CUDA(pcg_start(run.b, run.x0, ax0, run.d, run.x, s.r, s.z, s.p, n, ld, q, run.tol,
+                    run.force_step && run.x0 != nullptr, s.cols, s.partial, s.small, st));
   if (run.max_iter <= 0) {
     // the loop body never runs; converged is the initial test
     SG_CUDA(cudaMemcpyAsync(state.data(), s.cols.state, (size_t)q * 4, cudaMemcpyDeviceToHost, st));

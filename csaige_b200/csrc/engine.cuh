@@ -66,6 +66,7 @@ struct PcgRun {
   double tol = 1e-5;
   int max_iter = 500;
   int precision = SAIGE_PREC_FP32;
+  bool force_step = false;     // warm starts: at least one CG step per column
   // outputs
   double* x = nullptr;         // device n_pad x q
   std::vector<int32_t> iters, state;

@@ -116,7 +116,8 @@ __global__ void pcg_start_kernel(const double* __restrict__ b, const double* __r
   }
 }
 
-__global__ void pcg_start_finish(const double* __restrict__ sums, int q, double tol, PcgCols cols) {
+__global__ void pcg_start_finish(const double* __restrict__ sums, int q, double tol, int force_step,
+                                 PcgCols cols) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= q) return;
   const double rz = sums[c], rr = sums[q + c], bb = sums[2 * q + c];
@@ -126,7 +127,9 @@ __global__ void pcg_start_finish(const double* __restrict__ sums, int q, double 
   cols.rr[c] = rr;
   cols.tol_abs[c] = tol_abs;
   cols.iters[c] = 0;
-  cols.state[c] = sqrt(rr) < tol_abs ? kColConverged : kColActive;
+  // a warm-started column takes at least one CG step (force_step), so a start
+  // that already meets the tolerance is still refined against the current operator
+  cols.state[c] = (!force_step && sqrt(rr) < tol_abs) ? kColConverged : kColActive;
 }
 
 template <bool kWInverse>
@@ -375,12 +378,13 @@ cudaError_t cross_dots(const double* a, int p, const double* b, int q, const dou
 
 cudaError_t pcg_start(const double* b, const double* x0, const double* ax0, const double* d,
                       double* x, double* r, double* z, double* p, int64_t n, int64_t ld, int q,
-                      double tol, PcgCols cols, double* partial, double* scratch3q,
-                      cudaStream_t st) {
+                      double tol, bool force_step, PcgCols cols, double* partial,
+                      double* scratch3q, cudaStream_t st) {
   const int nb = red_blocks(n);
   pcg_start_kernel<<<dim3(nb, q), kT, 0, st>>>(b, x0, ax0, d, x, r, z, p, n, ld, partial);
   reduce_partials<<<(unsigned)ceil_div(3 * q, 8), 256, 0, st>>>(partial, nb, 3 * q, scratch3q);
-  pcg_start_finish<<<(unsigned)ceil_div(q, 64), 64, 0, st>>>(scratch3q, q, tol, cols);
+  pcg_start_finish<<<(unsigned)ceil_div(q, 64), 64, 0, st>>>(scratch3q, q, tol, force_step ? 1 : 0,
+                                                             cols);
   return cudaGetLastError();
 }
 

@@ -34,11 +34,11 @@ cudaError_t cross_dots(const double* a, int p, const double* b, int q, const dou
 // PCG building blocks (columns with state != active are left untouched).
 // Start: x = x0 (or 0), r = b - ax0 (ax0 may be NULL meaning A x0 = 0),
 // z = r / d, p = z; rz, rr and tol_abs per column; state = active, or
-// converged when ||r|| < tol_abs already.
+// converged when ||r|| < tol_abs already (unless force_step).
 cudaError_t pcg_start(const double* b, const double* x0, const double* ax0, const double* d,
                       double* x, double* r, double* z, double* p, int64_t n, int64_t ld, int q,
-                      double tol, PcgCols cols, double* partial, double* scratch3q,
-                      cudaStream_t st);
+                      double tol, bool force_step, PcgCols cols, double* partial,
+                      double* scratch3q, cudaStream_t st);
 // ap = tau0 p / wmax + tau1 kp, pap = p'ap; columns with |pap| < 1e-30 stop.
 cudaError_t pcg_apply(const double* p, const double* kp, const double* wmax, double tau0,
                       double tau1, double* ap, int64_t n, int64_t ld, int q, PcgCols cols,

@@ -1,0 +1,101 @@
+"""MIXED-precision (tcgen05 kind::i8) GRM product, PCG and AI-REML on the GPU.
+
+The integer tensor-core arithmetic is checked bit for bit against a CPU model
+of the same quantised arithmetic; the quantisation error is then bounded
+against the FP64 oracle."""
+import numpy as np
+import pytest
+
+import csaige_b200 as cs
+import mixed_model as MM
+import oracle_ffi as O
+
+pytestmark = pytest.mark.gpu
+MIXED = cs.PREC_MIXED
+
+
+def _case(n, m, seed=7, sidx=None, miss=0.03):
+    spec = cs.CohortSpec(n=n, m=m, seed=seed, missing_rate=miss)
+    bed = cs.gen_bed(spec)
+    af, mac, nv = O.marker_stats(bed, n, m, sidx)
+    keep = np.nonzero((af >= 0.01) & (af <= 0.99))[0]
+    grm = cs.OnTheFlyGrm.from_bed(bed, n, m, keep, af[keep], sample_idx=sidx, precision=MIXED)
+    return grm, bed, keep, af[keep]
+
+
+@pytest.mark.parametrize("n,m,r", [(1001, 300, 1), (700, 129, 5), (2048, 256, 3)])
+def test_mixed_kv_bit_exact_vs_model(n, m, r):
+    grm, bed, keep, afs = _case(n, m)
+    v = np.random.default_rng(n + r).standard_normal((r, grm.n_samples))
+    got = grm.mat_vec(v)
+    want = MM.kv(MM.codes(bed, n, keep), afs, v.T).T
+    assert np.array_equal(got, want)
+
+
+def test_mixed_kv_subset_bit_exact():
+    rng = np.random.default_rng(9)
+    sidx = rng.permutation(1500)[:1111]
+    grm, bed, keep, afs = _case(1500, 200, sidx=sidx)
+    v = rng.standard_normal((2, grm.n_samples))
+    got = grm.mat_vec(v)
+    want = MM.kv(MM.codes(bed, 1500, keep, sidx), afs, v.T).T
+    assert np.array_equal(got, want)
+
+
+def test_mixed_kv_more_columns_than_one_launch():
+    grm, bed, keep, afs = _case(513, 140)
+    v = np.random.default_rng(1).standard_normal((70, grm.n_samples))
+    got = grm.mat_vec(v)
+    want = MM.kv(MM.codes(bed, 513, keep), afs, v.T).T
+    assert np.array_equal(got, want)
+
+
+def test_mixed_kv_accuracy_vs_fp64_oracle():
+    grm, bed, keep, afs = _case(3000, 800)
+    v = np.random.default_rng(2).standard_normal((4, grm.n_samples))
+    z = O.standardize(O.dosages(bed, 3000, keep), afs, 0)
+    got = grm.mat_vec(v)
+    for c in range(4):
+        want = O.grm_matvec(z, v[c], 0)
+        err = np.abs(got[c] - want).max() / np.abs(want).max()
+        assert err < 5e-7, err
+
+
+def test_mixed_pcg_matches_fp64_oracle():
+    grm, bed, keep, afs = _case(1200, 500)
+    n = grm.n_samples
+    rng = np.random.default_rng(3)
+    mu = 1 / (1 + np.exp(-(rng.standard_normal(n) - 2)))
+    w = mu * (1 - mu)
+    tau = [1.0, 0.4]
+    b = rng.standard_normal((3, n))
+    k = O.grm_explicit(O.standardize(O.dosages(bed, 1200, keep), afs, 0))
+    res = cs.PcgSolver(1e-6, 500).solve(grm, w, tau, b, precision=MIXED)
+    for c in range(3):
+        xo, ito, rso, cvo = O.pcg_sigma(O.K_EXPLICIT, k, n, 0, 0, w, tau, b[c], tol=1e-6)
+        assert res[c].converged and abs(res[c].iterations - ito) <= 1
+        assert np.abs(res[c].x - xo).max() / np.abs(xo).max() < 1e-5
+
+
+@pytest.mark.parametrize("trait", [O.BINARY, O.QUANTITATIVE])
+def test_mixed_ai_reml_tau_within_1e4_of_fp64_oracle(trait):
+    spec = cs.CohortSpec(n=800, m=600, seed=21, trait=trait, n_covar=2, prevalence=0.2, h2=0.4)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = O.marker_stats(bed, 800, 600)
+    g, _ = O.select_markers(af, mac, nv, 800)
+    grm = cs.OnTheFlyGrm.from_bed(bed, 800, 600, g, af[g], precision=MIXED)
+    k = O.grm_explicit(O.standardize(O.dosages(bed, 800, g), af[g], 0))
+    o = O.fit_ai_reml(y, x, trait, O.K_EXPLICIT, k, max_iter=8, tol=1e-5)
+    for solve, warm in [(cs.SOLVE_SINGLE, cs.WARM_ZERO), (cs.SOLVE_BLOCK, cs.WARM_PREVIOUS)]:
+        cfg = cs.AiRemlConfig(max_iter=8, tol=1e-5, precision=MIXED, solve=solve, warm_start=warm)
+        r = cs.fit_ai_reml(y, x, grm, cs.TraitType(trait), cfg)
+        rel = np.abs(r.tau - o["tau"]) / np.abs(o["tau"])
+        print("solve", solve, "warm", warm, "tau", r.tau, "oracle", o["tau"], "rel", rel,
+              "iters", r.iterations, o["iterations"])
+        if warm == cs.WARM_ZERO:
+            # the reference's solve order and starts: the same trajectory
+            assert r.iterations == o["iterations"]
+        # warm starts change where each solve stops inside the PCG tolerance, so the
+        # tau trajectory differs at that level and the iteration count may differ
+        assert r.converged and np.all(rel <= 1e-4)
