@@ -120,8 +120,8 @@ static Status grm_alloc(saige_grm* h, int64_t n, int64_t m) {
   SG_CUDA(cudaMalloc(&h->zlut, (size_t)h->m_pad * sizeof(float4)));
   SG_CUDA(cudaMalloc(&h->two_p, (size_t)h->m_pad * sizeof(double)));
   SG_CUDA(cudaMalloc(&h->inv_s, (size_t)h->m_pad * sizeof(double)));
-  // padding rows: all codes missing
-  SG_CUDA(cudaMemsetAsync(h->geno + (size_t)m * h->wpr, 0x55,
+  // padding rows: all codes 11 (genotype 0, not missing); their 1/s and 2p are 0
+  SG_CUDA(cudaMemsetAsync(h->geno + (size_t)m * h->wpr, 0xFF,
                           (size_t)(h->m_pad - m) * h->wpr * 4, h->stream));
   h->n_splits = fp32_z_splits(h->n_pad, h->m_pad);
   return Status();
@@ -134,6 +134,18 @@ static Status grm_upload_meta(saige_grm* h, const double* af) {
   SG_CUDA(cudaMemcpy(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice));
   SG_CUDA(cudaMemcpy(h->two_p, tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice));
   SG_CUDA(cudaMemcpy(h->inv_s, is.data(), is.size() * sizeof(double), cudaMemcpyHostToDevice));
+  return Status();
+}
+
+// A marker whose standardised column is zero (denominator <= 1e-10, pcg.rs:108)
+// contributes nothing; its row is re-coded 11 so no kernel does work for its
+// missing calls.
+static Status grm_blank_degenerate_rows(saige_grm* h, const double* af) {
+  for (int64_t j = 0; j < h->m; ++j) {
+    const double denom = sqrt(2.0 * af[j] * (1.0 - af[j]));
+    if (!(denom > 1e-10))
+      SG_CUDA(cudaMemsetAsync(h->geno + (size_t)j * h->wpr, 0xFF, (size_t)h->wpr * 4, h->stream));
+  }
   return Status();
 }
 
@@ -519,6 +531,7 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
       }
       SG_TRY(bed_gather_dev(src, n_fam, rows, sidx, identity, n, h->geno, h->wpr, nullptr,
                             h->stream));
+      SG_TRY(grm_blank_degenerate_rows(h, allele_freqs));
     }
     SG_CUDA(cudaStreamSynchronize(h->stream));
     return Status();

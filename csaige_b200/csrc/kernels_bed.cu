@@ -1,5 +1,6 @@
 // K1: gather the sample subset out of raw PLINK .bed rows, repack it into
-// 128-byte-aligned 2-bit rows, and count alleles and missing calls exactly.
+// 128-byte-aligned 2-bit rows (device word layout, see to_device_layout), and
+// count alleles and missing calls exactly.
 //
 // Replaces PlinkReader::read_marker_raw / read_marker (saige-geno/src/
 // plink.rs:182-194, 237-249) and MarkerData::compute_af's sums
@@ -28,6 +29,19 @@ __device__ __forceinline__ void count_word(uint32_t w, uint32_t valid, long long
   miss += __popc(mis);
 }
 
+// Device layout of a 32-bit word of 16 codes.  PLINK puts sample s at bits
+// 2s; the packed rows put sample s = 4j + i at bit 16*(j>>1) + 2*(j&1) + 4i, so
+// that each 4-sample group's codes sit in the low bits of four nibbles that one
+// mask (or shift + mask) turns into a byte-permute selector.
+__device__ __forceinline__ uint32_t nibble_spread16x2(uint32_t x) {
+  x = (x | (x << 4)) & 0x0F0F0F0Fu;
+  return (x | (x << 2)) & 0x33333333u;
+}
+__device__ __forceinline__ uint32_t to_device_layout(uint32_t plink_word) {
+  return nibble_spread16x2(plink_word & 0x00FF00FFu) |
+         (nibble_spread16x2((plink_word >> 8) & 0x00FF00FFu) << 2);
+}
+
 __device__ __forceinline__ long long warp_sum_ll(long long v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -54,7 +68,9 @@ __global__ void __launch_bounds__(kThreads)
   const int64_t n_words_real = (n + 15) / 16;
   const int64_t n_words = out ? wpr : n_words_real;
   for (int64_t j = threadIdx.x; j < n_words; j += blockDim.x) {
-    uint32_t w = 0x55555555u;  // padding: all codes 01 (missing -> z = 0)
+    // Padding samples are coded 11 (genotype 0, not missing): every vector the
+    // products read is zero there, so they contribute nothing to any sum.
+    uint32_t w = 0xFFFFFFFFu;
     if (j < n_words_real) {
       const int64_t k0 = j * 16;
       const int kn = (n - k0) < 16 ? (int)(n - k0) : 16;
@@ -76,7 +92,8 @@ __global__ void __launch_bounds__(kThreads)
       }
       const uint32_t keep = kn >= 16 ? 0xFFFFFFFFu : ((1u << (2 * kn)) - 1u);
       count_word(word, keep & 0x55555555u, alt, miss);
-      w = (word & keep) | (0x55555555u & ~keep);
+      // padding samples are coded 11, then the word is re-laid out
+      w = to_device_layout((word & keep) | ~keep);
     }
     if (out) out[r * wpr + j] = w;
   }

@@ -3,9 +3,11 @@
 // f32 per marker and code exactly as OnTheFlyGrm::new (pcg.rs:101-122), v
 // rounded to f32, f32 products and sums — read straight from the 2-bit rows.
 //
-// Decode: two samples' codes form a 4-bit index into a per-marker table of
-// 16 float2 entries (z(code_even), z(code_odd)) held in shared memory; one
-// 64-bit shared load plus one packed f32x2 FMA covers two samples.  The 16
+// Decode: each nibble of a packed word holds two samples' codes (the device
+// word layout pairs samples (k, k+4) and (k+4, k+8)); the nibble indexes a
+// per-marker table of 16 float2 entries (z(code_lo), z(code_hi)) held in
+// shared memory, so one 64-bit shared load plus one packed f32x2 FMA covers
+// two samples.  The 16
 // entries span all 32 banks, so a warp's lookups never conflict.
 //   pass A  u_m  = sum_i z_mi v_i        (CTA = 16 markers x all samples)
 //   pass B  y_i  = sum_m z_mi u_m        (CTA = 4096 samples x a marker split)
@@ -49,13 +51,12 @@ __global__ void __launch_bounds__(kThreads)
   for (int64_t s = warp; s < n_steps; s += kWarps) {
     const int64_t wo = s * 32 + lane;
     const float4* vp = reinterpret_cast<const float4*>(v32 + wo * 16);
-    float2 vv[8];
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      const float4 t = __ldg(vp + q);
-      vv[2 * q] = make_float2(t.x, t.y);
-      vv[2 * q + 1] = make_float2(t.z, t.w);
-    }
+    // nibble k of a device-layout word holds samples (k, k+4) for k < 4 and
+    // (k+4, k+8) for k >= 4
+    const float4 f0 = __ldg(vp), f1 = __ldg(vp + 1), f2 = __ldg(vp + 2), f3 = __ldg(vp + 3);
+    const float2 vv[8] = {make_float2(f0.x, f1.x), make_float2(f0.y, f1.y), make_float2(f0.z, f1.z),
+                          make_float2(f0.w, f1.w), make_float2(f2.x, f3.x), make_float2(f2.y, f3.y),
+                          make_float2(f2.z, f3.z), make_float2(f2.w, f3.w)};
     uint32_t w[kMarkersA];
 #pragma unroll
     for (int mb = 0; mb < kMarkersA; ++mb) w[mb] = __ldg(rows + mb * wpr + wo);
@@ -132,9 +133,10 @@ __global__ void __launch_bounds__(kThreads)
   }
   if (active) {
     float4* o = reinterpret_cast<float4*>(ypart + (int64_t)blockIdx.y * n_pad + wo * 16);
-#pragma unroll
-    for (int q = 0; q < 4; ++q)
-      o[q] = make_float4(acc[2 * q].x, acc[2 * q].y, acc[2 * q + 1].x, acc[2 * q + 1].y);
+    o[0] = make_float4(acc[0].x, acc[1].x, acc[2].x, acc[3].x);
+    o[1] = make_float4(acc[0].y, acc[1].y, acc[2].y, acc[3].y);
+    o[2] = make_float4(acc[4].x, acc[5].x, acc[6].x, acc[7].x);
+    o[3] = make_float4(acc[4].y, acc[5].y, acc[6].y, acc[7].y);
   }
 }
 
