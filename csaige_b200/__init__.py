@@ -23,6 +23,8 @@ from .api import (  # noqa: F401
     bed_marker_stats,
     device_count,
     fit_ai_reml,
+    fit_null_from_bed,
+    kernel_launches,
     gen_bed,
     gen_bed_dev,
     gen_pheno,

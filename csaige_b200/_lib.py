@@ -67,6 +67,19 @@ class AiRemlSummaryC(C.Structure):
     ]
 
 
+class GrmStatsC(C.Structure):
+    _fields_ = [
+        ("n_kv", C.c_int64),
+        ("n_kv_launches", C.c_int64),
+        ("tc_pass_a_launches", C.c_int64),
+        ("tc_pass_b_launches", C.c_int64),
+        ("tc_pass_a_ms", C.c_double),
+        ("tc_pass_b_ms", C.c_double),
+        ("fp32_launches", C.c_int64),
+        ("fp32_ms", C.c_double),
+    ]
+
+
 class CohortSpecC(C.Structure):
     _fields_ = [
         ("seed", C.c_uint64),
@@ -143,6 +156,19 @@ SIGNATURES = {
         [_vp, _d, _d, C.c_int64, C.c_int32, C.c_int32, P(AiRemlConfigC), P(AiRemlSummaryC),
          _d, _d, _d, _d, _d],
     ),
+    "saige_bed_marker_stats_dev": (
+        C.c_int32,
+        [_vp, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _d, _d, _i64],
+    ),
+    "saige_fit_null_from_bed": (
+        C.c_int32,
+        [_u8, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _d, _d, C.c_int32, C.c_int32,
+         C.c_double, C.c_double, P(AiRemlConfigC), P(AiRemlSummaryC), _d, _d, _d, _i64, _i64],
+    ),
+    "saige_grm_set_profiling": (C.c_int32, [_vp, C.c_int32]),
+    "saige_grm_get_stats": (C.c_int32, [_vp, P(GrmStatsC)]),
+    "saige_grm_reset_stats": (C.c_int32, [_vp]),
+    "saige_kernel_launches": (C.c_int64, []),
     "saige_gen_bed": (C.c_int32, [P(CohortSpecC), _vp, C.c_int32]),
     "saige_gen_pheno": (C.c_int32, [P(CohortSpecC), _d, _d]),
 }

@@ -91,6 +91,19 @@ def bed_marker_stats(bed, n_fam: int, m_tot: int, sample_idx: Optional[Sequence[
     return af, mac, nv
 
 
+def bed_marker_stats_dev(bed_ptr: int, bed_len: int, n_fam: int, m_tot: int,
+                         sample_idx: Optional[Sequence[int]] = None):
+    """bed_marker_stats for a .bed already in device memory (bed_ptr: device address)."""
+    sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
+    n = n_fam if sidx is None else sidx.size
+    af = np.empty(m_tot)
+    mac = np.empty(m_tot)
+    nv = np.empty(m_tot, dtype=np.int64)
+    check(LIB.saige_bed_marker_stats_dev(C.c_void_p(bed_ptr), bed_len, n_fam, m_tot, _i64ptr(sidx),
+                                         n, _dptr(af), _dptr(mac), _i64ptr(nv)))
+    return af, mac, nv
+
+
 def select_grm_markers(af, mac, n_valid, n: int, min_maf: float = 0.01,
                        max_missing: float = 0.15, seed: int = 12345):
     """(grm_idx, vr_idx): QC plus the variance-ratio marker split of fit-null."""
@@ -398,3 +411,67 @@ def gen_pheno(spec: CohortSpec) -> tuple[np.ndarray, np.ndarray]:
     s = spec.c()
     check(LIB.saige_gen_pheno(C.byref(s), _dptr(y), _dptr(x)))
     return y, x.reshape(1 + spec.n_covar, spec.n).T.copy()
+
+
+# ---------------------------------------------------------------------------
+# whole fit-null from host buffers, instrumentation
+# ---------------------------------------------------------------------------
+@dataclass
+class FitNullResult:
+    ai_reml: AiRemlResult
+    m_grm: int
+    m_vr: int
+
+
+def fit_null_from_bed(bed, n_fam: int, m_tot: int, y, x, trait_type: TraitType,
+                      config: AiRemlConfig = AiRemlConfig(), sample_idx=None,
+                      min_maf: float = 0.01, max_missing: float = 0.15) -> FitNullResult:
+    """Marker statistics, QC + VR/GRM split, GRM operator and AI-REML in one call
+    (the genotype part of saige-cli fit_null::run)."""
+    b = _bed_array(bed)
+    yy = _f64(y)
+    n = yy.size
+    xc, p = _design(x, n)
+    sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
+    cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
+                             config.n_random_vectors, config.seed, config.precision, config.solve,
+                             config.warm_start, 0)
+    out = _lib.AiRemlSummaryC()
+    alpha = np.zeros(p)
+    mu = np.zeros(n)
+    trace = np.full(2 * max(config.max_iter, 1), np.nan)
+    mg, mv = C.c_int64(), C.c_int64()
+    check(LIB.saige_fit_null_from_bed(
+        b.ctypes.data_as(C.POINTER(C.c_uint8)), b.size, n_fam, m_tot, _i64ptr(sidx), n, _dptr(yy),
+        _dptr(xc), p, int(trait_type), min_maf, max_missing, C.byref(cfg), C.byref(out),
+        _dptr(alpha), _dptr(mu), _dptr(trace), C.byref(mg), C.byref(mv)))
+    it = out.iterations
+    res = AiRemlResult(
+        tau=np.array([out.tau[0], out.tau[1]]), iterations=it, converged=bool(out.converged),
+        mu=mu, working_weights=np.zeros(0), residuals=yy - mu, eta=np.zeros(0), alpha=alpha,
+        log_likelihood=out.log_likelihood, n_kv=out.n_kv, n_kv_launches=out.n_kv_launches,
+        pcg_iters=out.pcg_iters, seconds=out.seconds, tau_trace=trace[: 2 * it].reshape(-1, 2))
+    return FitNullResult(res, mg.value, mv.value)
+
+
+def kernel_launches() -> int:
+    return int(LIB.saige_kernel_launches())
+
+
+def _grm_stats(self) -> dict:
+    st = _lib.GrmStatsC()
+    check(LIB.saige_grm_get_stats(self._h, C.byref(st)))
+    return {f: getattr(st, f) for f, _ in _lib.GrmStatsC._fields_}
+
+
+def _grm_set_profiling(self, on: bool = True) -> None:
+    check(LIB.saige_grm_set_profiling(self._h, 1 if on else 0))
+
+
+def _grm_reset_stats(self) -> None:
+    check(LIB.saige_grm_reset_stats(self._h))
+
+
+OnTheFlyGrm.stats = _grm_stats
+OnTheFlyGrm.set_profiling = _grm_set_profiling
+OnTheFlyGrm.reset_stats = _grm_reset_stats

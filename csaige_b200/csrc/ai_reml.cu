@@ -452,3 +452,52 @@ SG_API int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x,
     return fail(SAIGE_EINVAL, "unexpected C++ exception").code;
   }
 }
+
+SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                       int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                       const double* y, const double* x, int32_t p, int32_t trait,
+                                       double min_maf, double max_missing,
+                                       const saige_ai_reml_config* cfg,
+                                       saige_ai_reml_summary* out, double* alpha, double* mu,
+                                       double* tau_trace, int64_t* m_grm_out, int64_t* m_vr_out) {
+  try {
+    set_error("");
+    if (!bed || !y || !x || !out || m_tot <= 0) return fail(SAIGE_EINVAL, "null argument").code;
+    saige_ai_reml_config c;
+    if (cfg) c = *cfg;
+    else saige_ai_reml_config_default(&c);
+    if (bed_len < 3) return fail(SAIGE_EBED, "Bed file too small").code;
+    // one upload of the .bed (fit_null.rs:118 maps it once as well)
+    DevBuf d_bed;
+    Status s = d_bed.reserve(bed_len);
+    if (!s.ok()) return s.code;
+    if (cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice) != cudaSuccess)
+      return fail(SAIGE_ECUDA, "bed upload failed: %s", cudaGetErrorString(cudaGetLastError())).code;
+    std::vector<double> af((size_t)m_tot), mac((size_t)m_tot);
+    std::vector<int64_t> nv((size_t)m_tot);
+    int32_t rc = saige_bed_marker_stats_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx,
+                                            n, af.data(), mac.data(), nv.data());
+    if (rc != SAIGE_OK) return rc;
+    std::vector<int64_t> gidx((size_t)m_tot), vidx((size_t)m_tot);
+    int64_t m_grm = 0, m_vr = 0;
+    rc = saige_select_grm_markers(af.data(), mac.data(), nv.data(), m_tot, n, min_maf, max_missing,
+                                  c.seed, gidx.data(), &m_grm, vidx.data(), &m_vr);
+    if (rc != SAIGE_OK) return rc;
+    if (m_grm_out) *m_grm_out = m_grm;
+    if (m_vr_out) *m_vr_out = m_vr;
+    std::vector<double> gaf((size_t)m_grm);
+    for (int64_t j = 0; j < m_grm; ++j) gaf[(size_t)j] = af[(size_t)gidx[(size_t)j]];
+    saige_grm* h = nullptr;
+    rc = saige_grm_create_from_bed_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx, n,
+                                       gidx.data(), m_grm, gaf.data(), -1, &h);
+    if (rc != SAIGE_OK) return rc;
+    d_bed.release();  // the handle holds the packed GRM rows
+    rc = saige_fit_ai_reml(h, y, x, n, p, trait, &c, out, alpha, mu, nullptr, nullptr, tau_trace);
+    saige_grm_destroy(h);
+    return rc;
+  } catch (const std::bad_alloc&) {
+    return fail(SAIGE_ENOMEM, "host allocation failed").code;
+  } catch (...) {
+    return fail(SAIGE_EINVAL, "unexpected C++ exception").code;
+  }
+}

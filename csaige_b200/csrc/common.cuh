@@ -24,6 +24,10 @@ struct Status {
 
 Status fail(int32_t code, const char* fmt, ...);
 
+// Process-wide count of kernels launched by this library.
+void count_launches(int k);
+int64_t launches_total();
+
 #define SG_CUDA(call)                                                                  \
   do {                                                                                 \
     cudaError_t _e = (call);                                                           \

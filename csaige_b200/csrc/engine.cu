@@ -4,6 +4,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <atomic>
 #include <string>
 #include <vector>
 
@@ -18,9 +19,12 @@ namespace saige {
 // errors
 // ---------------------------------------------------------------------------
 static thread_local std::string g_err;
+static std::atomic<int64_t> g_launches{0};
 
 void set_error(const std::string& msg) { g_err = msg; }
 const char* last_error() { return g_err.c_str(); }
+void count_launches(int k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+int64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 Status fail(int32_t code, const char* fmt, ...) {
   char buf[1024];
@@ -73,7 +77,7 @@ static Status pick_device(int32_t want, int* dev) {
     return fail(SAIGE_ECUDA, "device %d is sm_%d%d; this library is built for sm_100a only", d,
                 prop.major, prop.minor);
   SG_CUDA(cudaSetDevice(d));
-  *dev = d;
+  if (dev) *dev = d;
   return Status();
 }
 
@@ -234,6 +238,13 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
   SG_TRY(h->u32.reserve((size_t)h->m_pad * sizeof(float)));
   SG_TRY(h->ypart.reserve((size_t)h->n_splits * h->n_pad * sizeof(float)));
   const float scale = 1.0f / (float)h->m;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (h->profiling) {
+    SG_CUDA(cudaEventCreate(&e0));
+    SG_CUDA(cudaEventCreate(&e1));
+    SG_CUDA(cudaEventRecord(e0, st));
+  }
+  int64_t done = 0;
   for (int c = 0; c < q; ++c) {
     if (active && active[c] != kColActive) continue;
     const double* vc = v + (int64_t)c * h->n_pad;
@@ -245,7 +256,18 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
                           h->ypart.as<float>(), h->n_splits, st));
     SG_CUDA(launch_fp32_finish(h->ypart.as<float>(), h->n_splits, h->n_pad, h->n, scale, oc, st));
     h->n_kv += 1;
-    h->n_kv_launches += 1;
+    ++done;
+  }
+  h->n_kv_launches += 1;
+  h->stats.fp32_launches += done;
+  if (h->profiling) {
+    SG_CUDA(cudaEventRecord(e1, st));
+    SG_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    h->stats.fp32_ms += ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
   }
   return Status();
 }
@@ -389,20 +411,27 @@ SG_API int32_t saige_device_count(void) {
   return usable;
 }
 
-SG_API int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_t n_fam,
-                                      int64_t m_tot, const int64_t* sample_idx, int64_t n,
-                                      double* af, double* mac, int64_t* n_valid) {
-  SG_GUARD_BEGIN
-  set_error("");
+static int32_t marker_stats_impl(const uint8_t* bed, bool on_device, size_t bed_len,
+                                 int64_t n_fam, int64_t m_tot, const int64_t* sample_idx,
+                                 int64_t n, double* af, double* mac, int64_t* n_valid) {
   if (!bed || !af || !mac || !n_valid || m_tot < 0) return fail(SAIGE_EINVAL, "null argument").code;
-  Status s = check_bed_header(bed, bed_len, n_fam, m_tot);
+  uint8_t hdr[3] = {0, 0, 0};
+  Status s;
+  if (!on_device) {
+    if (bed_len >= 3) memcpy(hdr, bed, 3);
+  } else {
+    s = pick_device(-1, nullptr);
+    if (!s.ok()) return s.code;
+    if (bed_len >= 3 && cudaMemcpy(hdr, bed, 3, cudaMemcpyDeviceToHost) != cudaSuccess)
+      return fail(SAIGE_ECUDA, "reading the bed header from device memory failed").code;
+  }
+  s = check_bed_header(hdr, bed_len, n_fam, m_tot);
   if (!s.ok()) return s.code;
   std::vector<int32_t> sidx;
   bool identity;
   s = check_subset(sample_idx, n, n_fam, sidx, identity);
   if (!s.ok()) return s.code;
-  int dev;
-  s = pick_device(-1, &dev);
+  s = pick_device(-1, nullptr);
   if (!s.ok()) return s.code;
   const int64_t bpm = (n_fam + 3) / 4;
   const size_t used = (size_t)(3 + bpm * m_tot);
@@ -411,14 +440,18 @@ SG_API int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_
     return fail(SAIGE_ECUDA, "stream creation failed").code;
   DevBuf d_bed, d_cnt;
   auto body = [&]() -> Status {
-    SG_TRY(d_bed.reserve(used));
     SG_TRY(d_cnt.reserve((size_t)std::max<int64_t>(m_tot, 1) * 2 * sizeof(int64_t)));
-    SG_CUDA(cudaMemcpyAsync(d_bed.ptr, bed, used, cudaMemcpyHostToDevice, st));
+    const uint8_t* src = bed;
+    if (!on_device) {
+      SG_TRY(d_bed.reserve(used));
+      SG_CUDA(cudaMemcpyAsync(d_bed.ptr, bed, used, cudaMemcpyHostToDevice, st));
+      src = d_bed.as<uint8_t>();
+    }
     std::vector<int64_t> rows((size_t)m_tot);
     for (int64_t j = 0; j < m_tot; ++j) rows[(size_t)j] = j;
     if (m_tot > 0)
-      SG_TRY(bed_gather_dev(d_bed.as<uint8_t>(), n_fam, rows, sidx, identity, n, nullptr, 0,
-                            d_cnt.as<int64_t>(), st));
+      SG_TRY(bed_gather_dev(src, n_fam, rows, sidx, identity, n, nullptr, 0, d_cnt.as<int64_t>(),
+                            st));
     std::vector<int64_t> cnt((size_t)m_tot * 2);
     if (m_tot > 0) {
       SG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -441,8 +474,51 @@ SG_API int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_
   d_cnt.release();
   cudaStreamDestroy(st);
   return s.code;
+}
+
+SG_API int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                      int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                      double* af, double* mac, int64_t* n_valid) {
+  SG_GUARD_BEGIN
+  set_error("");
+  return marker_stats_impl(bed, false, bed_len, n_fam, m_tot, sample_idx, n, af, mac, n_valid);
   SG_GUARD_END
 }
+
+SG_API int32_t saige_bed_marker_stats_dev(const uint8_t* bed_dev, size_t bed_len, int64_t n_fam,
+                                          int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                          double* af, double* mac, int64_t* n_valid) {
+  SG_GUARD_BEGIN
+  set_error("");
+  return marker_stats_impl(bed_dev, true, bed_len, n_fam, m_tot, sample_idx, n, af, mac, n_valid);
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_set_profiling(saige_grm* h, int32_t on) {
+  if (!h) return fail(SAIGE_EINVAL, "null handle").code;
+  std::lock_guard<std::recursive_mutex> lk(h->mu);
+  h->profiling = on != 0;
+  return SAIGE_OK;
+}
+
+SG_API int32_t saige_grm_get_stats(const saige_grm* h, saige_grm_stats* out) {
+  if (!h || !out) return fail(SAIGE_EINVAL, "null argument").code;
+  *out = h->stats;
+  out->n_kv = h->n_kv;
+  out->n_kv_launches = h->n_kv_launches;
+  return SAIGE_OK;
+}
+
+SG_API int32_t saige_grm_reset_stats(saige_grm* h) {
+  if (!h) return fail(SAIGE_EINVAL, "null handle").code;
+  std::lock_guard<std::recursive_mutex> lk(h->mu);
+  h->stats = saige_grm_stats{};
+  h->n_kv = 0;
+  h->n_kv_launches = 0;
+  return SAIGE_OK;
+}
+
+SG_API int64_t saige_kernel_launches(void) { return launches_total(); }
 
 SG_API int32_t saige_select_grm_markers(const double* af, const double* mac,
                                         const int64_t* n_valid, int64_t m_tot, int64_t n,

@@ -45,6 +45,8 @@ struct saige_grm {
   saige::DevBuf ws_vec, ws_red, ws_cols, ws_io;
   // statistics
   int64_t n_kv = 0, n_kv_launches = 0;
+  bool profiling = false;
+  saige_grm_stats stats{};
 };
 
 namespace saige {

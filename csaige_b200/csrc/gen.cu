@@ -78,6 +78,7 @@ SG_API int32_t saige_gen_bed(const saige_cohort_spec* spec, uint8_t* bed_out, in
     if (cudaMemcpy(bed_out, hdr, 3, cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(SAIGE_ECUDA, "header copy failed: %s", cudaGetErrorString(cudaGetLastError())).code;
     gen_bed_kernel<<<148 * 16, 256>>>(L, bed_out, bpm);
+    count_launches(1);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return fail(SAIGE_ECUDA, "gen_bed_kernel: %s", cudaGetErrorString(e)).code;
     return SAIGE_OK;

@@ -139,6 +139,7 @@ cudaError_t launch_bed_gather(const uint8_t* bed, int64_t bpm, const int64_t* sr
     bed_gather_kernel<true><<<(unsigned)n_rows, kThreads, 0, st>>>(
         bed, bpm, src_rows, nullptr, n, geno_out, words_per_row, counts, 0);
   }
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -169,6 +169,7 @@ int fp32_z_splits(int64_t n_pad, int64_t m_pad) {
 cudaError_t launch_fp32_zt(const uint32_t* geno, int64_t wpr, const float4* zlut, int64_t m_pad,
                            const float* v32, float* u, cudaStream_t st) {
   fp32_zt_kernel<<<(unsigned)(m_pad / kMarkersA), kThreads, 0, st>>>(geno, wpr, zlut, v32, u);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -178,6 +179,7 @@ cudaError_t launch_fp32_z(const uint32_t* geno, int64_t wpr, const float4* zlut,
   const int64_t per_split = round_up(ceil_div(m_pad, n_splits), 4);
   dim3 grid((unsigned)windows, (unsigned)n_splits);
   fp32_z_kernel<<<grid, kThreads, 0, st>>>(geno, wpr, zlut, m_pad, u, ypart, wpr * 16, per_split);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -185,11 +187,13 @@ cudaError_t launch_fp32_finish(const float* ypart, int n_splits, int64_t n_pad, 
                                float scale, double* out, cudaStream_t st) {
   fp32_finish_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(ypart, n_splits, n_pad, n, scale,
                                                                  out);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t launch_to_f32(const double* v, int64_t n, int64_t n_pad, float* v32, cudaStream_t st) {
   to_f32_kernel<<<(unsigned)ceil_div(n_pad, 256), 256, 0, st>>>(v, n, n_pad, v32);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -844,6 +844,7 @@ template <bool kPassB, bool kSparse>
 static cudaError_t launch_tc(const TcPlan* p, unsigned grid, const TcArgs& a, cudaStream_t st) {
   tc_grm_kernel<kPassB, kSparse><<<grid, kThreads, tc_smem_bytes(a.ng, a.r, kPassB, kSparse), st>>>(
       p->codes_map, a);
+  count_launches(1);
   return cudaGetLastError();
 }
 
@@ -872,6 +873,16 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
   SG_CUDA(cudaMemcpyAsync(p->cmap.ptr, cols.data(), cols.size() * sizeof(int),
                           cudaMemcpyHostToDevice, st));
   SG_CUDA(cudaMemsetAsync(sc.err, 0, sizeof(unsigned int), st));
+  // per-pass CUDA-event timing when profiling is on (events on the launching stream)
+  std::vector<cudaEvent_t> ev;
+  auto mark = [&](cudaEvent_t* e) -> Status {
+    if (!h->profiling) return Status();
+    SG_CUDA(cudaEventCreate(e));
+    ev.push_back(*e);
+    SG_CUDA(cudaEventRecord(*e, st));
+    return Status();
+  };
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_a, ev_b;
   for (size_t c0 = 0; c0 < cols.size(); c0 += kMaxR) {
     const int r = (int)std::min<size_t>(kMaxR, cols.size() - c0);
     const int ng = (int)round_up(3 * r, 16);
@@ -883,6 +894,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     {
       dim3 g1((unsigned)std::min<int64_t>(ceil_div(h->n, 256), 296), (unsigned)r);
       amax_v_kernel<<<g1, 256, 0, st>>>(v, h->n_pad, h->n, cmap, sc.amax_v);
+      count_launches(2);
       dim3 g2((unsigned)n_stages_a, (unsigned)r);
       quant_v_kernel<<<g2, 128, 0, st>>>(v, h->n_pad, h->n, cmap, sc.amax_v, sc.scale_v,
                                          p->img_a.as<uint8_t>(), ng, sc.sum_v,
@@ -907,9 +919,14 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.err = sc.err;
       a.trace = p->tracing ? p->trace.as<unsigned long long>() : nullptr;
       const unsigned grid = (unsigned)(h->m_pad / kRows);
+      cudaEvent_t t0 = nullptr, t1 = nullptr;
+      SG_TRY(mark(&t0));
       const cudaError_t e = sparse ? launch_tc<false, true>(p, grid, a, st)
                                    : launch_tc<false, false>(p, grid, a, st);
       SG_CUDA(e);
+      SG_TRY(mark(&t1));
+      if (h->profiling) ev_a.emplace_back(t0, t1);
+      h->stats.tc_pass_a_launches += 1;
       if (p->tracing) SG_TRY(trace_dump(p, "pass A", st));
     }
     // ---- pass B operands ----
@@ -917,6 +934,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       SG_CUDA(cudaMemsetAsync(p->img_w.ptr, 0, (size_t)h->m_pad * ng, st));
       if (!sparse) SG_CUDA(cudaMemsetAsync(p->img_c.ptr, 0, (size_t)h->m_pad * ng, st));
       dim3 g1((unsigned)std::min<int64_t>(ceil_div(h->m_pad, 256), 296), (unsigned)r);
+      count_launches(2);
       amax_wc_kernel<<<g1, 256, 0, st>>>(p->u.as<double>(), h->m_pad, h->m_pad, h->inv_s,
                                          h->two_p, sc.amax_w, sc.amax_c);
       dim3 g2((unsigned)n_stages_b, (unsigned)r);
@@ -947,9 +965,14 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.err = sc.err;
       a.trace = p->tracing ? p->trace.as<unsigned long long>() : nullptr;
       const unsigned grid = (unsigned)(h->n_pad / kRows);
+      cudaEvent_t t0 = nullptr, t1 = nullptr;
+      SG_TRY(mark(&t0));
       const cudaError_t e = sparse ? launch_tc<true, true>(p, grid, a, st)
                                    : launch_tc<true, false>(p, grid, a, st);
       SG_CUDA(e);
+      SG_TRY(mark(&t1));
+      if (h->profiling) ev_b.emplace_back(t0, t1);
+      h->stats.tc_pass_b_launches += 1;
       if (p->tracing) SG_TRY(trace_dump(p, "pass B", st));
     }
     h->n_kv += r;
@@ -958,6 +981,17 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
   unsigned int err = 0;
   SG_CUDA(cudaMemcpyAsync(&err, sc.err, sizeof(err), cudaMemcpyDeviceToHost, st));
   SG_CUDA(cudaStreamSynchronize(st));
+  for (auto& pr : ev_a) {
+    float ms = 0.f;
+    SG_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    h->stats.tc_pass_a_ms += ms;
+  }
+  for (auto& pr : ev_b) {
+    float ms = 0.f;
+    SG_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    h->stats.tc_pass_b_ms += ms;
+  }
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
   if (err) return fail(SAIGE_TIMEOUT, "tensor-core GRM product: a pipeline wait timed out");
   return Status();
 }

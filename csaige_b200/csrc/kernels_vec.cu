@@ -365,6 +365,7 @@ cudaError_t col_dots(const double* a, const double* b, int64_t n, int64_t ld, in
   const int nb = red_blocks(n);
   col_dots_kernel<<<dim3(nb, q), kT, 0, st>>>(a, b, n, ld, partial);
   reduce_partials<<<(unsigned)ceil_div(q, 8), 256, 0, st>>>(partial, nb, q, out);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -373,6 +374,7 @@ cudaError_t cross_dots(const double* a, int p, const double* b, int q, const dou
   const int nb = red_blocks(n);
   cross_dots_kernel<<<dim3(nb, p * q), kT, 0, st>>>(a, b, q, w, n, ld, partial);
   reduce_partials<<<(unsigned)ceil_div(p * q, 8), 256, 0, st>>>(partial, nb, p * q, out);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -385,6 +387,7 @@ cudaError_t pcg_start(const double* b, const double* x0, const double* ax0, cons
   reduce_partials<<<(unsigned)ceil_div(3 * q, 8), 256, 0, st>>>(partial, nb, 3 * q, scratch3q);
   pcg_start_finish<<<(unsigned)ceil_div(q, 64), 64, 0, st>>>(scratch3q, q, tol, force_step ? 1 : 0,
                                                              cols);
+  count_launches(3);
   return cudaGetLastError();
 }
 
@@ -395,6 +398,7 @@ cudaError_t pcg_apply(const double* p, const double* kp, const double* wmax, dou
   pcg_apply_kernel<true><<<dim3(nb, q), kT, 0, st>>>(p, kp, wmax, tau0, tau1, ap, n, ld,
                                                      cols.state, partial);
   pcg_apply_finish<<<(unsigned)ceil_div(q, 8), 256, 0, st>>>(partial, nb, q, cols);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -405,6 +409,7 @@ cudaError_t pcg_apply_w(const double* p, const double* kp, const double* w, doub
   pcg_apply_kernel<false><<<dim3(nb, q), kT, 0, st>>>(p, kp, w, tau0, tau1, ap, n, ld,
                                                       cols.state, partial);
   pcg_apply_finish<<<(unsigned)ceil_div(q, 8), 256, 0, st>>>(partial, nb, q, cols);
+  count_launches(2);
   return cudaGetLastError();
 }
 
@@ -418,59 +423,69 @@ cudaError_t pcg_step(double* x, double* r, double* z, double* p, const double* a
   unsigned gx = (unsigned)ceil_div(n, kT);
   if (gx > 1024) gx = 1024;
   pcg_p_kernel<<<dim3(gx, q), kT, 0, st>>>(p, z, n, ld, cols.state, scratch2q);
+  count_launches(3);
   return cudaGetLastError();
 }
 
 cudaError_t sigma_diag(const double* w, double tau0, double tau1, double* wmax, double* d,
                        int64_t n, cudaStream_t st) {
   sigma_diag_kernel<<<g1(n), kT, 0, st>>>(w, tau0, tau1, wmax, d, n);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t sigma_diag_w(const double* w, double tau0, double tau1, double* d, int64_t n,
                          cudaStream_t st) {
   sigma_diag_w_kernel<<<g1(n), kT, 0, st>>>(w, tau0, tau1, d, n);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t eta_mu(const double* x, int p, const double* alpha, int trait, double* eta, double* mu,
                    int64_t n, int64_t ld, cudaStream_t st) {
   eta_mu_kernel<<<g1(n), kT, 0, st>>>(x, p, alpha, trait, eta, mu, n, ld);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t work_vectors(const double* y, const double* eta, const double* mu, int trait,
                          double* w, double* ytil, int64_t n, cudaStream_t st) {
   work_vectors_kernel<<<g1(n), kT, 0, st>>>(y, eta, mu, trait, w, ytil, n);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t init_mu(const double* y, int trait, double* mu, double* eta, int64_t n,
                     cudaStream_t st) {
   init_mu_kernel<<<g1(n), kT, 0, st>>>(y, trait, mu, eta, n);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t sub_combo(double* y, int q, const double* a, int p, const double* coef, int64_t n,
                       int64_t ld, cudaStream_t st) {
   sub_combo_kernel<<<dim3(g1(n), q), kT, 0, st>>>(y, q, a, p, coef, n, ld);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t div_w(const double* v, const double* w, double* out, int64_t n, cudaStream_t st) {
   div_w_kernel<<<g1(n), kT, 0, st>>>(v, w, out, n);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t expand_signs(const uint8_t* signs, double* out, int64_t n, int64_t ld, int q,
                          cudaStream_t st) {
   expand_signs_kernel<<<dim3(g1(ld), q), kT, 0, st>>>(signs, out, n, ld);
+  count_launches(1);
   return cudaGetLastError();
 }
 
 cudaError_t zero_pad(double* v, int64_t n, int64_t ld, int q, cudaStream_t st) {
   if (ld <= n) return cudaSuccess;
   zero_pad_kernel<<<dim3(g1(ld - n), q), kT, 0, st>>>(v, n, ld);
+  count_launches(1);
   return cudaGetLastError();
 }
 

@@ -87,6 +87,11 @@ int32_t saige_bed_marker_stats(const uint8_t* bed, size_t bed_len, int64_t n_fam
                                const int64_t* sample_idx, int64_t n, double* af, double* mac,
                                int64_t* n_valid);
 
+/* Same as saige_bed_marker_stats with the .bed already in device memory. */
+int32_t saige_bed_marker_stats_dev(const uint8_t* bed_dev, size_t bed_len, int64_t n_fam,
+                                   int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                   double* af, double* mac, int64_t* n_valid);
+
 /* Marker QC and the variance-ratio / GRM marker split of fit-null
  * (saige-cli/src/commands/fit_null.rs:209-259): keep af in
  * [min_maf, 1-min_maf] and missing rate <= max_missing; draw 1000 indices
@@ -224,6 +229,44 @@ int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x, int64_
                           int32_t trait, const saige_ai_reml_config* cfg,
                           saige_ai_reml_summary* out, double* alpha, double* mu, double* eta,
                           double* w, double* tau_trace);
+
+/* The fit-null pipeline of saige-cli/src/commands/fit_null.rs:199-287 from
+ * host buffers in one call: marker statistics over the sample subset
+ * (plink.rs:237-267), QC and the VR/GRM split (fit_null.rs:209-259), the GRM
+ * operator over the GRM markers (pcg.rs:101-122) and fit_ai_reml
+ * (ai_reml.rs:86-427).  The .bed is copied to the device once.  Phenotype
+ * and covariate parsing stay with the caller (y, x as for saige_fit_ai_reml).
+ * m_grm / m_vr (optional) receive the marker split sizes. */
+int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                                const int64_t* sample_idx, int64_t n, const double* y,
+                                const double* x, int32_t p, int32_t trait, double min_maf,
+                                double max_missing, const saige_ai_reml_config* cfg,
+                                saige_ai_reml_summary* out, double* alpha, double* mu,
+                                double* tau_trace, int64_t* m_grm, int64_t* m_vr);
+
+/* ---------------------------------------------------------------------
+ * Instrumentation (the reference logs per-phase times through `tracing`,
+ * saige-cli/src/main.rs:53-65; here the GPU kernels are timed with CUDA
+ * events on the handle's stream)
+ * ------------------------------------------------------------------- */
+typedef struct {
+  int64_t n_kv;               /* GRM product columns                         */
+  int64_t n_kv_launches;      /* GRM product calls                           */
+  int64_t tc_pass_a_launches; /* tensor-core product, pass u = Z'v           */
+  int64_t tc_pass_b_launches; /* tensor-core product, pass y = Z u / M       */
+  double tc_pass_a_ms;        /* summed device time (profiling on)           */
+  double tc_pass_b_ms;
+  int64_t fp32_launches;      /* FP32 product columns                        */
+  double fp32_ms;
+} saige_grm_stats;
+
+/* Turn per-kernel CUDA-event timing on (1) or off (0) for a handle. */
+int32_t saige_grm_set_profiling(saige_grm* h, int32_t on);
+int32_t saige_grm_get_stats(const saige_grm* h, saige_grm_stats* out);
+int32_t saige_grm_reset_stats(saige_grm* h);
+
+/* Kernels this library has launched in the process so far. */
+int64_t saige_kernel_launches(void);
 
 /* ---------------------------------------------------------------------
  * Synthetic cohorts (seeded; no counterpart in the reference — test and

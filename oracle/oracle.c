@@ -330,6 +330,52 @@ void orc_grm_explicit(const double* z, int64_t n, int64_t m, double* k_out) {
   }
 }
 
+int orc_grm_matvec_f32_packed(const uint8_t* bed_body, int64_t bpm, int64_t n,
+                              const int64_t* rows, int64_t m, const double* af, const double* v,
+                              double* out, int threads) {
+  int nt = 1;
+#ifdef _OPENMP
+  nt = threads > 0 ? threads : omp_get_max_threads();
+#endif
+  float* v32 = (float*)malloc(sizeof(float) * (size_t)n);
+  float* accs = (float*)calloc((size_t)n * (size_t)nt, sizeof(float));
+  for (int64_t i = 0; i < n; ++i) v32[i] = (float)v[i];
+#pragma omp parallel num_threads(nt)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    float* acc = accs + (size_t)tid * (size_t)n;
+#pragma omp for schedule(static)
+    for (int64_t j = 0; j < m; ++j) {
+      float lut[4] = {0.f, 0.f, 0.f, 0.f};
+      const double p = af[j];
+      const double denom = sqrt(2.0 * p * (1.0 - p));
+      if (denom > 1e-10) {
+        const double mean = 2.0 * p;
+        lut[0] = (float)((2.0 - mean) / denom);
+        lut[1] = 0.0f; /* missing -> mean -> 0 */
+        lut[2] = (float)((1.0 - mean) / denom);
+        lut[3] = (float)((0.0 - mean) / denom);
+      }
+      const uint8_t* row = bed_body + rows[j] * bpm;
+      float dot = 0.0f;
+      for (int64_t i = 0; i < n; ++i) dot += lut[(row[i >> 2] >> ((i & 3) * 2)) & 3] * v32[i];
+      for (int64_t i = 0; i < n; ++i) acc[i] += lut[(row[i >> 2] >> ((i & 3) * 2)) & 3] * dot;
+    }
+  }
+  const float scale = 1.0f / (float)m;
+  for (int64_t i = 0; i < n; ++i) {
+    float s = 0.0f;
+    for (int t = 0; t < nt; ++t) s += accs[(size_t)t * (size_t)n + i];
+    out[i] = (double)(s * scale);
+  }
+  free(v32);
+  free(accs);
+  return nt;
+}
+
 /* ===================================================================== */
 /* Dense linear algebra (saige-linalg/src/decomposition.rs)               */
 /* ===================================================================== */

@@ -67,6 +67,14 @@ void orc_grm_standardize(const double* dosages, const double* af, int64_t n, int
                          double* z_out);
 void orc_grm_matvec(const double* z, int64_t n, int64_t m, const double* v, double* out, int mode);
 void orc_grm_explicit(const double* z, int64_t n, int64_t m, double* k_out);
+/* pcg.rs:128-180 arithmetic (f32 z from pcg.rs:101-122, f32 dot and axpy per
+ * marker, one f32 accumulator per thread, summed at the end as rayon's
+ * fold/reduce does) on packed PLINK rows: markers rows[0..m) of the .bed
+ * body (bed points past the 3-byte header), all n_fam samples in order.
+ * threads <= 0 uses every OpenMP thread.  Returns the threads used. */
+int orc_grm_matvec_f32_packed(const uint8_t* bed_body, int64_t bytes_per_marker, int64_t n,
+                              const int64_t* rows, int64_t m, const double* af, const double* v,
+                              double* out, int threads);
 
 /* ---- linear algebra (decomposition.rs:35-89, 212-298) ------------------ */
 int orc_cholesky(const double* a, int p, double* l);
