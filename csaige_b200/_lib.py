@@ -142,6 +142,10 @@ SIGNATURES = {
         C.c_int32,
         [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, _vp],
     ),
+    "saige_grm_matvec_dev_noalloc": (
+        C.c_int32,
+        [_vp, _vp, _vp, C.c_int64, C.c_int32, _vp],
+    ),
     "saige_pcg_solve": (
         C.c_int32,
         [_vp, _d, _d, _d, _d, _d, C.c_int64, C.c_int32, P(PcgOptions), _i32, _d, _u8],

@@ -28,6 +28,7 @@ SOURCES = [
     "kernels_fp32.cu",
     "kernels_vec.cu",
     "kernels_tc.cu",
+    "noalloc.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

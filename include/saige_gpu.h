@@ -147,6 +147,22 @@ int32_t saige_grm_matvec(saige_grm* h, const double* v, double* out, int64_t n, 
 int32_t saige_grm_matvec_dev(saige_grm* h, const double* v_dev, double* out_dev, int64_t n,
                              int32_t nrhs, int32_t precision, void* stream);
 
+/* No counterpart in the reference.  FP32 product like saige_grm_matvec_dev
+ * (same kernels, same results) for callers that cannot let a library call
+ * cudaMalloc: processes whose own pool already holds nearly all of the GPU's
+ * memory, and latency-critical callers that cannot afford the device
+ * synchronisation cudaMalloc/cudaFree may cause.  It allocates nothing: its
+ * scratch is a 32 MiB array compiled into the library, which every GPU that
+ * loads the library holds until the process exits.  The GRM must fit in it
+ * (about 1.5 million samples); larger ones get SAIGE_EINVAL with the sizes in
+ * saige_last_error().  The first call on a device looks up the array's device
+ * address, so make that call before any stream capture.  v_dev/out_dev hold
+ * nrhs columns of n doubles; the work is enqueued on `stream` (NULL: the
+ * handle's stream) and the call returns without waiting for it.  All calls on
+ * one device share the array: calls that overlap on the GPU race. */
+int32_t saige_grm_matvec_dev_noalloc(saige_grm* h, const double* v_dev, double* out_dev,
+                                     int64_t n, int32_t nrhs, void* stream);
+
 /* ---------------------------------------------------------------------
  * PCG solves
  * ------------------------------------------------------------------- */
