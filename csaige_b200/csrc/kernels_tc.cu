@@ -16,20 +16,32 @@
 //   sum_i nm (g - 2p) v = scale (G - 2p (S - Mi)),  G = sum g q, Mi = sum miss q,
 //   S = sum q (exact int64), so the only error is the rounding of v to q.
 //
-// Data movement.  The packed 2-bit rows (HBM, 128-byte aligned) arrive by TMA
-// (2D tensor map, 128 rows x 32 bytes = 128 samples per stage); the quantised
-// vector operand arrives by one bulk copy per stage from an image written
-// already in the swizzled shared-memory layout.  Four warps expand the 2-bit
-// codes into the two int8 operand tiles with byte permutes (PRMT) and write
-// them in the 128-byte-swizzled layout the MMA reads:
-//   pass A: rows = markers (M), 128 samples = K  -> K-major A
-//   pass B: rows = markers (K), 128 samples = M  -> MN-major A
-// Roles: warp 0 issues TMA, warp 1 owns TMEM and issues MMAs, warps 2-5 unpack
-// and then run the epilogue.  Every mbarrier wait is bounded; a wait that runs
-// out sets an error word the host reads back (SAIGE_TIMEOUT).
+// Genotype tiles.  The tensor-core passes read the packed codes as 4 KB tiles
+// (128 rows x 128 K entries, 32 bytes per row) stored contiguously in HBM, so
+// that each pipeline stage is one sequential 4 KB burst:
+//   tiles_m: rows = markers, K = samples  (pass A)
+//   tiles_s: rows = samples, K = markers  (pass B, the transpose)
+// Both use the device word layout of the row-major copy (entry 4j+i of a
+// 16-entry word at bit 16(j>>1) + 2(j&1) + 4i), built once per GRM.
+//
+// Pipeline (one CTA per 128-row tile, K swept in 128-entry stages):
+//   warp 0      bulk-copies the stage's code tile and its vector-limb tile(s)
+//               (written beforehand in the 128-byte-swizzled K-major layout)
+//               into a shared-memory load ring;
+//   warps 2-9   two groups of four warps take alternate stages; each thread
+//               expands its row's 128 codes into 128 int8 genotypes and 128
+//               int8 missing flags with byte permutes and stores them straight
+//               into a TMEM operand slot (tcgen05.st): the A operand never
+//               touches shared memory;
+//   warp 1      issues tcgen05.mma kind::i8 with A from TMEM and B (limbs)
+//               from shared memory, and commits each stage to mbarriers;
+//   warps 2-9   finally run the FP64 epilogue from the TMEM accumulators.
+// Every mbarrier wait is bounded; a wait that runs out sets an error word the
+// host reads back (SAIGE_TIMEOUT).
 #include <cuda.h>
 #include <math.h>
 
+#include <algorithm>
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -41,20 +53,17 @@ namespace saige {
 
 namespace {
 
-constexpr int kRows = 128;     // MMA M: rows of a CTA tile
-constexpr int kKt = 128;       // K per pipeline stage
-constexpr int kMaxSA = 4;         // unpacked int8 operand buffers at most
-constexpr int kMaxSL = 16;       // load-ring stages at most
+constexpr int kRows = 128;                    // MMA M: rows of a CTA tile
+constexpr int kKt = 128;                      // K entries per pipeline stage
+constexpr uint32_t kTileBytes = kRows * kKt / 4;  // 4 KB of 2-bit codes
+constexpr int kMaxSA = 6;                     // TMEM operand slots at most
+constexpr int kMaxSL = 24;                    // load-ring stages at most
 constexpr int kUnpackWarps = 8;
 constexpr int kThreads = 64 + 32 * kUnpackWarps;  // producer warp, MMA warp, 8 unpack warps
 constexpr size_t kSmemBudget = 227 * 1024;
-constexpr int kSparseR = 4;    // capacity of the sparse missing-call correction
-// Launches with r <= kSparseUseR use it.  Measured on B200 at N=200k, M=150k it is
-// slower than the dense indicator product (31 ms vs 13 ms per product at r = 1):
-// nearly every word of a warp holds some missing code, so the divergent scan runs
-// on almost every word.  It stays selectable here; the dense path is the default.
-constexpr int kSparseUseR = 0;
-constexpr int kMaxR = 64;      // right-hand sides per launch (3*64 = 192 <= 256 MMA N)
+constexpr uint32_t kTmemCols = 512;           // the whole TMEM (one CTA per SM)
+constexpr uint32_t kSlotCols = 64;            // per slot: 32 columns of genotypes + 32 of flags
+constexpr int kMaxR = 64;                     // right-hand sides per launch (3*64 = 192 <= 256 MMA N)
 constexpr double kQ = 127.0 * 65536.0;
 constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 
@@ -62,11 +71,12 @@ struct TcArgs {
   int ng;                   // B tile rows (= MMA N), multiple of 16
   int r;                    // right-hand sides in this launch
   int nk;                   // pipeline stages over K
-  int sl;                   // load-ring depth
-  int sa;                   // unpacked-ring depth (2 or 4)
+  int sub;                  // 128-entry sub-stages per load stage (1, 2 or 4)
+  int sl;                   // load-ring depth in load stages (>= 2)
+  int sa;                   // TMEM operand slots, one per sub-stage (even)
+  const uint8_t* tiles;     // this pass's code tiles, tile t at (t*nk + k)*4 KB
   const uint8_t* img_g;     // nk x ng x 128 bytes
-  const uint8_t* img_m;     // pass B, dense: c image (same shape)
-  const int* img_q;         // sparse: exact int32 q, nk x r x 128
+  const uint8_t* img_m;     // pass B: c image (same shape)
   const double* scale_g;    // [r]
   const double* scale_m;    // [r] pass B
   const long long* sum_q;   // [r] pass A: sum q_v; pass B: sum q_c
@@ -135,7 +145,7 @@ __device__ __forceinline__ bool mbar_wait_impl(uint32_t bar, uint32_t parity,
     if (kBackoff) {
       // waiting warps yield their issue slots to the MMA-issuing warp
       __nanosleep(sleep_ns);
-      if (sleep_ns < 256) sleep_ns <<= 1;
+      if (sleep_ns < 128) sleep_ns <<= 1;
     }
     if ((polls & 63u) == 0) {  // the clock and the abort flag are checked every 64 polls
       if (*abort_flag) return false;
@@ -160,15 +170,8 @@ __device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity,
   return mbar_wait_impl<true>(bar, parity, abort_flag, err);
 }
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
-                                            uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
+// Non-tensor bulk copy global -> shared (16-byte aligned addresses, size a
+// multiple of 16), completing on an mbarrier.  No multicast.
 __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
                                           uint32_t bar) {
   asm volatile(
@@ -178,38 +181,57 @@ __device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_
       : "memory");
 }
 
-// Shared-memory matrix descriptor, 128-byte swizzle, version 1 (sm_100).
-// K-major:  SBO = 1024 B between 8-row groups, LBO unused (1).
-// MN-major: SBO = 1024 B between 8-row K groups, one 128-byte atom along M.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr, bool mn_major) {
+// Shared-memory matrix descriptor of a K-major operand in the 128-byte swizzle
+// (version 1, sm_100): SBO = 1024 B between 8-row groups, LBO unused (1).
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
   uint64_t d = 0;
   d |= (uint64_t)((addr >> 4) & 0x3FFFu);
-  d |= (uint64_t)(mn_major ? 64u : 1u) << 16;   // leading byte offset >> 4
-  d |= (uint64_t)64u << 32;                      // stride byte offset (1024) >> 4
-  d |= (uint64_t)1u << 46;                       // version
-  d |= (uint64_t)2u << 61;                       // SWIZZLE_128B
+  d |= (uint64_t)1u << 16;    // leading byte offset >> 4
+  d |= (uint64_t)64u << 32;   // stride byte offset (1024) >> 4
+  d |= (uint64_t)1u << 46;    // version
+  d |= (uint64_t)2u << 61;    // SWIZZLE_128B
   return d;
 }
 
-// Instruction descriptor: kind::i8, s32 accumulate, signed A and B, M = 128.
-__host__ __device__ constexpr uint32_t i8_idesc(int n, bool a_mn_major) {
-  return (2u << 4)                        // c_format = S32
-         | (1u << 7)                      // a_format = signed int8
-         | (1u << 10)                     // b_format = signed int8
-         | ((a_mn_major ? 1u : 0u) << 15) // a_major
-         | (0u << 16)                     // b_major = K
-         | ((uint32_t)(n >> 3) << 17)     // N >> 3
-         | ((uint32_t)(kRows >> 4) << 24);// M >> 4
+// Instruction descriptor: kind::i8, s32 accumulate, signed A and B, both
+// K-major, M = 128.
+__host__ __device__ constexpr uint32_t i8_idesc(int n) {
+  return (2u << 4)                          // c_format = S32
+         | (1u << 7)                        // a_format = signed int8
+         | (1u << 10)                       // b_format = signed int8
+         | ((uint32_t)(n >> 3) << 17)       // N >> 3
+         | ((uint32_t)(kRows >> 4) << 24);  // M >> 4
 }
 
-__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                       uint32_t idesc, uint32_t accumulate) {
+// D[tmem] (+)= A[tmem] * B[smem]
+__device__ __forceinline__ void mma_i8_ts(uint32_t tmem_d, uint32_t tmem_a, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
   const uint32_t z = 0;
   asm volatile(
       "{\n\t.reg .pred p;\n\t"
       "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], [%1], %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+      "r"(tmem_a), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(z), "r"(z), "r"(z), "r"(z));
+}
+
+__device__ __forceinline__ uint4 lds128(uint32_t addr) {
+  uint4 v;
+  asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w)
+               : "r"(addr));
+  return v;
+}
+
+// Named barriers 1..sa hand operand slot ab from its unpack group (four warps,
+// bar.arrive) to the MMA warp (bar.sync).
+constexpr int kHandoffThreads = 32 + 32 * (kUnpackWarps / 2);
+
+__device__ __forceinline__ void named_bar_sync(int id, int nthreads) {
+  asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
+}
+
+__device__ __forceinline__ void named_bar_arrive(int id, int nthreads) {
+  asm volatile("bar.arrive %0, %1;" ::"r"(id), "r"(nthreads) : "memory");
 }
 
 __device__ __forceinline__ void mma_commit(uint32_t bar) {
@@ -232,14 +254,22 @@ __device__ __forceinline__ void tmem_wait_ld() {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Byte-permute selectors of the four 4-sample groups of a device-layout word
-// (sample 4j+i at bit 16*(j>>1) + 2*(j&1) + 4i): one nibble per sample.
-__device__ __forceinline__ void selectors(uint32_t w, uint32_t& s0, uint32_t& s1, uint32_t& s2,
-                                          uint32_t& s3) {
-  s0 = w & 0x3333u;
-  s1 = (w >> 2) & 0x3333u;
-  s2 = (w >> 16) & 0x3333u;
-  s3 = (w >> 18) & 0x3333u;
+// 32 consecutive TMEM columns of this thread's lane <- v[0..31].
+__device__ __forceinline__ void tmem_st32(uint32_t taddr, const uint32_t (&v)[32]) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, "
+      "%29, %30, %31, %32};" ::"r"(taddr),
+      "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]),
+      "r"(v[8]), "r"(v[9]), "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]),
+      "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]), "r"(v[19]), "r"(v[20]), "r"(v[21]),
+      "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]), "r"(v[28]),
+      "r"(v[29]), "r"(v[30]), "r"(v[31])
+      : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory");
 }
 
 // Codes 00,01,10,11 -> genotype bytes {2,0,1,0} and missing bytes {0,1,0,0}.
@@ -247,104 +277,87 @@ constexpr uint32_t kLutG = 0x00010002u;
 constexpr uint32_t kLutM = 0x00000100u;
 
 // Shared-memory plan (1024-byte aligned):
-//   unpacked ring  sa x [A_g 16 KB | A_m 16 KB (dense missing product only)]
-//   load ring      sl x [codes 4 KB | B_g ng*128 | B_m ng*128 (pass B, dense) |
-//                        Q r*512 (sparse: exact int32 q of the stage's 128 entries)]
-//   barriers       FULL[sl] EMPTY_L[sl] UNP[sa] EMPTY_A[sa] ACCF
-//   misc           TMEM address, abort flag, sparse missing sums int64 [128][kSparseR]
-// The load ring runs up to sl stages ahead of the MMA so that HBM latency is
-// covered; two groups of four unpack warps fill alternate unpacked buffers.
-//
-// Missing calls.  Dense: the missing indicator is a second int8 operand and a
-// second MMA (right for many right-hand sides).  Sparse (r <= kSparseR): the
-// unpack threads find the ~1% missing codes with bit tricks and add the exact
-// int32 q of those entries on CUDA cores, which halves the MMAs and drops the
-// indicator tile.
+//   load ring  sl x [codes sub x 4 KB | B_g sub x ng*128 | B_m sub x ng*128 (pass B)]
+//   barriers   FULL[sl] (load stage landed), LDONE[sl] (its MMAs complete),
+//              ADONE[sa] (MMAs reading operand slot complete), ACCF
+//   misc       TMEM address, abort flag
+// A load stage carries `sub` consecutive 128-entry sub-stages in one
+// transaction-counted mbarrier phase: a CTA completes only about one such
+// phase per ~550 cycles on sm_100, so 4 KB phases would cap a CTA near
+// 15 GB/s; 16 KB and more per phase reach HBM speed.
+// TMEM: accumulators G at columns [0, ng), Mi at [ng, 2 ng); operand slots of
+// 64 columns (one sub-stage) from column a0 = round_up(2 ng, 32).
 struct SmemPlan {
-  uint32_t base, a_stage, l_stage, b_bytes, q_off, bars;
-  int sl, sa;
-  __device__ uint32_t A_g(int a) const { return base + (uint32_t)a * a_stage; }
-  __device__ uint32_t A_m(int a) const { return A_g(a) + kRows * kKt; }
-  __device__ uint32_t L(int s) const { return base + (uint32_t)sa * a_stage + (uint32_t)s * l_stage; }
-  __device__ uint32_t CODES(int s) const { return L(s); }
-  __device__ uint32_t B_g(int s) const { return L(s) + kRows * 32u; }
-  __device__ uint32_t B_m(int s) const { return B_g(s) + b_bytes; }
-  __device__ uint32_t Q(int s) const { return L(s) + q_off; }
+  uint32_t base, l_stage, b_bytes, sub, bars;
+  __device__ uint32_t L(int s) const { return base + (uint32_t)s * l_stage; }
+  __device__ uint32_t CODES(int s, int t) const { return L(s) + (uint32_t)t * kTileBytes; }
+  __device__ uint32_t B_g(int s, int t) const {
+    return L(s) + sub * kTileBytes + (uint32_t)t * b_bytes;
+  }
+  __device__ uint32_t B_m(int s, int t) const {
+    return L(s) + sub * (kTileBytes + b_bytes) + (uint32_t)t * b_bytes;
+  }
   __device__ uint32_t FULL(int s) const { return bars + 8u * s; }
-  __device__ uint32_t EMPTY_L(int s) const { return bars + 8u * (kMaxSL + s); }
-  __device__ uint32_t UNP(int a) const { return bars + 8u * (2 * kMaxSL + a); }
-  __device__ uint32_t EMPTY_A(int a) const { return bars + 8u * (2 * kMaxSL + kMaxSA + a); }
-  __device__ uint32_t ACCF() const { return bars + 8u * (2 * kMaxSL + 2 * kMaxSA); }
+  __device__ uint32_t LDONE(int s) const { return bars + 8u * (kMaxSL + s); }
+  __device__ uint32_t ADONE(int a) const { return bars + 8u * (2 * kMaxSL + a); }
+  __device__ uint32_t ACCF() const { return bars + 8u * (2 * kMaxSL + kMaxSA); }
   __device__ uint32_t MISC() const { return ACCF() + 8u; }
-  __device__ uint32_t MACC() const { return MISC() + 16u; }
 };
 
 __host__ __device__ constexpr uint32_t round1k(uint32_t x) { return (x + 1023u) & ~1023u; }
 
-// Offset of the Q tile inside a load stage, and the stage size.
-__host__ __device__ constexpr uint32_t plan_q_off(int ng, bool pass_b, bool sparse) {
-  return kRows * 32u + (uint32_t)ng * kKt * ((pass_b && !sparse) ? 2u : 1u);
-}
-__host__ __device__ constexpr uint32_t plan_l_stage(int ng, int r, bool pass_b, bool sparse) {
-  return round1k(plan_q_off(ng, pass_b, sparse) + (sparse ? (uint32_t)r * 512u : 0u));
-}
-__host__ __device__ constexpr uint32_t plan_a_stage(bool sparse) {
-  return (sparse ? 1u : 2u) * kRows * kKt;
+// bytes of one sub-stage in the load ring
+__host__ __device__ constexpr uint32_t plan_sub_bytes(int ng, bool pass_b) {
+  return kTileBytes + (uint32_t)ng * kKt * (pass_b ? 2u : 1u);
 }
 
-__device__ __forceinline__ int lds_s32(uint32_t addr) {
-  int v;
-  asm volatile("ld.shared.s32 %0, [%1];" : "=r"(v) : "r"(addr));
-  return v;
+__host__ __device__ constexpr uint32_t plan_l_stage(int ng, bool pass_b, int sub) {
+  return round1k((uint32_t)sub * plan_sub_bytes(ng, pass_b));
 }
 
-// Fire-and-forget 64-bit add to shared memory.
-__device__ __forceinline__ void red_add_u64(uint32_t addr, unsigned long long v) {
-  asm volatile("red.shared.add.u64 [%0], %1;" ::"r"(addr), "l"(v) : "memory");
+__host__ __device__ constexpr uint32_t tmem_a0(int ng) { return ((uint32_t)(2 * ng) + 31u) & ~31u; }
+
+// Expands one 16-entry code word into 16 genotype bytes (g[0..3]) and 16
+// missing-flag bytes (m[0..3]), entries in order.  PRMT reads only the low
+// 16 bits of its selector, so each selector is one nibble group.
+__device__ __forceinline__ void expand_word(uint32_t w, uint32_t* g, uint32_t* m) {
+  const uint32_t lo = w & 0x33333333u;         // entries 0-3 (bits 0-15), 8-11 (bits 16-31)
+  const uint32_t hi = (w >> 2) & 0x33333333u;  // entries 4-7, 12-15
+  const uint32_t lo2 = lo >> 16, hi2 = hi >> 16;
+  g[0] = __byte_perm(kLutG, 0u, lo);
+  g[1] = __byte_perm(kLutG, 0u, hi);
+  g[2] = __byte_perm(kLutG, 0u, lo2);
+  g[3] = __byte_perm(kLutG, 0u, hi2);
+  m[0] = __byte_perm(kLutM, 0u, lo);
+  m[1] = __byte_perm(kLutM, 0u, hi);
+  m[2] = __byte_perm(kLutM, 0u, lo2);
+  m[3] = __byte_perm(kLutM, 0u, hi2);
 }
 
-// Sample index (0..15) of the code at even bit p of a device-layout word.
-__device__ __forceinline__ int sample_of_bit(int p) {
-  return ((p >> 4) << 3) | (((p >> 1) & 1) << 2) | ((p >> 2) & 3);
-}
-
-template <bool kPassB, bool kSparse>
-__global__ void __launch_bounds__(kThreads, 1)
-    tc_grm_kernel(const __grid_constant__ CUtensorMap codes_map, TcArgs a) {
+template <bool kPassB>
+__global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
   SmemPlan P;
   P.base = (raw + 1023u) & ~1023u;
   P.b_bytes = (uint32_t)a.ng * kKt;
-  P.a_stage = plan_a_stage(kSparse);
-  P.q_off = plan_q_off(a.ng, kPassB, kSparse);
-  P.l_stage = plan_l_stage(a.ng, a.r, kPassB, kSparse);
-  P.sl = a.sl;
-  P.sa = a.sa;
-  P.bars = P.base + (uint32_t)a.sa * P.a_stage + (uint32_t)a.sl * P.l_stage;
+  P.sub = (uint32_t)a.sub;
+  P.l_stage = plan_l_stage(a.ng, kPassB, a.sub);
+  P.bars = P.base + (uint32_t)a.sl * P.l_stage;
   uint8_t* gen = smem_raw + (P.base - raw);  // generic pointer of P.base
   auto gptr = [&](uint32_t saddr) { return gen + (saddr - P.base); };
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(gptr(P.MISC()));
   volatile int* abort_flag = reinterpret_cast<volatile int*>(gptr(P.MISC() + 8u));
-  unsigned long long* macc = reinterpret_cast<unsigned long long*>(gptr(P.MACC()));
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int tile = blockIdx.x;
-  const uint32_t acc_cols = (kSparse ? 1u : 2u) * (uint32_t)a.ng;
-  uint32_t tmem_cols = 32;
-  while (tmem_cols < acc_cols) tmem_cols <<= 1;
 
-  if (kSparse)
-    for (int e = threadIdx.x; e < kRows * kSparseR; e += kThreads) macc[e] = 0ull;
   if (threadIdx.x == 0) {
     for (int s = 0; s < a.sl; ++s) {
       mbar_init(P.FULL(s), 1);
-      mbar_init(P.EMPTY_L(s), 1);
+      mbar_init(P.LDONE(s), 1);
     }
-    for (int s = 0; s < a.sa; ++s) {
-      mbar_init(P.UNP(s), kUnpackWarps / 2);  // one arrival per warp of the owning group
-      mbar_init(P.EMPTY_A(s), 1);
-    }
+    for (int s = 0; s < a.sa; ++s) mbar_init(P.ADONE(s), 1);
     mbar_init(P.ACCF(), 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -352,7 +365,7 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                      smem_u32(tmem_slot)),
-                 "r"(tmem_cols));
+                 "r"(kTmemCols));
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -360,152 +373,131 @@ __global__ void __launch_bounds__(kThreads, 1)
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = *tmem_slot;
   const uint32_t tmem_g = tmem, tmem_m = tmem + (uint32_t)a.ng;
+  const uint32_t tmem_a = tmem + tmem_a0(a.ng);
 
   if (warp == 0) {
-    // ---------------- producer: codes by TMA, vector tiles by bulk copy ----------------
+    // ---------------- producer: code tiles and limb tiles by bulk copy ----------------
     if (lane == 0) {
-      const uint32_t q_bytes = (uint32_t)a.r * 512u;
-      const uint32_t tx = kRows * 32u + P.b_bytes * ((kPassB && !kSparse) ? 2u : 1u) +
-                          (kSparse ? q_bytes : 0u);
-      int s = 0;
-      uint32_t ph = 0;
-      for (int k = 0; k < a.nk; ++k) {
-        if (k >= a.sl && !mbar_wait_sleep(P.EMPTY_L(s), ph ^ 1u, abort_flag, a.err)) break;
-        trace_mark(a, k, 0);  // load issued
-        mbar_expect_tx(P.FULL(s), tx);
-        // pass A: x = 32-byte column (128 samples) k, y = marker tile;
-        // pass B: x = sample tile, y = marker block k.
-        const int x = kPassB ? tile * 32 : k * 32;
-        const int y = kPassB ? k * kRows : tile * kRows;
-        tma_load_2d(P.CODES(s), &codes_map, x, y, P.FULL(s));
-        bulk_load(P.B_g(s), a.img_g + (size_t)k * P.b_bytes, P.b_bytes, P.FULL(s));
-        if (kPassB && !kSparse)
-          bulk_load(P.B_m(s), a.img_m + (size_t)k * P.b_bytes, P.b_bytes, P.FULL(s));
-        if (kSparse) bulk_load(P.Q(s), a.img_q + (size_t)k * a.r * 128, q_bytes, P.FULL(s));
-        if (++s == a.sl) { s = 0; ph ^= 1u; }
+      const int n_load = (a.nk + a.sub - 1) / a.sub;
+      const uint8_t* codes = a.tiles + (size_t)tile * a.nk * kTileBytes;
+      int S = 0;
+      uint32_t ph = 0;  // (J / sl) & 1
+      for (int J = 0; J < n_load; ++J) {
+        // the slot is free once the MMAs of load stage J - sl completed
+        if (J >= a.sl && !mbar_wait_sleep(P.LDONE(S), ph ^ 1u, abort_flag, a.err)) break;
+        if (J < kTraceStages) trace_mark(a, J, 0);  // load issued
+        const int k0 = J * a.sub;
+        const uint32_t cnt = (uint32_t)min(a.sub, a.nk - k0);
+        mbar_expect_tx(P.FULL(S), cnt * (kTileBytes + P.b_bytes * (kPassB ? 2u : 1u)));
+        bulk_load(P.CODES(S, 0), codes + (size_t)k0 * kTileBytes, cnt * kTileBytes, P.FULL(S));
+        for (uint32_t t = 0; t < cnt; ++t) {  // limb tiles: one copy per sub-stage (<= 24 KB)
+          bulk_load(P.B_g(S, t), a.img_g + (size_t)(k0 + t) * P.b_bytes, P.b_bytes, P.FULL(S));
+          if (kPassB)
+            bulk_load(P.B_m(S, t), a.img_m + (size_t)(k0 + t) * P.b_bytes, P.b_bytes, P.FULL(S));
+        }
+        if (++S == a.sl) { S = 0; ph ^= 1u; }
       }
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
-    if (lane == 0) {
-      const uint32_t idesc = i8_idesc(a.ng, kPassB);
-      int s = 0, ab = 0;
-      uint32_t ph_l = 0, ph_a = 0;  // phase parities of the current load / unpacked slots
-      for (int k = 0; k < a.nk; ++k) {
-        trace_mark(a, k, 6);  // MMA thread reaches the stage
-        if (!mbar_wait(P.UNP(ab), ph_a, abort_flag, a.err)) break;
-        if (!mbar_wait(P.FULL(s), ph_l, abort_flag, a.err)) break;
-        trace_mark(a, k, 4);  // MMA may issue
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint64_t ag = sw128_desc(P.A_g(ab), kPassB);
-        const uint64_t bg = sw128_desc(P.B_g(s), false);
-        const uint64_t am = kSparse ? 0ull : sw128_desc(P.A_m(ab), kPassB);
-        const uint64_t bm = kSparse ? 0ull : sw128_desc(kPassB ? P.B_m(s) : P.B_g(s), false);
+    // The whole warp takes each filled operand slot from its unpack group through
+    // a named barrier and lane 0 issues the stage's MMAs.  The issuing thread
+    // performs no memory access while its MMAs are in flight: on sm_100 such an
+    // access waits for all of them to complete, which would drain the tensor
+    // pipe at every stage.  One commit per stage releases both the load slot
+    // and the operand slot.
+    // Ring positions advance incrementally: no division in the loop.
+    const uint32_t idesc = i8_idesc(a.ng);
+    int t = 0, s = 0, ab = 0;  // sub-stage within the load stage, load slot, operand slot
+    for (int k = 0; k < a.nk; ++k) {
+      // trace stores come from lane 1: a memory access by the issuing lane would drain its MMAs
+      if (lane == 1) {
+        trace_mark(a, k, 6);  // MMA warp reaches the stage
+        if (a.trace && blockIdx.x == 0 && k < kTraceStages)
+          a.trace[k * kTraceSlots + 7] = (unsigned long long)clock64();  // SM clock at the same point
+      }
+      named_bar_sync(1 + ab, kHandoffThreads);
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      if (lane == 1) trace_mark(a, k, 4);  // MMA may issue
+      if (lane == 0) {
+        const uint64_t bg = sw128_desc(P.B_g(s, t));
+        const uint64_t bm = kPassB ? sw128_desc(P.B_m(s, t)) : bg;
+        const uint32_t ag = tmem_a + (uint32_t)ab * kSlotCols, am = ag + 32u;
 #pragma unroll
         for (int kk = 0; kk < kKt / 32; ++kk) {
-          // K advance of 32: 32 bytes along a K-major row, or 32 rows (4 KB) of an MN-major tile
-          const uint64_t da = kPassB ? (uint64_t)(kk * 256) : (uint64_t)(kk * 2);
-          const uint64_t db = (uint64_t)(kk * 2);
+          // K advance of 32 int8: 8 TMEM columns of A, 32 bytes (2 x 16 B) along a B row
           const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
-          mma_i8(tmem_g, ag + da, bg + db, idesc, acc);
-          if (!kSparse) mma_i8(tmem_m, am + da, bm + db, idesc, acc);
-          if (kk == 0) trace_mark(a, k, 7);  // first MMA issued
+          mma_i8_ts(tmem_g, ag + 8u * kk, bg + 2u * kk, idesc, acc);
+          mma_i8_ts(tmem_m, am + 8u * kk, bm + 2u * kk, idesc, acc);
         }
-        mma_commit(P.EMPTY_A(ab));
-        mma_commit(P.EMPTY_L(s));
-        trace_mark(a, k, 5);  // MMAs issued
-        if (++ab == a.sa) { ab = 0; ph_a ^= 1u; }
-        if (++s == a.sl) { s = 0; ph_l ^= 1u; }
+        mma_commit(P.ADONE(ab));
+        if (t == a.sub - 1 || k == a.nk - 1) mma_commit(P.LDONE(s));
       }
-      mma_commit(P.ACCF());
+      __syncwarp();
+      if (lane == 1) trace_mark(a, k, 5);  // MMAs issued
+      if (++t == a.sub) {
+        t = 0;
+        if (++s == a.sl) s = 0;
+      }
+      if (++ab == a.sa) ab = 0;
     }
+    if (lane == 0) mma_commit(P.ACCF());
   } else {
     // ---------------- unpack (warps 2-9) ----------------
     // group 0 (warps 2-5) takes even stages, group 1 (warps 6-9) odd stages;
-    // within a group one thread expands one 32-byte code row (128 entries).
-    const int t = threadIdx.x - 64;  // 0..255
-    const int grp = t >> 7, row = t & 127;
-    const int sw = row & 7;
-    long long ms0 = 0, ms1 = 0, ms2 = 0, ms3 = 0;  // pass A sparse: missing sums of this row
-    int s = grp % a.sl, ab = grp % a.sa;
-    uint32_t ph_l = 0, ph_a = 0;
+    // a warp may only address its own TMEM lane group (warp % 4), so thread
+    // `lane` of warp w expands row 32 (w % 4) + lane.
+    const int grp = (warp - 2) >> 2;
+    const int lg = warp & 3;
+    const int row = lg * 32 + lane;
+    const uint32_t lane_off = (uint32_t)(lg * 32) << 16;
+    bool live = true;  // false once a wait gave up: the remaining stages only hand over
+    // ring positions of sub-stage k, advanced incrementally by 2 (no division in the loop)
+    int t = grp % a.sub, s = (grp / a.sub) % a.sl, ab = grp;
+    uint32_t ph_l = (uint32_t)((grp / a.sub) / a.sl) & 1u;  // phase parity of FULL(s) for k
+    uint32_t ph_a = 0;                                        // (k / sa) & 1
     for (int k = grp; k < a.nk; k += 2) {
-      if (!mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err)) break;
-      if (row == 0) trace_mark(a, k, 1);  // codes landed
-      if (k >= a.sa && !mbar_wait_sleep(P.EMPTY_A(ab), ph_a ^ 1u, abort_flag, a.err)) break;
-      if (row == 0) trace_mark(a, k, 2);  // unpacked buffer free
-      const uint4* crow = reinterpret_cast<const uint4*>(gptr(P.CODES(s)) + row * 32);
-      const uint4 c0 = crow[0], c1 = crow[1];
-      const uint32_t words[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-      uint8_t* ag = gptr(P.A_g(ab)) + row * 128;
-      uint8_t* am = kSparse ? nullptr : gptr(P.A_m(ab)) + row * 128;
-      const uint32_t qt = P.Q(s);  // shared address of the stage's exact int32 q [r][128]
+      if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err);
+      if (live && row == 0) trace_mark(a, k, 1);  // codes landed
+      // operand slot ab is free once the MMAs of its previous use (sub-stage k - sa) completed
+      if (live && k >= a.sa) live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err);
+      live = __all_sync(0xffffffffu, live);  // warp-uniform: the barrier calls below must agree
+      if (live) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (row == 0) trace_mark(a, k, 2);  // operand slot free
+        const uint32_t crow = P.CODES(s, t) + (uint32_t)row * 32u;
+        const uint4 c0 = lds128(crow), c1 = lds128(crow + 16u);
+        const uint32_t words[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+        uint32_t g[32], m[32];
 #pragma unroll
-      for (int c = 0; c < 8; ++c) {  // 16-byte chunk c = entries 16c .. 16c+15
-        uint32_t s0, s1, s2, s3;
-        selectors(words[c], s0, s1, s2, s3);
-        uint4 g;
-        g.x = __byte_perm(kLutG, 0u, s0);
-        g.y = __byte_perm(kLutG, 0u, s1);
-        g.z = __byte_perm(kLutG, 0u, s2);
-        g.w = __byte_perm(kLutG, 0u, s3);
-        const int pos = (c ^ sw) * 16;
-        *reinterpret_cast<uint4*>(ag + pos) = g;
-        if (!kSparse) {
-          uint4 m;
-          m.x = __byte_perm(kLutM, 0u, s0);
-          m.y = __byte_perm(kLutM, 0u, s1);
-          m.z = __byte_perm(kLutM, 0u, s2);
-          m.w = __byte_perm(kLutM, 0u, s3);
-          *reinterpret_cast<uint4*>(am + pos) = m;
-        } else {
-          uint32_t mm = words[c] & ~(words[c] >> 1) & 0x55555555u;  // codes 01
-          while (mm) {
-            const int bit = __ffs(mm) - 1;
-            mm &= mm - 1u;
-            const int j = c * 16 + sample_of_bit(bit);  // entry of the 128 (always a sample)
-            if (!kPassB) {
-              // pass A: the row is a marker, j a sample; Q holds q_v of the stage's samples
-              const uint32_t qa = qt + 4u * (uint32_t)j;
-              ms0 += lds_s32(qa);
-              if (a.r > 1) ms1 += lds_s32(qa + 512u);
-              if (a.r > 2) ms2 += lds_s32(qa + 1024u);
-              if (a.r > 3) ms3 += lds_s32(qa + 1536u);
-            } else {
-              // pass B: the row is a marker (K); Q holds q_c of the stage's markers
-              const uint32_t qa = qt + 4u * (uint32_t)row;
-              const uint32_t ma = P.MACC() + 8u * (uint32_t)(j * kSparseR);
-#pragma unroll
-              for (int r = 0; r < kSparseR; ++r)
-                if (r < a.r)
-                  red_add_u64(ma + 8u * r, (unsigned long long)(long long)lds_s32(qa + 512u * r));
-            }
-          }
-        }
+        for (int c = 0; c < 8; ++c) expand_word(words[c], g + 4 * c, m + 4 * c);
+        const uint32_t slot = tmem_a + lane_off + (uint32_t)ab * kSlotCols;
+        tmem_st32(slot, g);
+        tmem_st32(slot + 32u, m);
+        tmem_wait_st();
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        if (row == 0) trace_mark(a, k, 3);  // unpack done
       }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      __syncwarp();
-      if (lane == 0) mbar_arrive(P.UNP(ab));
-      if (row == 0) trace_mark(a, k, 3);  // unpack done
-      s += 2;
-      if (s >= a.sl) { s -= a.sl; ph_l ^= 1u; }
+      // Every sub-stage is handed over, also after an abort, so that the MMA warp
+      // never waits for an arrival that does not come.  While live, the wait on
+      // ADONE of sub-stage k - sa keeps this group at most one use ahead of the
+      // MMA warp on each named barrier; after an abort bar.sync does that instead.
+      if (live)
+        named_bar_arrive(1 + ab, kHandoffThreads);
+      else
+        named_bar_sync(1 + ab, kHandoffThreads);
+      t += 2;
+      while (t >= a.sub) {
+        t -= a.sub;
+        if (++s == a.sl) { s = 0; ph_l ^= 1u; }
+      }
       ab += 2;
       if (ab >= a.sa) { ab -= a.sa; ph_a ^= 1u; }
     }
-    if (kSparse) {
-      if (!kPassB) {
-        const long long ms[kSparseR] = {ms0, ms1, ms2, ms3};
-#pragma unroll
-        for (int r = 0; r < kSparseR; ++r)
-          if (r < a.r) red_add_u64(P.MACC() + 8u * (uint32_t)(row * kSparseR + r), (unsigned long long)ms[r]);
-      }
-      asm volatile("bar.sync 1, %0;" ::"r"(kUnpackWarps * 32) : "memory");  // unpack warps only
-    }
     // ---------------- epilogue: two warps per TMEM lane group ----------------
     __syncwarp();
-    const int lg = warp & 3;          // TMEM lane group this warp may access
-    const int sub = (warp - 2) >> 2;  // 0 or 1: which half of the column chunks
-    const int trow = lg * 32 + lane;
+    const int sub = grp;  // 0 or 1: which half of the column chunks
+    const int trow = row;
     const bool ok = mbar_wait_sleep(P.ACCF(), 0u, abort_flag, a.err);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int64_t grow = (int64_t)tile * kRows + trow;  // marker (A) or sample (B)
@@ -514,7 +506,6 @@ __global__ void __launch_bounds__(kThreads, 1)
       rowa = a.inv_s[grow];
       rowb = a.two_p[grow];
     }
-    const uint32_t lane_off = (uint32_t)(lg * 32) << 16;
     for (int r0 = 16 * sub; r0 < a.r; r0 += 32) {
       uint32_t g[48], m[48];
 #pragma unroll
@@ -525,11 +516,9 @@ __global__ void __launch_bounds__(kThreads, 1)
           tmem_ld16(tmem_g + lane_off + (uint32_t)col, tv);
 #pragma unroll
           for (int e = 0; e < 16; ++e) g[16 * j + e] = tv[e];
-          if (!kSparse) {
-            tmem_ld16(tmem_m + lane_off + (uint32_t)col, tv);
+          tmem_ld16(tmem_m + lane_off + (uint32_t)col, tv);
 #pragma unroll
-            for (int e = 0; e < 16; ++e) m[16 * j + e] = tv[e];
-          }
+          for (int e = 0; e < 16; ++e) m[16 * j + e] = tv[e];
         }
       }
       tmem_wait_ld();
@@ -540,9 +529,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         if (r >= a.r) break;
         const double G = 65536.0 * (double)(int)g[3 * e] + 256.0 * (double)(int)g[3 * e + 1] +
                          (double)(int)g[3 * e + 2];
-        const double Mi =
-            kSparse ? (double)(long long)macc[trow * kSparseR + (r < kSparseR ? r : 0)]
-                    : 65536.0 * (double)(int)m[3 * e] + 256.0 * (double)(int)m[3 * e + 1] +
+        const double Mi = 65536.0 * (double)(int)m[3 * e] + 256.0 * (double)(int)m[3 * e + 1] +
                           (double)(int)m[3 * e + 2];
         const double S = (double)a.sum_q[r];
         if (!kPassB) {
@@ -564,8 +551,55 @@ __global__ void __launch_bounds__(kThreads, 1)
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
-                 "r"(tmem_cols));
+                 "r"(kTmemCols));
   }
+}
+
+// ---------------------------------------------------------------------------
+// genotype tiles
+// ---------------------------------------------------------------------------
+// Bit offset of entry e (0..15) of a 16-entry word in the device word layout.
+__device__ __forceinline__ int entry_bit(int e) {
+  const int j = e >> 2, i = e & 3;
+  return 16 * (j >> 1) + 2 * (j & 1) + 4 * i;
+}
+
+// tiles_m[(mt * n_kt + kt)] row r = row-major row mt*128 + r, words kt*8 .. kt*8+7.
+__global__ void __launch_bounds__(256)
+    pack_tiles_kernel(const uint32_t* __restrict__ geno, int64_t wpr, int64_t n_kt,
+                      uint8_t* __restrict__ tiles) {
+  const int64_t kt = blockIdx.x, mt = blockIdx.y;
+  const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
+  const uint4 v = *reinterpret_cast<const uint4*>(geno + (mt * kRows + r) * wpr + kt * 8 + half * 4);
+  *reinterpret_cast<uint4*>(tiles + (mt * n_kt + kt) * kTileBytes + r * 32 + half * 16) = v;
+}
+
+// tiles_s[(st * n_mt + mt)] row r = sample st*128 + r, word j = markers
+// mt*128 + 16j .. +15, read from tiles_m[(mt * n_st + st)].
+__global__ void __launch_bounds__(256)
+    transpose_tiles_kernel(const uint8_t* __restrict__ tiles_m, int64_t n_st, int64_t n_mt,
+                           uint8_t* __restrict__ tiles_s) {
+  __shared__ __align__(16) uint32_t src[kTileBytes / 4];
+  __shared__ __align__(16) uint32_t dst[kTileBytes / 4];
+  const int64_t mt = blockIdx.x, st = blockIdx.y;
+  const uint4* s4 = reinterpret_cast<const uint4*>(tiles_m + (mt * n_st + st) * kTileBytes);
+  reinterpret_cast<uint4*>(src)[threadIdx.x] = s4[threadIdx.x];
+  __syncthreads();
+  // output word (r, j): thread handles r = idx & 127, j = idx >> 7 for idx = t, t+256, ...
+  for (int idx = threadIdx.x; idx < kRows * 8; idx += 256) {
+    const int r = idx & 127, j = idx >> 7;
+    const int sb = entry_bit(r & 15);
+    uint32_t w = 0;
+#pragma unroll
+    for (int e = 0; e < 16; ++e) {
+      const uint32_t sw = src[(16 * j + e) * 8 + (r >> 4)];  // marker row 16j+e, sample word r/16
+      w |= ((sw >> sb) & 3u) << entry_bit(e);
+    }
+    dst[r * 8 + j] = w;
+  }
+  __syncthreads();
+  reinterpret_cast<uint4*>(tiles_s + (st * n_mt + mt) * kTileBytes)[threadIdx.x] =
+      reinterpret_cast<const uint4*>(dst)[threadIdx.x];
 }
 
 // ---------------------------------------------------------------------------
@@ -624,6 +658,7 @@ __device__ __forceinline__ void limbs(long long q, int& l2, int& l1, int& l0) {
   l2 = (int)((q1 - l1) >> 8);
 }
 
+// Limb rows 3r, 3r+1, 3r+2 of a stage image (K-major, 128-byte swizzle).
 __device__ __forceinline__ void put_limbs(uint8_t* stage_img, int r, int pos, long long q) {
   int l2, l1, l0;
   limbs(q, l2, l1, l0);
@@ -647,13 +682,13 @@ __device__ __forceinline__ long long block_sum_ll(long long v, long long* sh) {
   return s;
 }
 
-// One block = one 128-row stage of one column: quantise v, write the limbs
+// One block = one 128-entry stage of one column: quantise v, write the limbs
 // into the swizzled stage image, accumulate sum q.
 __global__ void __launch_bounds__(128)
     quant_v_kernel(const double* __restrict__ v, int64_t ld, int64_t len,
                    const int* __restrict__ col_map, const unsigned long long* __restrict__ amax,
                    double* __restrict__ scale_out, uint8_t* __restrict__ img, int ng,
-                   unsigned long long* __restrict__ sum_q, int* __restrict__ qimg) {
+                   unsigned long long* __restrict__ sum_q) {
   __shared__ long long sh[4];
   const int r = blockIdx.y;
   const int64_t stage = blockIdx.x;
@@ -663,7 +698,6 @@ __global__ void __launch_bounds__(128)
   const double x = i < len ? v[(int64_t)col_map[r] * ld + i] : 0.0;
   const long long q = __double2ll_rn(x / sc);
   put_limbs(img + stage * (int64_t)ng * 128, r, pos, q);
-  if (qimg) qimg[(stage * gridDim.y + r) * 128 + pos] = (int)q;
   const long long s = block_sum_ll(q, sh);
   if (threadIdx.x == 0) {
     atomicAdd(&sum_q[r], (unsigned long long)s);
@@ -676,8 +710,7 @@ __global__ void __launch_bounds__(128)
                     const double* __restrict__ two_p, const unsigned long long* __restrict__ amax_w,
                     const unsigned long long* __restrict__ amax_c, double* __restrict__ scale_w,
                     double* __restrict__ scale_c, uint8_t* __restrict__ img_w,
-                    uint8_t* __restrict__ img_c, int ng, unsigned long long* __restrict__ sum_c,
-                    int* __restrict__ qimg_c) {
+                    uint8_t* __restrict__ img_c, int ng, unsigned long long* __restrict__ sum_c) {
   __shared__ long long sh[4];
   const int r = blockIdx.y;
   const int64_t stage = blockIdx.x;
@@ -689,8 +722,7 @@ __global__ void __launch_bounds__(128)
   const long long qw = __double2ll_rn(w / sw);
   const long long qc = __double2ll_rn(c / scc);
   put_limbs(img_w + stage * (int64_t)ng * 128, r, pos, qw);
-  if (img_c) put_limbs(img_c + stage * (int64_t)ng * 128, r, pos, qc);
-  if (qimg_c) qimg_c[(stage * gridDim.y + r) * 128 + pos] = (int)qc;
+  put_limbs(img_c + stage * (int64_t)ng * 128, r, pos, qc);
   const long long s = block_sum_ll(qc, sh);
   if (threadIdx.x == 0) {
     atomicAdd(&sum_c[r], (unsigned long long)s);
@@ -701,106 +733,104 @@ __global__ void __launch_bounds__(128)
   }
 }
 
-size_t tc_fixed_bytes() {
-  return 1024 + 8 * (2 * kMaxSL + 2 * kMaxSA + 1) + 16 + 8 * kRows * kSparseR;
+size_t tc_fixed_bytes() { return 1024 + 8 * (2 * kMaxSL + kMaxSA + 1) + 16; }
+
+struct Rings {
+  int sub, sl, sa;
+};
+
+// Ring shapes for a launch: load stages of up to four sub-stages (16 KB of
+// codes) while at least two such stages fit in shared memory; as many load
+// stages as fit (at most kMaxSL); as many TMEM operand slots as the
+// accumulators leave room for (at most kMaxSA, even, so that each unpack group
+// owns its slots and named barriers).
+Rings tc_rings(int ng, bool pass_b) {
+  Rings g;
+  const size_t room = kSmemBudget - tc_fixed_bytes();
+  g.sub = 4;
+  while (g.sub > 1 && 2 * (size_t)plan_l_stage(ng, pass_b, g.sub) > room) g.sub >>= 1;
+  g.sl = (int)std::min<size_t>(kMaxSL, room / plan_l_stage(ng, pass_b, g.sub));
+  g.sa = std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols)) & ~1;
+  return g;
 }
 
-// Ring depths for a launch: four unpacked buffers when at least four load
-// stages still fit, else two; the load ring takes the rest (at most kMaxSL),
-// rounded down to an even depth so that each unpack group owns the same load
-// slots at every use and its parity waits never skip a phase.
-void tc_rings(int ng, int r, bool pass_b, bool sparse, int& sa, int& sl) {
-  const size_t per = plan_l_stage(ng, r, pass_b, sparse);
-  const size_t a_stage = plan_a_stage(sparse);
-  for (sa = kMaxSA; sa >= 2; sa -= 2) {
-    const size_t room = kSmemBudget - tc_fixed_bytes() - (size_t)sa * a_stage;
-    sl = (int)std::min<size_t>(kMaxSL, room / per) & ~1;
-    if (sl >= 4 || sa == 2) break;
-  }
+size_t tc_smem_bytes(int ng, bool pass_b) {
+  const Rings g = tc_rings(ng, pass_b);
+  return tc_fixed_bytes() + (size_t)g.sl * plan_l_stage(ng, pass_b, g.sub);
 }
-
-size_t tc_smem_bytes(int ng, int r, bool pass_b, bool sparse) {
-  int sa, sl;
-  tc_rings(ng, r, pass_b, sparse, sa, sl);
-  return tc_fixed_bytes() + (size_t)sa * plan_a_stage(sparse) +
-         (size_t)sl * plan_l_stage(ng, r, pass_b, sparse);
-}
-
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 }  // namespace
 
 struct TcPlan {
-  CUtensorMap codes_map;
-  DevBuf img_a, img_w, img_c, img_qa, img_qc, u, scal, cmap, trace;
+  DevBuf tiles_m, tiles_s, img_a, img_w, img_c, u, scal, cmap, trace;
   bool tracing = false;
 };
 
 // Pipeline trace: with SAIGE_TC_TRACE=1 each tensor-core launch records, for
 // CTA 0 and its first stages, when loads were issued and landed, when the
-// unpacked buffer was free and filled, and when MMAs issued; the per-stage
+// operand slot was free and filled, and when MMAs issued; the per-stage
 // offsets (ns from the first load) are printed to stderr.
 static Status trace_dump(TcPlan* p, const char* what, cudaStream_t st) {
   std::vector<unsigned long long> t((size_t)kTraceStages * kTraceSlots);
   SG_CUDA(cudaMemcpyAsync(t.data(), p->trace.ptr, t.size() * 8, cudaMemcpyDeviceToHost, st));
   SG_CUDA(cudaStreamSynchronize(st));
   const unsigned long long t0 = t[0];
-  fprintf(stderr, "[tc trace] %s: stage load landed free filled may-issue issued reach first-pair (ns)\n", what);
+  fprintf(stderr, "[tc trace] %s: stage load landed free filled may-issue issued reach (ns) | SM clock (MHz)\n", what);
   for (int k = 0; k < kTraceStages; k += (k < 8 ? 1 : 8)) {
     fprintf(stderr, "[tc trace] %3d", k);
-    for (int e = 0; e < 8; ++e) {
+    for (int e = 0; e < 7; ++e) {
       const unsigned long long v = t[(size_t)k * kTraceSlots + e];
       fprintf(stderr, " %9lld", v ? (long long)(v - t0) : -1LL);
     }
+    // effective SM clock between the MMA warp's arrivals at stage 0 and stage k
+    const unsigned long long c0 = t[7], ck = t[(size_t)k * kTraceSlots + 7];
+    const unsigned long long g0 = t[6], gk = t[(size_t)k * kTraceSlots + 6];
+    fprintf(stderr, " | %6.0f", (k > 0 && gk > g0) ? (double)(ck - c0) * 1e3 / (double)(gk - g0) : 0.0);
     fprintf(stderr, "\n");
   }
   SG_CUDA(cudaMemsetAsync(p->trace.ptr, 0, t.size() * 8, st));
   return Status();
 }
 
+// Builds the two tile copies of the packed genotypes (marker-major for pass A,
+// sample-major for pass B) from the row-major copy, on the handle's stream.
+static Status build_tiles(saige_grm* h, TcPlan* p) {
+  const int64_t n_mt = h->m_pad / kRows, n_st = h->n_pad / kKt;
+  const size_t bytes = (size_t)n_mt * n_st * kTileBytes;
+  SG_TRY(p->tiles_m.reserve(bytes));
+  SG_TRY(p->tiles_s.reserve(bytes));
+  pack_tiles_kernel<<<dim3((unsigned)n_st, (unsigned)n_mt), 256, 0, h->stream>>>(
+      h->geno, h->wpr, n_st, p->tiles_m.as<uint8_t>());
+  SG_CHECK_LAUNCH();
+  transpose_tiles_kernel<<<dim3((unsigned)n_mt, (unsigned)n_st), 256, 0, h->stream>>>(
+      p->tiles_m.as<uint8_t>(), n_st, n_mt, p->tiles_s.as<uint8_t>());
+  SG_CHECK_LAUNCH();
+  count_launches(2);
+  return Status();
+}
+
 static Status tc_init(saige_grm* h) {
   if (h->tc) return Status();
   TcPlan* p = new TcPlan();
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  SG_CUDA(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
-  if (!fn || q != cudaDriverEntryPointSuccess) {
+  auto bail = [&](Status s) {
     delete p;
-    return fail(SAIGE_ECUDA, "cuTensorMapEncodeTiled is not available");
-  }
-  const cuuint64_t dims[2] = {(cuuint64_t)(h->wpr * 4), (cuuint64_t)h->m_pad};
-  const cuuint64_t strides[1] = {(cuuint64_t)(h->wpr * 4)};
-  const cuuint32_t box[2] = {32, (cuuint32_t)kRows};
-  const cuuint32_t estr[2] = {1, 1};
-  CUresult r = reinterpret_cast<EncodeTiledFn>(fn)(
-      &p->codes_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, (void*)h->geno, dims, strides, box, estr,
-      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-  if (r != CUDA_SUCCESS) {
-    delete p;
-    return fail(SAIGE_ECUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
-  }
-  for (auto kern : {tc_grm_kernel<false, false>, tc_grm_kernel<true, false>,
-                    tc_grm_kernel<false, true>, tc_grm_kernel<true, true>}) {
+    return s;
+  };
+  for (auto kern : {tc_grm_kernel<false>, tc_grm_kernel<true>}) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSmemBudget);
-    if (e != cudaSuccess) {
-      delete p;
-      return fail(SAIGE_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e));
-    }
+    if (e != cudaSuccess)
+      return bail(fail(SAIGE_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e)));
   }
+  Status bs = build_tiles(h, p);
+  if (!bs.ok()) return bail(bs);
   const char* tr = getenv("SAIGE_TC_TRACE");
   p->tracing = tr && tr[0] == '1';
   if (p->tracing) {
     Status ts = p->trace.reserve((size_t)kTraceStages * kTraceSlots * 8);
-    if (!ts.ok()) {
-      delete p;
-      return ts;
-    }
-    SG_CUDA(cudaMemset(p->trace.ptr, 0, (size_t)kTraceStages * kTraceSlots * 8));
+    if (!ts.ok()) return bail(ts);
+    cudaError_t e = cudaMemset(p->trace.ptr, 0, (size_t)kTraceStages * kTraceSlots * 8);
+    if (e != cudaSuccess) return bail(fail(SAIGE_ECUDA, "cudaMemset: %s", cudaGetErrorString(e)));
   }
   h->tc = p;
   return Status();
@@ -840,10 +870,12 @@ static Scal carve(TcPlan* p) {
   return s;
 }
 
-template <bool kPassB, bool kSparse>
-static cudaError_t launch_tc(const TcPlan* p, unsigned grid, const TcArgs& a, cudaStream_t st) {
-  tc_grm_kernel<kPassB, kSparse><<<grid, kThreads, tc_smem_bytes(a.ng, a.r, kPassB, kSparse), st>>>(
-      p->codes_map, a);
+template <bool kPassB>
+static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
+  if (a.sa < 2 || (a.sa & 1) || a.sa > kMaxSA || a.sl < 2 || a.sl > kMaxSL || a.sub < 1 ||
+      a.sub > 4)
+    return cudaErrorInvalidValue;
+  tc_grm_kernel<kPassB><<<grid, kThreads, tc_smem_bytes(a.ng, kPassB), st>>>(a);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -856,16 +888,21 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
   for (int c = 0; c < q; ++c)
     if (!active || active[c] == kColActive) cols.push_back(c);
   if (cols.empty()) return Status();
+  if (st != h->stream) {
+    // the tiles were built on the handle's stream
+    cudaEvent_t built;
+    SG_CUDA(cudaEventCreateWithFlags(&built, cudaEventDisableTiming));
+    SG_CUDA(cudaEventRecord(built, h->stream));
+    SG_CUDA(cudaStreamWaitEvent(st, built, 0));
+    cudaEventDestroy(built);
+  }
   const int64_t n_stages_a = h->n_pad / kKt;  // samples
   const int64_t n_stages_b = h->m_pad / kKt;  // markers
   const int rmax = (int)std::min<size_t>(cols.size(), (size_t)kMaxR);
   const int ng_max = (int)round_up(3 * rmax, 16);
-  const int rq = std::min(rmax, kSparseR);
   SG_TRY(p->img_a.reserve((size_t)h->n_pad * ng_max));
   SG_TRY(p->img_w.reserve((size_t)h->m_pad * ng_max));
   SG_TRY(p->img_c.reserve((size_t)h->m_pad * ng_max));
-  SG_TRY(p->img_qa.reserve((size_t)h->n_pad * rq * sizeof(int)));
-  SG_TRY(p->img_qc.reserve((size_t)h->m_pad * rq * sizeof(int)));
   SG_TRY(p->u.reserve((size_t)h->m_pad * rmax * sizeof(double)));
   SG_TRY(p->scal.reserve(9 * kMaxR * 8 + 64));
   SG_TRY(p->cmap.reserve((size_t)q * sizeof(int) + 64));
@@ -886,7 +923,6 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
   for (size_t c0 = 0; c0 < cols.size(); c0 += kMaxR) {
     const int r = (int)std::min<size_t>(kMaxR, cols.size() - c0);
     const int ng = (int)round_up(3 * r, 16);
-    const bool sparse = r <= kSparseUseR;
     const int* cmap = p->cmap.as<int>() + c0;
     SG_CUDA(cudaMemsetAsync(p->scal.ptr, 0, 5 * kMaxR * 8, st));
     SG_CUDA(cudaMemsetAsync(p->img_a.ptr, 0, (size_t)h->n_pad * ng, st));
@@ -897,8 +933,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       count_launches(2);
       dim3 g2((unsigned)n_stages_a, (unsigned)r);
       quant_v_kernel<<<g2, 128, 0, st>>>(v, h->n_pad, h->n, cmap, sc.amax_v, sc.scale_v,
-                                         p->img_a.as<uint8_t>(), ng, sc.sum_v,
-                                         sparse ? p->img_qa.as<int>() : nullptr);
+                                         p->img_a.as<uint8_t>(), ng, sc.sum_v);
       SG_CHECK_LAUNCH();
     }
     // ---- pass A: u = Z' v ----
@@ -907,9 +942,12 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.ng = ng;
       a.r = r;
       a.nk = (int)n_stages_a;
-      tc_rings(ng, r, false, sparse, a.sa, a.sl);
+      const Rings g = tc_rings(ng, false);
+      a.sub = g.sub;
+      a.sl = g.sl;
+      a.sa = g.sa;
+      a.tiles = p->tiles_m.as<uint8_t>();
       a.img_g = p->img_a.as<uint8_t>();
-      a.img_q = sparse ? p->img_qa.as<int>() : nullptr;
       a.scale_g = sc.scale_v;
       a.sum_q = reinterpret_cast<const long long*>(sc.sum_v);
       a.two_p = h->two_p;
@@ -921,9 +959,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       const unsigned grid = (unsigned)(h->m_pad / kRows);
       cudaEvent_t t0 = nullptr, t1 = nullptr;
       SG_TRY(mark(&t0));
-      const cudaError_t e = sparse ? launch_tc<false, true>(p, grid, a, st)
-                                   : launch_tc<false, false>(p, grid, a, st);
-      SG_CUDA(e);
+      SG_CUDA(launch_tc<false>(grid, a, st));
       SG_TRY(mark(&t1));
       if (h->profiling) ev_a.emplace_back(t0, t1);
       h->stats.tc_pass_a_launches += 1;
@@ -932,7 +968,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     // ---- pass B operands ----
     {
       SG_CUDA(cudaMemsetAsync(p->img_w.ptr, 0, (size_t)h->m_pad * ng, st));
-      if (!sparse) SG_CUDA(cudaMemsetAsync(p->img_c.ptr, 0, (size_t)h->m_pad * ng, st));
+      SG_CUDA(cudaMemsetAsync(p->img_c.ptr, 0, (size_t)h->m_pad * ng, st));
       dim3 g1((unsigned)std::min<int64_t>(ceil_div(h->m_pad, 256), 296), (unsigned)r);
       count_launches(2);
       amax_wc_kernel<<<g1, 256, 0, st>>>(p->u.as<double>(), h->m_pad, h->m_pad, h->inv_s,
@@ -940,9 +976,8 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       dim3 g2((unsigned)n_stages_b, (unsigned)r);
       quant_wc_kernel<<<g2, 128, 0, st>>>(p->u.as<double>(), h->m_pad, h->inv_s, h->two_p,
                                           sc.amax_w, sc.amax_c, sc.scale_w, sc.scale_c,
-                                          p->img_w.as<uint8_t>(),
-                                          sparse ? nullptr : p->img_c.as<uint8_t>(), ng, sc.sum_c,
-                                          sparse ? p->img_qc.as<int>() : nullptr);
+                                          p->img_w.as<uint8_t>(), p->img_c.as<uint8_t>(), ng,
+                                          sc.sum_c);
       SG_CHECK_LAUNCH();
     }
     // ---- pass B: y = Z w / M ----
@@ -951,10 +986,13 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.ng = ng;
       a.r = r;
       a.nk = (int)n_stages_b;
-      tc_rings(ng, r, true, sparse, a.sa, a.sl);
+      const Rings g = tc_rings(ng, true);
+      a.sub = g.sub;
+      a.sl = g.sl;
+      a.sa = g.sa;
+      a.tiles = p->tiles_s.as<uint8_t>();
       a.img_g = p->img_w.as<uint8_t>();
-      a.img_m = sparse ? nullptr : p->img_c.as<uint8_t>();
-      a.img_q = sparse ? p->img_qc.as<int>() : nullptr;
+      a.img_m = p->img_c.as<uint8_t>();
       a.scale_g = sc.scale_w;
       a.scale_m = sc.scale_c;
       a.sum_q = reinterpret_cast<const long long*>(sc.sum_c);
@@ -967,9 +1005,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       const unsigned grid = (unsigned)(h->n_pad / kRows);
       cudaEvent_t t0 = nullptr, t1 = nullptr;
       SG_TRY(mark(&t0));
-      const cudaError_t e = sparse ? launch_tc<true, true>(p, grid, a, st)
-                                   : launch_tc<true, false>(p, grid, a, st);
-      SG_CUDA(e);
+      SG_CUDA(launch_tc<true>(grid, a, st));
       SG_TRY(mark(&t1));
       if (h->profiling) ev_b.emplace_back(t0, t1);
       h->stats.tc_pass_b_launches += 1;
