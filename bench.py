@@ -44,7 +44,19 @@ WORKLOAD = dict(n=200_000, m=150_000, prevalence=0.02, n_covar=10, sib_frac=0.10
 # (one PCG per right-hand side from zero, the A*0 product of each solve, and the
 # 30 probe products repeated every iteration, ai_reml.rs:175-306), measured with
 # the FP32 path of this library; used to extrapolate the CPU per-product time.
-REF_KV_PER_FIT = None  # filled in from a measured plain fit when available
+# Counted from a fit of this library's FP32 path with the reference strategy on the
+# default workload (N=200,000, M=150,000; 2 AI-REML iterations, 172 PCG iterations:
+# 172 + 2*(11+2) + 2*31 = 320, see ref_kv_count); the run without --no-plain
+# recounts it on the spot.
+REF_KV_PER_FIT = 320
+# Markers in the bounded CPU sample (~1.6 GB of packed rows at N=200,000; about a
+# second per product on 16 cores).
+CPU_SAMPLE_MARKERS = 32768
+# DRAM bytes read per marker row by one tensor-core launch (packed genotype tile rows
+# plus the vector-limb tiles), from the ncu capture at N=200,000, m_pad=18,048:
+# pass A 922.8 MB, pass B 928.5 MB.  Reads scale with m_pad; the output writes
+# (pass A: m_pad*R*8 bytes, pass B: N*R*8 bytes) are added per launch.
+TC_READ_PER_MARKER_ROW = {"A": 922.8e6 / 18048, "B": 928.5e6 / 18048}
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 
@@ -131,6 +143,23 @@ def dist_setup():
     return world, rank, local
 
 
+def reduce_max(x: float, world: int, device: str) -> float:
+    """Maximum of x over all ranks (device "cuda" under NCCL, "cpu" under gloo)."""
+    if world == 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_seconds_per_fit(step_max_s: float, world: int) -> float:
+    """N replicas each fit their own cohort in one step: the job completes N fits
+    in the slowest rank's step time."""
+    return step_max_s / world
+
+
 def ref_kv_count(iterations: int, p: int, nrv: int, pcg_iters: int, solves_per_iter: int) -> int:
     """GRM products of the reference strategy: PCG iterations, one A*0 product
     per solve, and K*Py plus the probe products every iteration."""
@@ -140,49 +169,61 @@ def ref_kv_count(iterations: int, p: int, nrv: int, pcg_iters: int, solves_per_i
 # ---------------------------------------------------------------------------
 # reference arm: CPU restatement, bounded marker sample, extrapolated
 # ---------------------------------------------------------------------------
-def cpu_kv_seconds(n: int, m_full: int, sample_markers: int, reps: int):
-    sys.path.insert(0, str(ROOT / "tests"))
-    import numpy as np
+class CpuSample:
+    """The oracle's packed f32 OnTheFlyGrm::mat_vec (saige-core/src/glmm/pcg.rs:128-180
+    arithmetic, per-thread fold, all host threads) on `markers` synthetic markers of
+    the workload's cohort; products are timed and extrapolated to m_full markers."""
 
-    import csaige_b200 as cs
-    import oracle_ffi as O
+    def __init__(self, n: int, markers: int):
+        sys.path.insert(0, str(ROOT / "tests"))
+        import numpy as np
 
-    O.L.orc_grm_matvec_f32_packed.restype = C.c_int
-    O.L.orc_grm_matvec_f32_packed.argtypes = [C.POINTER(C.c_uint8), C.c_int64, C.c_int64,
-                                              C.POINTER(C.c_int64), C.c_int64, O._d, O._d, O._d,
-                                              C.c_int]
-    spec = cs.CohortSpec(n=n, m=sample_markers, seed=WORKLOAD["seed"],
-                         sib_frac=WORKLOAD["sib_frac"], cousin_frac=WORKLOAD["cousin_frac"],
-                         missing_rate=WORKLOAD["missing_rate"])
-    bed = cs.gen_bed(spec)
-    af, _, _ = O.marker_stats(bed, n, sample_markers)
-    body = np.ascontiguousarray(bed[3:])
-    rows = np.arange(sample_markers, dtype=np.int64)
-    v = np.random.default_rng(1).standard_normal(n)
-    out = np.empty(n)
-    bpm = (n + 3) // 4
-    times = []
-    threads = 0
-    for _ in range(reps):
+        import csaige_b200 as cs
+        import oracle_ffi as O
+
+        O.L.orc_grm_matvec_f32_packed.restype = C.c_int
+        O.L.orc_grm_matvec_f32_packed.argtypes = [C.POINTER(C.c_uint8), C.c_int64, C.c_int64,
+                                                  C.POINTER(C.c_int64), C.c_int64, O._d, O._d,
+                                                  O._d, C.c_int]
+        self.O, self.np = O, np
+        self.n, self.markers = n, markers
+        spec = cs.CohortSpec(n=n, m=markers, seed=WORKLOAD["seed"],
+                             sib_frac=WORKLOAD["sib_frac"], cousin_frac=WORKLOAD["cousin_frac"],
+                             missing_rate=WORKLOAD["missing_rate"])
+        bed = cs.gen_bed(spec)  # host generator, no GPU
+        self.af, _, _ = O.marker_stats(bed, n, markers)
+        self.body = np.ascontiguousarray(bed[3:])
+        self.rows = np.arange(markers, dtype=np.int64)
+        self.v = np.random.default_rng(1).standard_normal(n)
+        self.out = np.empty(n)
+        self.threads = 0
+
+    def product_seconds(self) -> float:
+        """Seconds of one product over the sample."""
+        O = self.O
         t0 = time.perf_counter()
-        threads = O.L.orc_grm_matvec_f32_packed(body.ctypes.data_as(C.POINTER(C.c_uint8)), bpm, n,
-                                                rows.ctypes.data_as(C.POINTER(C.c_int64)),
-                                                sample_markers, O.dp(af), O.dp(v), O.dp(out), 0)
-        times.append(time.perf_counter() - t0)
-    per_kv = statistics.median(times) * m_full / sample_markers
-    return per_kv, threads, times
+        self.threads = O.L.orc_grm_matvec_f32_packed(
+            self.body.ctypes.data_as(C.POINTER(C.c_uint8)), (self.n + 3) // 4, self.n,
+            self.rows.ctypes.data_as(C.POINTER(C.c_int64)), self.markers, O.dp(self.af),
+            O.dp(self.v), O.dp(self.out), 0)
+        return time.perf_counter() - t0
+
+    def describe(self, m_full: int, kv_fit: int) -> str:
+        return (f"OnTheFlyGrm::mat_vec arithmetic (f32, per-thread fold) on {self.markers} of "
+                f"{m_full} markers x {self.n} samples, extrapolated x{m_full / self.markers:.1f} "
+                f"per product and x{kv_fit} products per fit (reference strategy count)")
 
 
 def run_reference(args, rank):
+    """The reference's strategy on the host cores: each step times one product of the
+    oracle over a bounded marker sample and extrapolates to a whole fit."""
     if rank != 0:
         return
+    smp = CpuSample(args.n, min(CPU_SAMPLE_MARKERS, args.m))
     steps = []
-    sample = 2048
-    per_kv = threads = None
-    kv_fit = _plain_kv_estimate()
     for _ in range(args.warmup + args.steps):
-        per_kv, threads, _ = cpu_kv_seconds(args.n, args.m, sample, 1)
-        steps.append(per_kv * kv_fit)
+        per_kv = smp.product_seconds() * args.m / smp.markers
+        steps.append(per_kv * REF_KV_PER_FIT)
     timed = steps[args.warmup:]
     val = statistics.median(timed)
     line = {
@@ -190,25 +231,12 @@ def run_reference(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": val * 1e3,
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": _config(args),
-        "cpu_baseline": {"value": val, "unit": "s", "cores": threads, "kind": "port",
-                         "sample": f"OnTheFlyGrm::mat_vec arithmetic on {sample} of {args.m} "
-                                   f"markers x {args.n} samples, x{args.m / sample:.1f} per "
-                                   f"product, x{kv_fit} products per fit",
-                         "sec_per_kv": per_kv},
+        "cpu_baseline": {"value": val, "unit": "s", "cores": smp.threads, "kind": "port",
+                         "sample": smp.describe(args.m, REF_KV_PER_FIT),
+                         "sec_per_kv": val / REF_KV_PER_FIT},
         "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
-
-
-def _plain_kv_estimate() -> int:
-    """GRM products of one reference-strategy fit on this workload (see
-    profiles/plain_fit_n200k_m150k.txt); 0 when unknown."""
-    p = ROOT / "profiles" / "plain_fit_n200k_m150k.txt"
-    if p.exists():
-        for ln in p.read_text().splitlines():
-            if ln.startswith("reference_kv_per_fit"):
-                return int(ln.split("=")[1])
-    return 0
 
 
 def _config(args):
@@ -279,11 +307,7 @@ def run_ours(args, world, rank, local):
     st = grm.stats()
     grm.set_profiling(False)
     dev_s = [r.seconds for r in results]
-    step_s = statistics.mean(dev_s)
-    if world > 1:
-        t = torch.tensor([step_s], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        step_s = float(t.item())
+    step_s = reduce_max(statistics.mean(dev_s), world, "cuda")  # device time, max over ranks
     last = results[-1]
 
     # roofline of the dominant tensor-core pass, from the live CUDA-event timing
@@ -308,14 +332,19 @@ def run_ours(args, world, rank, local):
         roof = {"bound": "tensor", "achieved": flops_launch / avg_s / 1e12, "peak": int8_peak_tops,
                 "unit": "TFLOP/s"}
     roof["frac"] = roof["achieved"] / roof["peak"]
-    roof["traffic"] = None
+    # per-launch DRAM traffic: measured read bytes per marker row scaled to this m_pad,
+    # plus the launch's output writes
+    m_pad = -(-m_grm // 128) * 128
+    out_bytes = (m_pad if dom == "A" else n) * cols * 8
+    roof["traffic"] = TC_READ_PER_MARKER_ROW[dom] * m_pad + out_bytes
     roof["kernel"] = f"tc_grm_kernel pass {dom} (MIXED, {cols:.1f} rhs per launch)"
     roof["peak_source"] = (f"{pk_kind} MEASURED_PEAKS.json" if pk_kind == "measured" else "fallback")
     roof["avg_launch_ms"] = avg_s * 1e3
     roof["share_of_step"] = (st["tc_pass_a_ms"] + st["tc_pass_b_ms"]) / 1e3 / (step_s * args.steps)
 
     line = {
-        "metric": METRIC, "value": step_s, "unit": "s", "n_gpus": world, "steps": args.steps,
+        "metric": METRIC, "value": whole_job_seconds_per_fit(step_s, world), "unit": "s",
+        "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": step_s * 1e3, "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "int8 tensor products, f64 solver",
         "data": "synthetic", "config": _config(args),
@@ -336,7 +365,8 @@ def run_ours(args, world, rank, local):
             t0 = time.perf_counter()
             fr = cs.fit_null_from_bed(hb, n, m, y, x, cs.TraitType.Binary, fast)
             e2e_t.append(time.perf_counter() - t0)
-        line["e2e"] = {"value": statistics.mean(e2e_t), "unit": "s",
+        e2e_s = reduce_max(statistics.mean(e2e_t), world, "cuda")
+        line["e2e"] = {"value": whole_job_seconds_per_fit(e2e_s, world), "unit": "s",
                        "h2d_bytes_per_step": int(spec.bed_len + y.nbytes + x.nbytes),
                        "d2h_bytes_per_step": int(8 * (p + n + 2 * fast.max_iter)),
                        "tau": [float(fr.ai_reml.tau[0]), float(fr.ai_reml.tau[1])]}
@@ -358,15 +388,13 @@ def run_ours(args, world, rank, local):
         line["tau_rel_diff_vs_plain"] = abs(float(last.tau[1]) - float(pr.tau[1])) / abs(float(pr.tau[1]))
     # CPU baseline (rank 0): bounded sample, extrapolated with the reference product count
     if rank == 0 and world == 1:
-        kv_fit = plain_kv or _plain_kv_estimate()
-        if kv_fit:
-            per_kv, threads, times = cpu_kv_seconds(n, m, 2048, 3)
-            line["cpu_baseline"] = {
-                "value": per_kv * kv_fit, "unit": "s", "cores": threads, "kind": "port",
-                "sample": f"OnTheFlyGrm::mat_vec arithmetic (f32, per-thread fold) on 2048 of {m} "
-                          f"markers x {n} samples, extrapolated x{m / 2048:.1f} per product and "
-                          f"x{kv_fit} products per fit (reference strategy count)",
-                "sec_per_kv": per_kv}
+        kv_fit = plain_kv or REF_KV_PER_FIT
+        smp = CpuSample(n, min(CPU_SAMPLE_MARKERS, m))
+        times = [smp.product_seconds() for _ in range(3)]
+        per_kv = statistics.median(times) * m / smp.markers
+        line["cpu_baseline"] = {
+            "value": per_kv * kv_fit, "unit": "s", "cores": smp.threads, "kind": "port",
+            "sample": smp.describe(m, kv_fit), "sec_per_kv": per_kv}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
