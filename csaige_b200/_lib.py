@@ -142,6 +142,8 @@ SIGNATURES = {
         C.c_int32,
         [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, _vp],
     ),
+    "saige_release_cached_memory": (C.c_int32, []),
+    "saige_rademacher_probes": (C.c_int32, [C.c_uint64, C.c_int32, C.c_int64, _d, C.c_int32]),
     "saige_grm_matvec_dev_noalloc": (
         C.c_int32,
         [_vp, _vp, _vp, C.c_int64, C.c_int32, _vp],

@@ -104,6 +104,19 @@ def bed_marker_stats_dev(bed_ptr: int, bed_len: int, n_fam: int, m_tot: int,
     return af, mac, nv
 
 
+def release_cached_memory() -> None:
+    """Frees the library's cached large device blocks (see saige_release_cached_memory)."""
+    check(LIB.saige_release_cached_memory())
+
+
+def rademacher_probes(seed: int, n_vec: int, n: int, device: int = -1) -> np.ndarray:
+    """The +1/-1 probe vectors of fit_ai_reml (ai_reml.rs:121-130), shape (n_vec, n),
+    generated on the GPU from the ChaCha8Rng::seed_from_u64(seed) stream."""
+    out = np.empty((n_vec, n))
+    check(LIB.saige_rademacher_probes(seed, n_vec, n, _dptr(out), device))
+    return out
+
+
 def select_grm_markers(af, mac, n_valid, n: int, min_maf: float = 0.01,
                        max_missing: float = 0.15, seed: int = 12345):
     """(grm_idx, vr_idx): QC plus the variance-ratio marker split of fit-null."""

@@ -5,6 +5,8 @@
 #include <string.h>
 
 #include <cstdlib>
+#include <chrono>
+#include <cstdlib>
 #include <vector>
 
 #include "engine.cuh"
@@ -147,10 +149,31 @@ SG_API void saige_ai_reml_config_default(saige_ai_reml_config* c) {
   c->reserved = 0;
 }
 
+// With SAIGE_TIMING=1 in the environment, saige_fit_null_from_bed and the AI-REML
+// fit print the wall time of each phase (device synchronised at each mark) to stderr.
+struct PhaseTimer {
+  bool on = false;
+  std::chrono::steady_clock::time_point t0;
+  PhaseTimer() {
+    const char* e = getenv("SAIGE_TIMING");
+    on = e && e[0] == '1';
+    t0 = std::chrono::steady_clock::now();
+  }
+  void mark(const char* what) {
+    if (!on) return;
+    cudaDeviceSynchronize();
+    const auto t1 = std::chrono::steady_clock::now();
+    fprintf(stderr, "[saige timing] %-10s %8.2f ms\n", what,
+            std::chrono::duration<double, std::milli>(t1 - t0).count());
+    t0 = t1;
+  }
+};
+
 static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n, int32_t p,
                        int32_t trait, const saige_ai_reml_config* cfg, saige_ai_reml_summary* out,
                        double* alpha_out, double* mu_out, double* eta_out, double* w_out,
                        double* tau_trace) {
+  PhaseTimer tm;
   Fit f;
   f.h = h;
   f.st = h->stream;
@@ -192,6 +215,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   if (base != vec_end || ci != sizeof(cols) / sizeof(cols[0])) std::abort();
   f.dsmall = base;
   f.partial = base + small / 8;
+  tm.mark("  setup");
 
   cudaEvent_t e0, e1;
   SG_CUDA(cudaEventCreate(&e0));
@@ -230,21 +254,18 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
 
   // ---- probes (ai_reml.rs:121-130), fixed for the whole fit ------------
   {
-    std::vector<uint8_t> signs((size_t)f.nrv * n);
-    ChaCha8 rng(cfg->seed);
-    for (size_t k = 0; k < signs.size(); ++k) signs[k] = rng.gen_bool() ? 1 : 0;
-    DevBuf ds;
-    SG_TRY(ds.reserve(signs.size()));
-    SG_CUDA(cudaMemcpyAsync(ds.ptr, signs.data(), signs.size(), cudaMemcpyHostToDevice, f.st));
+    // the ChaCha8 stream is counter based: the probe matrix is generated on the GPU
+    const ChaCha8 rng(cfg->seed);
     double* u = f.rhs + (size_t)(1 + p) * ld;
-    SG_CUDA(expand_signs(ds.as<uint8_t>(), u, n, ld, f.nrv, f.st));
-    SG_CUDA(cudaStreamSynchronize(f.st));
+    SG_CUDA(rademacher_probes_dev(rng.key(), u, n, ld, f.nrv, f.st));
   }
   double* U = f.rhs + (size_t)(1 + p) * ld;
   SG_CUDA(cudaMemcpy2DAsync(f.rhs + ld, (size_t)ld * 8, f.x, (size_t)ld * 8, (size_t)ld * 8,
                             (size_t)p, cudaMemcpyDeviceToDevice, f.st));
   // K u is the same every iteration (K and the probes are fixed): one block product.
+  tm.mark("  irls");
   SG_TRY(grm_product(h, U, f.ku, f.nrv, nullptr, cfg->precision, f.st));
+  tm.mark("  Ku");
 
   const bool fix_tau_e = trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL;
   double tau[2] = {1.0, 0.0};
@@ -389,6 +410,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   // final W, log-likelihood (ai_reml.rs:393-414)
   SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, nullptr, n, f.st));
   SG_CUDA(cudaEventRecord(e1, f.st));
+  tm.mark("  iters");
   std::vector<double> mu((size_t)n), yh(y, y + n);
   SG_CUDA(cudaMemcpyAsync(mu.data(), f.mu, (size_t)n * 8, cudaMemcpyDeviceToHost, f.st));
   if (eta_out) SG_CUDA(cudaMemcpyAsync(eta_out, f.eta, (size_t)n * 8, cudaMemcpyDeviceToHost, f.st));
@@ -406,6 +428,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
       ll += yh[(size_t)i] * log(mi) + (1.0 - yh[(size_t)i]) * log(1.0 - mi);
     }
   }
+  tm.mark("  loglik");
   float ms = 0.f;
   SG_CUDA(cudaEventElapsedTime(&ms, e0, e1));
   cudaEventDestroy(e0);
@@ -467,17 +490,21 @@ SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64
     if (cfg) c = *cfg;
     else saige_ai_reml_config_default(&c);
     if (bed_len < 3) return fail(SAIGE_EBED, "Bed file too small").code;
+    PhaseTimer tm;
     // one upload of the .bed (fit_null.rs:118 maps it once as well)
     DevBuf d_bed;
     Status s = d_bed.reserve(bed_len);
     if (!s.ok()) return s.code;
+    tm.mark("alloc bed");
     if (cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice) != cudaSuccess)
       return fail(SAIGE_ECUDA, "bed upload failed: %s", cudaGetErrorString(cudaGetLastError())).code;
+    tm.mark("upload");
     std::vector<double> af((size_t)m_tot), mac((size_t)m_tot);
     std::vector<int64_t> nv((size_t)m_tot);
     int32_t rc = saige_bed_marker_stats_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx,
                                             n, af.data(), mac.data(), nv.data());
     if (rc != SAIGE_OK) return rc;
+    tm.mark("counts");
     std::vector<int64_t> gidx((size_t)m_tot), vidx((size_t)m_tot);
     int64_t m_grm = 0, m_vr = 0;
     rc = saige_select_grm_markers(af.data(), mac.data(), nv.data(), m_tot, n, min_maf, max_missing,
@@ -485,15 +512,20 @@ SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64
     if (rc != SAIGE_OK) return rc;
     if (m_grm_out) *m_grm_out = m_grm;
     if (m_vr_out) *m_vr_out = m_vr;
+    tm.mark("select");
     std::vector<double> gaf((size_t)m_grm);
     for (int64_t j = 0; j < m_grm; ++j) gaf[(size_t)j] = af[(size_t)gidx[(size_t)j]];
     saige_grm* h = nullptr;
     rc = saige_grm_create_from_bed_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx, n,
                                        gidx.data(), m_grm, gaf.data(), -1, &h);
     if (rc != SAIGE_OK) return rc;
+    tm.mark("grm");
     d_bed.release();  // the handle holds the packed GRM rows
+    tm.mark("free bed");
     rc = saige_fit_ai_reml(h, y, x, n, p, trait, &c, out, alpha, mu, nullptr, nullptr, tau_trace);
+    tm.mark("fit");
     saige_grm_destroy(h);
+    tm.mark("destroy");
     return rc;
   } catch (const std::bad_alloc&) {
     return fail(SAIGE_ENOMEM, "host allocation failed").code;

@@ -36,11 +36,74 @@ Status fail(int32_t code, const char* fmt, ...) {
   return Status(code);
 }
 
+namespace {
+struct CachedBlock {
+  int dev;
+  size_t bytes;
+  void* ptr;
+};
+std::mutex g_cache_mu;
+std::vector<CachedBlock> g_cache;
+
+// Takes the smallest cached block of `dev` with want <= bytes <= 1.25 want.
+bool cache_take(int dev, size_t want, void** ptr, size_t* bytes) {
+  std::lock_guard<std::mutex> lk(g_cache_mu);
+  size_t best = g_cache.size();
+  for (size_t i = 0; i < g_cache.size(); ++i) {
+    const CachedBlock& b = g_cache[i];
+    if (b.dev == dev && b.bytes >= want && b.bytes <= want + want / 4 &&
+        (best == g_cache.size() || b.bytes < g_cache[best].bytes))
+      best = i;
+  }
+  if (best == g_cache.size()) return false;
+  *ptr = g_cache[best].ptr;
+  *bytes = g_cache[best].bytes;
+  g_cache.erase(g_cache.begin() + (std::ptrdiff_t)best);
+  return true;
+}
+
+// Frees every cached block of `dev` (all devices when dev < 0); returns how many.
+size_t cache_flush(int dev) {
+  std::vector<CachedBlock> out;
+  {
+    std::lock_guard<std::mutex> lk(g_cache_mu);
+    for (size_t i = 0; i < g_cache.size();) {
+      if (dev < 0 || g_cache[i].dev == dev) {
+        out.push_back(g_cache[i]);
+        g_cache.erase(g_cache.begin() + (std::ptrdiff_t)i);
+      } else {
+        ++i;
+      }
+    }
+  }
+  int cur = -1;
+  cudaGetDevice(&cur);
+  for (const CachedBlock& b : out) {
+    cudaSetDevice(b.dev);
+    cudaFree(b.ptr);
+  }
+  if (cur >= 0) cudaSetDevice(cur);
+  return out.size();
+}
+}  // namespace
+
+void release_cached_blocks() { cache_flush(-1); }
+
 Status DevBuf::reserve(size_t want) {
   if (want <= bytes) return Status();
   release();
   if (want == 0) return Status();
+  int d = 0;
+  if (cudaGetDevice(&d) != cudaSuccess) d = 0;
+  if (want >= kCacheMinBytes && cache_take(d, want, &ptr, &bytes)) {
+    dev = d;
+    return Status();
+  }
   cudaError_t e = cudaMalloc(&ptr, want);
+  if (e == cudaErrorMemoryAllocation && cache_flush(d) > 0) {
+    (void)cudaGetLastError();
+    e = cudaMalloc(&ptr, want);
+  }
   if (e != cudaSuccess) {
     ptr = nullptr;
     bytes = 0;
@@ -48,13 +111,28 @@ Status DevBuf::reserve(size_t want) {
     return fail(SAIGE_ENOMEM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
   }
   bytes = want;
+  dev = d;
   return Status();
 }
 
 void DevBuf::release() {
-  if (ptr) cudaFree(ptr);
+  if (ptr) {
+    if (bytes >= kCacheMinBytes && dev >= 0) {
+      // as cudaFree would, wait for the device's work before the block can be reused
+      int cur = -1;
+      cudaGetDevice(&cur);
+      if (cur != dev) cudaSetDevice(dev);
+      cudaDeviceSynchronize();
+      if (cur >= 0 && cur != dev) cudaSetDevice(cur);
+      std::lock_guard<std::mutex> lk(g_cache_mu);
+      g_cache.push_back(CachedBlock{dev, bytes, ptr});
+    } else {
+      cudaFree(ptr);
+    }
+  }
   ptr = nullptr;
   bytes = 0;
+  dev = -1;
 }
 
 // ---------------------------------------------------------------------------
@@ -120,7 +198,8 @@ static Status grm_alloc(saige_grm* h, int64_t n, int64_t m) {
   h->m = m;
   h->m_pad = round_up(std::max<int64_t>(m, 1), kMarkerPad);
   SG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
-  SG_CUDA(cudaMalloc(&h->geno, (size_t)h->m_pad * h->wpr * 4));
+  SG_TRY(h->geno_buf.reserve((size_t)h->m_pad * h->wpr * 4));
+  h->geno = h->geno_buf.as<uint32_t>();
   SG_CUDA(cudaMalloc(&h->zlut, (size_t)h->m_pad * sizeof(float4)));
   SG_CUDA(cudaMalloc(&h->two_p, (size_t)h->m_pad * sizeof(double)));
   SG_CUDA(cudaMalloc(&h->inv_s, (size_t)h->m_pad * sizeof(double)));
@@ -165,7 +244,8 @@ static void grm_free(saige_grm* h) {
   h->ws_red.release();
   h->ws_cols.release();
   h->ws_io.release();
-  if (h->geno) cudaFree(h->geno);
+  h->geno_buf.release();
+  h->geno = nullptr;
   if (h->zlut) cudaFree(h->zlut);
   if (h->two_p) cudaFree(h->two_p);
   if (h->inv_s) cudaFree(h->inv_s);
@@ -519,6 +599,33 @@ SG_API int32_t saige_grm_reset_stats(saige_grm* h) {
 }
 
 SG_API int64_t saige_kernel_launches(void) { return launches_total(); }
+
+SG_API int32_t saige_release_cached_memory(void) {
+  SG_GUARD_BEGIN
+  release_cached_blocks();
+  return SAIGE_OK;
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_rademacher_probes(uint64_t seed, int32_t n_vec, int64_t n, double* out,
+                                      int32_t device) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!out || n_vec <= 0 || n <= 0) return fail(SAIGE_EINVAL, "null argument or empty size").code;
+  int dev = 0;
+  Status ps = pick_device(device, &dev);
+  if (!ps.ok()) return ps.code;
+  auto body = [&]() -> Status {
+    DevBuf d;
+    SG_TRY(d.reserve((size_t)n_vec * n * sizeof(double)));
+    const ChaCha8 rng(seed);
+    SG_CUDA(rademacher_probes_dev(rng.key(), d.as<double>(), n, n, n_vec, 0));
+    SG_CUDA(cudaMemcpy(out, d.ptr, (size_t)n_vec * n * sizeof(double), cudaMemcpyDeviceToHost));
+    return Status();
+  };
+  return body().code;
+  SG_GUARD_END
+}
 
 SG_API int32_t saige_select_grm_markers(const double* af, const double* mac,
                                         const int64_t* n_valid, int64_t m_tot, int64_t n,

@@ -13,14 +13,24 @@
 namespace saige {
 
 // Growable device buffer.
+// Device buffer.  Blocks of at least kCacheMinBytes go through a per-device cache:
+// release() keeps them (after synchronising their device, as cudaFree would) and
+// reserve() reuses a cached block of the same device of 1 to 1.25 times the size,
+// so that repeated fits of one cohort shape do not map and unmap tens of GB each
+// time.  release_cached_blocks() hands the cache back to the driver.
+constexpr size_t kCacheMinBytes = (size_t)256 << 20;
+
 struct DevBuf {
   void* ptr = nullptr;
   size_t bytes = 0;
+  int dev = -1;
   Status reserve(size_t want);
   void release();
   template <class T> T* as() const { return static_cast<T*>(ptr); }
   ~DevBuf() { release(); }
 };
+
+void release_cached_blocks();
 
 struct TcPlan;  // tensor-core path state (kernels_tc.cu)
 
@@ -32,7 +42,8 @@ struct saige_grm {
   std::recursive_mutex mu;
   int64_t n = 0, n_pad = 0, wpr = 0;  // samples, padded samples, 32-bit words per row
   int64_t m = 0, m_pad = 0;           // markers, padded markers
-  uint32_t* geno = nullptr;           // m_pad x wpr packed 2-bit codes
+  uint32_t* geno = nullptr;           // m_pad x wpr packed 2-bit codes (in geno_buf)
+  saige::DevBuf geno_buf;
   float4* zlut = nullptr;             // per marker: f32 z for codes 00,01,10,11
   double* two_p = nullptr;            // per marker 2p (0 for padding)
   double* inv_s = nullptr;            // per marker 1/sqrt(2p(1-p)) (0 when degenerate / padding)

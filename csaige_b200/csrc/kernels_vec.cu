@@ -7,6 +7,7 @@
 
 #include "common.cuh"
 #include "kernels_vec.cuh"
+#include "rng.hpp"
 
 namespace saige {
 
@@ -335,12 +336,34 @@ __global__ void div_w_kernel(const double* __restrict__ v, const double* __restr
   out[i] = v[i] / wm;
 }
 
-__global__ void expand_signs_kernel(const uint8_t* __restrict__ s, double* __restrict__ out,
-                                    int64_t n, int64_t ld) {
-  const int c = blockIdx.y;
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= ld) return;
-  out[(int64_t)c * ld + i] = i < n ? (s[(int64_t)c * n + i] ? 1.0 : -1.0) : 0.0;
+struct Key8 {
+  uint32_t w[8];
+};
+
+// Rademacher probes from the ChaCha8 stream: word k = r * n + i (one block of 16
+// words per thread) gives column r, sample i the value +1 when its sign bit is set
+// (rand's gen::<bool>), else -1; rows n .. ld-1 of every column are zeroed.
+__global__ void rademacher_kernel(Key8 key, int64_t n, int64_t ld, int nrv, double* __restrict__ out) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const int64_t words = (int64_t)nrv * n;
+  if (c * 16 < words) {
+    uint32_t w[16];
+    chacha8_block(key.w, (uint64_t)c, w);
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+      const int64_t k = c * 16 + j;
+      if (k < words) {
+        const int64_t r = k / n, i = k - r * n;
+        out[r * ld + i] = static_cast<int32_t>(w[j]) < 0 ? 1.0 : -1.0;
+      }
+    }
+  }
+  // padding rows (ld - n per column)
+  const int64_t pad = (ld - n) * nrv;
+  for (int64_t e = c; e < pad; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = e / (ld - n), i = n + (e - r * (ld - n));
+    out[r * ld + i] = 0.0;
+  }
 }
 
 __global__ void zero_pad_kernel(double* __restrict__ v, int64_t n, int64_t ld) {
@@ -475,9 +498,14 @@ cudaError_t div_w(const double* v, const double* w, double* out, int64_t n, cuda
   return cudaGetLastError();
 }
 
-cudaError_t expand_signs(const uint8_t* signs, double* out, int64_t n, int64_t ld, int q,
-                         cudaStream_t st) {
-  expand_signs_kernel<<<dim3(g1(ld), q), kT, 0, st>>>(signs, out, n, ld);
+cudaError_t rademacher_probes_dev(const uint32_t* key, double* out, int64_t n, int64_t ld, int nrv,
+                                  cudaStream_t st) {
+  Key8 k;
+  for (int i = 0; i < 8; ++i) k.w[i] = key[i];
+  const int64_t blocks = ceil_div((int64_t)nrv * n, 16);
+  const int64_t pad = (ld - n) * nrv;
+  const int64_t threads = blocks > pad ? blocks : pad;
+  rademacher_kernel<<<(unsigned)ceil_div(threads > 0 ? threads : 1, kT), kT, 0, st>>>(k, n, ld, nrv, out);
   count_launches(1);
   return cudaGetLastError();
 }

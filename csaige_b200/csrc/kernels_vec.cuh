@@ -74,9 +74,10 @@ cudaError_t sub_combo(double* y, int q, const double* a, int p, const double* co
 // out = v / max(w,1e-30)
 cudaError_t div_w(const double* v, const double* w, double* out, int64_t n, cudaStream_t st);
 // Rademacher probes: out[c*ld + i] = signs from the host, expanded (bytes -> doubles).
-cudaError_t expand_signs(const uint8_t* signs, double* out, int64_t n, int64_t ld, int q,
-                         cudaStream_t st);
-// Zero rows n..ld-1 of every column (padding invariant).
+// nrv Rademacher probe columns (ld apart, padding rows zeroed) from the ChaCha8
+// stream with the given key (ai_reml.rs:121-130).
+cudaError_t rademacher_probes_dev(const uint32_t* key, double* out, int64_t n, int64_t ld, int nrv,
+                                  cudaStream_t st);
 cudaError_t zero_pad(double* v, int64_t n, int64_t ld, int q, cudaStream_t st);
 
 }  // namespace saige

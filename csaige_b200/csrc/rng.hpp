@@ -14,7 +14,34 @@
 
 #include <array>
 
+#if defined(__CUDACC__)
+#define SG_HD __host__ __device__
+#else
+#define SG_HD
+#endif
+
 namespace saige {
+
+// One ChaCha8 block: key words 4-11, 64-bit counter in words 12-13, stream 0.
+SG_HD inline void chacha8_block(const uint32_t* key, uint64_t ctr, uint32_t* out) {
+  uint32_t in[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
+                     key[0], key[1], key[2], key[3], key[4], key[5], key[6], key[7],
+                     static_cast<uint32_t>(ctr), static_cast<uint32_t>(ctr >> 32), 0u, 0u};
+  uint32_t s[16];
+  for (int i = 0; i < 16; ++i) s[i] = in[i];
+  auto rotl = [](uint32_t v, int c) { return (v << c) | (v >> (32 - c)); };
+  auto qr = [&](int a, int b, int c, int d) {
+    s[a] += s[b]; s[d] = rotl(s[d] ^ s[a], 16);
+    s[c] += s[d]; s[b] = rotl(s[b] ^ s[c], 12);
+    s[a] += s[b]; s[d] = rotl(s[d] ^ s[a], 8);
+    s[c] += s[d]; s[b] = rotl(s[b] ^ s[c], 7);
+  };
+  for (int dr = 0; dr < 4; ++dr) {
+    qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
+    qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
+  }
+  for (int i = 0; i < 16; ++i) out[i] = s[i] + in[i];
+}
 
 class ChaCha8 {
  public:
@@ -39,6 +66,9 @@ class ChaCha8 {
   }
   bool gen_bool() { return static_cast<int32_t>(next_u32()) < 0; }
 
+  // Key words (set by the seed); word w of the stream is word w % 16 of block w / 16.
+  const uint32_t* key() const { return key_; }
+
   // gen_range(low..high) for usize/u64, high > low.
   uint64_t gen_range(uint64_t low, uint64_t high) {
     const uint64_t range = high - low;
@@ -50,28 +80,8 @@ class ChaCha8 {
   }
 
  private:
-  static uint32_t rotl(uint32_t v, int c) { return (v << c) | (v >> (32 - c)); }
-
-  void block(uint64_t ctr, uint32_t* out) const {
-    uint32_t in[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u,
-                       key_[0], key_[1], key_[2], key_[3], key_[4], key_[5], key_[6], key_[7],
-                       static_cast<uint32_t>(ctr), static_cast<uint32_t>(ctr >> 32), 0u, 0u};
-    uint32_t s[16];
-    for (int i = 0; i < 16; ++i) s[i] = in[i];
-    auto qr = [&](int a, int b, int c, int d) {
-      s[a] += s[b]; s[d] = rotl(s[d] ^ s[a], 16);
-      s[c] += s[d]; s[b] = rotl(s[b] ^ s[c], 12);
-      s[a] += s[b]; s[d] = rotl(s[d] ^ s[a], 8);
-      s[c] += s[d]; s[b] = rotl(s[b] ^ s[c], 7);
-    };
-    for (int dr = 0; dr < 4; ++dr) {
-      qr(0, 4, 8, 12); qr(1, 5, 9, 13); qr(2, 6, 10, 14); qr(3, 7, 11, 15);
-      qr(0, 5, 10, 15); qr(1, 6, 11, 12); qr(2, 7, 8, 13); qr(3, 4, 9, 14);
-    }
-    for (int i = 0; i < 16; ++i) out[i] = s[i] + in[i];
-  }
   void refill() {
-    for (int b = 0; b < 4; ++b) block(counter_ + b, buf_.data() + 16 * b);
+    for (int b = 0; b < 4; ++b) chacha8_block(key_, counter_ + b, buf_.data() + 16 * b);
     counter_ += 4;
     pos_ = 0;
   }

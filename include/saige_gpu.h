@@ -104,6 +104,21 @@ int32_t saige_select_grm_markers(const double* af, const double* mac, const int6
                                  uint64_t seed, int64_t* grm_idx, int64_t* m_grm, int64_t* vr_idx,
                                  int64_t* m_vr);
 
+/* No counterpart in the reference (memory management).  Device buffers of 256 MiB
+ * and more (packed genotypes, tiles, the uploaded .bed) are kept in a per-device
+ * cache when released and reused by later allocations of 1 to 1.25 times their size,
+ * so that repeated fits of one cohort shape skip mapping and unmapping tens of GB.
+ * This call frees the cached blocks of every device.  The cache also gives its
+ * blocks back by itself when an allocation would otherwise fail. */
+int32_t saige_release_cached_memory(void);
+
+/* The Rademacher probe vectors of fit_ai_reml (saige-core/src/glmm/ai_reml.rs:121-130):
+ * ChaCha8Rng::seed_from_u64(seed), n_vec vectors of n entries drawn in order with
+ * gen::<bool>() -> +1 / -1.  Generated on `device` (the stream is counter based)
+ * and copied to out (n_vec * n doubles, vector-major). */
+int32_t saige_rademacher_probes(uint64_t seed, int32_t n_vec, int64_t n, double* out,
+                                int32_t device);
+
 /* ---------------------------------------------------------------------
  * GRM operator (OnTheFlyGrm, saige-core/src/glmm/pcg.rs:91-180)
  * ------------------------------------------------------------------- */

@@ -99,3 +99,24 @@ def test_mixed_ai_reml_tau_within_1e4_of_fp64_oracle(trait):
         # warm starts change where each solve stops inside the PCG tolerance, so the
         # tau trajectory differs at that level and the iteration count may differ
         assert r.converged and np.all(rel <= 1e-4)
+
+
+def test_large_blocks_reused_from_cache_give_same_products():
+    # genotypes 602 MB and two 602 MB tile copies: above the 256 MiB cache threshold
+    torch = pytest.importorskip("torch")
+    n, m = 200000, 12000
+    spec = cs.CohortSpec(n=n, m=m, seed=21)
+    bed = torch.empty(spec.bed_len, dtype=torch.uint8, device="cuda")
+    cs.gen_bed_dev(spec, bed.data_ptr())
+    torch.cuda.synchronize()
+    af = np.linspace(0.05, 0.5, m)
+    v = np.random.default_rng(4).standard_normal((2, n))
+    outs = []
+    for rep in range(3):
+        if rep == 2:
+            cs.api.release_cached_memory()
+        grm = cs.OnTheFlyGrm.from_bed_dev(bed.data_ptr(), spec.bed_len, n, m, np.arange(m), af,
+                                          precision=MIXED)
+        outs.append(grm.mat_vec(v))
+        grm.close()
+    assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])

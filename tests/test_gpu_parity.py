@@ -59,6 +59,14 @@ def test_generator_device_matches_host():
     assert np.array_equal(dev.cpu().numpy(), host)
 
 
+@pytest.mark.parametrize("seed,n_vec,n", [(12345, 30, 1001), (7, 3, 17), (1, 2, 100003)])
+def test_rademacher_probes_bit_exact(seed, n_vec, n):
+    # the GPU draws the ChaCha8 stream block-parallel; the oracle draws it in order
+    got = cs.api.rademacher_probes(seed, n_vec, n)
+    want = O.probes(seed, n_vec, n)
+    assert np.array_equal(got, want)
+
+
 # ---------------------------------------------------------------- GRM product
 def _grm_case(n=1001, m=300, seed=7, sidx=None):
     spec, bed = _cohort(n, m, seed=seed)
