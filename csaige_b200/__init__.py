@@ -20,6 +20,11 @@ from .api import (  # noqa: F401
     PcgSolver,
     SaigePcgConfig,
     TraitType,
+    VarianceRatioConfig,
+    VarianceRatioResult,
+    estimate_variance_ratio,
+    vr_marker_order,
+    write_variance_ratio_file,
     bed_marker_stats,
     device_count,
     fit_ai_reml,

@@ -67,6 +67,35 @@ class AiRemlSummaryC(C.Structure):
     ]
 
 
+class VrConfigC(C.Structure):
+    _fields_ = [
+        ("n_markers", C.c_int32),
+        ("use_categorical", C.c_int32),
+        ("min_mac", C.c_double),
+        ("ratio_cv_cutoff", C.c_double),
+        ("seed", C.c_uint64),
+        ("precision", C.c_int32),
+        ("xadjust", C.c_int32),
+        ("block", C.c_int32),
+        ("reserved", C.c_int32),
+    ]
+
+
+class VrSummaryC(C.Structure):
+    _fields_ = [
+        ("variance_ratio", C.c_double),
+        ("n_markers_used", C.c_int32),
+        ("n_categories", C.c_int32),
+        ("cat_upper", C.c_double * 8),
+        ("cat_vr", C.c_double * 8),
+        ("n_solved", C.c_int32),
+        ("n_blocks", C.c_int32),
+        ("pcg_iters", C.c_int64),
+        ("n_kv", C.c_int64),
+        ("seconds", C.c_double),
+    ]
+
+
 class GrmStatsC(C.Structure):
     _fields_ = [
         ("n_kv", C.c_int64),
@@ -143,6 +172,13 @@ SIGNATURES = {
         [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, _vp],
     ),
     "saige_release_cached_memory": (C.c_int32, []),
+    "saige_vr_config_default": (C.c_int32, [P(VrConfigC)]),
+    "saige_vr_marker_order": (C.c_int32, [C.c_uint64, C.c_int64, _i64]),
+    "saige_estimate_variance_ratio": (
+        C.c_int32,
+        [_vp, _d, _d, C.c_int64, _d, _d, _d, C.c_int32, _d, C.c_int32, P(VrConfigC),
+         P(VrSummaryC), _d, _i64],
+    ),
     "saige_rademacher_probes": (C.c_int32, [C.c_uint64, C.c_int32, C.c_int64, _d, C.c_int32]),
     "saige_grm_matvec_dev_noalloc": (
         C.c_int32,

@@ -427,6 +427,125 @@ def gen_pheno(spec: CohortSpec) -> tuple[np.ndarray, np.ndarray]:
 
 
 # ---------------------------------------------------------------------------
+# variance ratio (variance_ratio.rs:87-246, fit_null.rs:290-373)
+# ---------------------------------------------------------------------------
+VR_XADJUST_REFERENCE = 0   # (X'WX)^-1 X'W laid out as fit_null.rs:294-306 builds it
+VR_XADJUST_PROJECTION = 1  # the projection X (X'WX)^-1 X'W g
+
+
+@dataclass
+class VarianceRatioConfig:
+    """VarianceRatioConfig (variance_ratio.rs:28-56) plus the solver settings."""
+    n_markers: int = 30
+    min_mac: float = 20.0
+    use_categorical: bool = False
+    ratio_cv_cutoff: float = 0.001
+    seed: int = 12345
+    precision: int = PREC_FP32
+    xadjust: int = VR_XADJUST_REFERENCE
+    block: int = 0  # candidates per block PCG; 0: 64 for MIXED, else n_markers then 10
+
+    def c(self) -> "_lib.VrConfigC":
+        return _lib.VrConfigC(self.n_markers, int(self.use_categorical), self.min_mac,
+                              self.ratio_cv_cutoff, self.seed, self.precision, self.xadjust,
+                              self.block, 0)
+
+
+@dataclass
+class VarianceRatioResult:
+    """VarianceRatioResult (variance_ratio.rs:59-71) plus work counters."""
+    variance_ratio: float
+    categorical_vr: list
+    n_markers_used: int
+    per_marker_vr: np.ndarray
+    used_idx: np.ndarray
+    n_solved: int = 0
+    n_blocks: int = 0
+    pcg_iters: int = 0
+    n_kv: int = 0
+    seconds: float = 0.0
+
+
+def vr_marker_order(seed: int, n_cand: int) -> np.ndarray:
+    """Order in which estimate_variance_ratio tries its candidates (variance_ratio.rs:116-120)."""
+    out = np.empty(max(n_cand, 0), dtype=np.int64)
+    check(LIB.saige_vr_marker_order(seed, n_cand, _i64ptr(out)))
+    return out
+
+
+def estimate_variance_ratio(grm: "OnTheFlyGrm", dosage_vectors, mac_values, mu, working_weights,
+                            tau, trait_type: TraitType, x,
+                            config: VarianceRatioConfig = VarianceRatioConfig()
+                            ) -> VarianceRatioResult:
+    """estimate_variance_ratio with Sigma^-1 = (tau0 diag(1/w) + tau1 K)^-1 over the GRM
+    handle and XVX_inv_XV built from the working weights, as fit_null.rs:290-342 does.
+    dosage_vectors: (n_cand, n) with NaN for missing calls; x: (n, p)."""
+    d = np.ascontiguousarray(dosage_vectors, dtype=np.float64)
+    if d.ndim == 1:
+        d = d[None, :]
+    n_cand = d.shape[0] if d.size else 0
+    mac = _f64(mac_values, n_cand)
+    n = grm.n_samples
+    mu_ = _f64(mu, n)
+    w_ = _f64(working_weights, n)
+    t = _f64(tau, 2)
+    xa = np.asarray(x, dtype=np.float64)
+    if xa.ndim == 1:
+        xa = xa[:, None]
+    p = xa.shape[1]
+    xc = np.ascontiguousarray(xa.T)  # column-major n x p
+    cfg = config.c()
+    out = _lib.VrSummaryC()
+    vr = np.empty(max(n_cand, 1))
+    used = np.empty(max(n_cand, 1), dtype=np.int64)
+    check(LIB.saige_estimate_variance_ratio(grm._h, _dptr(d), _dptr(mac), n_cand, _dptr(mu_),
+                                            _dptr(w_), _dptr(t), int(trait_type), _dptr(xc), p,
+                                            C.byref(cfg), C.byref(out), _dptr(vr),
+                                            _i64ptr(used)))
+    k = out.n_markers_used
+    cats = [(out.cat_upper[i], out.cat_vr[i]) for i in range(out.n_categories)]
+    return VarianceRatioResult(out.variance_ratio, cats, k, vr[:k].copy(), used[:k].copy(),
+                               out.n_solved, out.n_blocks, out.pcg_iters, out.n_kv, out.seconds)
+
+
+def write_variance_ratio_file(result: VarianceRatioResult, path) -> None:
+    """write_variance_ratio_file (variance_ratio.rs:322-338): "<vr> null 1", or one line
+    per MAC category "<vr> null <k>"."""
+    with open(path, "w") as f:
+        if not result.categorical_vr:
+            f.write(f"{_rust_f64(result.variance_ratio)} null 1\n")
+        else:
+            for k, (_, vr) in enumerate(result.categorical_vr):
+                f.write(f"{_rust_f64(vr)} null {k + 1}\n")
+
+
+def _rust_f64(x: float) -> str:
+    """Rust's Display for f64: the shortest repr that round-trips, no exponent for
+    ordinary magnitudes, integers without a fractional part (1.0 -> "1")."""
+    if x != x:
+        return "NaN"
+    if x in (float("inf"), float("-inf")):
+        return "inf" if x > 0 else "-inf"
+    if x == int(x) and abs(x) < 1e16:
+        return str(int(x))
+    r = repr(x)
+    if "e" in r:
+        mant, exp = r.split("e")
+        e = int(exp)
+        digits = mant.replace("-", "").replace(".", "")
+        sign = "-" if x < 0 else ""
+        point = mant.replace("-", "").find(".")
+        point = len(mant.replace("-", "")) if point < 0 else point
+        pos = point + e
+        if pos <= 0:
+            return sign + "0." + "0" * (-pos) + digits
+        if pos >= len(digits):
+            return sign + digits + "0" * (pos - len(digits))
+        return sign + digits[:pos] + "." + digits[pos:]
+    return r
+
+
+# ---------------------------------------------------------------------------
 # whole fit-null from host buffers, instrumentation
 # ---------------------------------------------------------------------------
 @dataclass

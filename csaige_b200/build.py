@@ -29,6 +29,7 @@ SOURCES = [
     "kernels_vec.cu",
     "kernels_tc.cu",
     "noalloc.cu",
+    "vr.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

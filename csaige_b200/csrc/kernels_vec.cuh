@@ -73,7 +73,6 @@ cudaError_t sub_combo(double* y, int q, const double* a, int p, const double* co
                       int64_t ld, cudaStream_t st);
 // out = v / max(w,1e-30)
 cudaError_t div_w(const double* v, const double* w, double* out, int64_t n, cudaStream_t st);
-// Rademacher probes: out[c*ld + i] = signs from the host, expanded (bytes -> doubles).
 // nrv Rademacher probe columns (ld apart, padding rows zeroed) from the ChaCha8
 // stream with the given key (ai_reml.rs:121-130).
 cudaError_t rademacher_probes_dev(const uint32_t* key, double* out, int64_t n, int64_t ld, int nrv,

@@ -8,7 +8,10 @@
 //    with PCG32 (XSH-RR, O'Neill 2014) outputs;
 //  - rand 0.8.5 mappings: bool = sign bit of next_u32; uniform integers in
 //    [low, high) by widening multiply with the "(range << lz) - 1" zone.
-// Used by ai_reml.rs:121-130 (probes) and fit_null.rs:234-240 (VR draws).
+//  - SliceRandom::shuffle of rand 0.8.5 (Fisher-Yates from the back; indices by
+//    the u32 gen_range when they fit).
+// Used by ai_reml.rs:121-130 (probes), fit_null.rs:234-240 (VR draws) and
+// variance_ratio.rs:116-120 (the order in which VR markers are tried).
 #pragma once
 #include <stdint.h>
 
@@ -68,6 +71,29 @@ class ChaCha8 {
 
   // Key words (set by the seed); word w of the stream is word w % 16 of block w / 16.
   const uint32_t* key() const { return key_; }
+
+  // gen_range(low..high) for u32, high > low: the 32-bit widening multiply.
+  uint32_t gen_range_u32(uint32_t low, uint32_t high) {
+    const uint32_t range = high - low;
+    const uint32_t zone = (range << __builtin_clz(range)) - 1u;
+    while (true) {
+      const uint64_t wide = static_cast<uint64_t>(next_u32()) * range;
+      if (static_cast<uint32_t>(wide) <= zone) return low + static_cast<uint32_t>(wide >> 32);
+    }
+  }
+
+  // SliceRandom::shuffle of rand 0.8.5: Fisher-Yates from the back, the index
+  // drawn with gen_range(0..i+1) on u32 when i+1 fits in 32 bits.
+  template <class T>
+  void shuffle(T* v, size_t len) {
+    for (size_t i = len; i-- > 1;) {
+      const size_t j = (i + 1) <= 0xFFFFFFFFull ? gen_range_u32(0, (uint32_t)(i + 1))
+                                                 : (size_t)gen_range(0, (uint64_t)(i + 1));
+      T t = v[i];
+      v[i] = v[j];
+      v[j] = t;
+    }
+  }
 
   // gen_range(low..high) for usize/u64, high > low.
   uint64_t gen_range(uint64_t low, uint64_t high) {

@@ -104,6 +104,65 @@ int32_t saige_select_grm_markers(const double* af, const double* mac, const int6
                                  uint64_t seed, int64_t* grm_idx, int64_t* m_grm, int64_t* vr_idx,
                                  int64_t* m_vr);
 
+/* ---------------------------------------------------------------------
+ * Variance ratio (saige-core/src/glmm/variance_ratio.rs:87-246, driven as in
+ * saige-cli/src/commands/fit_null.rs:290-373)
+ * ------------------------------------------------------------------- */
+#define SAIGE_VR_XADJUST_REFERENCE 0  /* fit_null.rs:294-306 exactly: (X'WX)^-1 X'W filled
+                                         p x n row-major and read back column-major */
+#define SAIGE_VR_XADJUST_PROJECTION 1 /* the projection X (X'WX)^-1 X'W g */
+
+/* VarianceRatioConfig (variance_ratio.rs:28-56) plus the solver settings. */
+typedef struct saige_vr_config {
+  int32_t n_markers;       /* markers before the first CV test (30) */
+  int32_t use_categorical; /* MAC-binned ratios (0) */
+  double min_mac;          /* 20 */
+  double ratio_cv_cutoff;  /* 0.001 */
+  uint64_t seed;           /* shuffle seed (12345) */
+  int32_t precision;       /* SAIGE_PREC_* of the GRM products (FP32) */
+  int32_t xadjust;         /* SAIGE_VR_XADJUST_* (REFERENCE) */
+  int32_t block;           /* candidates per block PCG; 0: 64 for MIXED, else n_markers then 10 */
+  int32_t reserved;
+} saige_vr_config;
+
+/* VarianceRatioResult (variance_ratio.rs:59-71) plus work counters. */
+typedef struct saige_vr_summary {
+  double variance_ratio;
+  int32_t n_markers_used;
+  int32_t n_categories;    /* categorical_vr entries: (cat_upper[k], cat_vr[k]) */
+  double cat_upper[8];
+  double cat_vr[8];
+  int32_t n_solved;        /* candidates solved (a block may solve more than are used) */
+  int32_t n_blocks;
+  int64_t pcg_iters;       /* PCG iterations summed over columns */
+  int64_t n_kv;            /* GRM products (columns) */
+  double seconds;          /* device time */
+} saige_vr_summary;
+
+int32_t saige_vr_config_default(saige_vr_config* cfg);
+
+/* The order in which estimate_variance_ratio tries its candidates
+ * (variance_ratio.rs:116-120: ChaCha8Rng::seed_from_u64(seed) and rand 0.8.5's
+ * SliceRandom::shuffle of 0..n_cand).  Host only. */
+int32_t saige_vr_marker_order(uint64_t seed, int64_t n_cand, int64_t* order);
+
+/* estimate_variance_ratio(dosage_vectors, mac_values, mu, tau, trait, x,
+ * xvx_inv_xv, sigma_inv, config) on the GPU: dosages are n_cand x n doubles
+ * (candidate-major, NaN = missing call), mac per candidate, mu and w the fit's
+ * final mean and working weights (XVX_inv_XV and Sigma^-1 are built from w and
+ * tau as fit_null.rs does), x n x p column-major.  A missing call is set to
+ * 2*af of the marker's called genotypes (the reference keeps NaN, which makes
+ * its ratio NaN); markers without missing calls are treated as the reference
+ * treats them.  per_marker_vr / used_idx (capacity n_cand, may be NULL)
+ * receive the ratios and the candidate indices in the order used.  Returns
+ * SAIGE_EINVAL with "No markers available ..." when no candidate is usable. */
+int32_t saige_estimate_variance_ratio(saige_grm* h, const double* dosages, const double* mac,
+                                      int64_t n_cand, const double* mu, const double* w,
+                                      const double tau[2], int32_t trait, const double* x,
+                                      int32_t p, const saige_vr_config* cfg,
+                                      saige_vr_summary* out, double* per_marker_vr,
+                                      int64_t* used_idx);
+
 /* No counterpart in the reference (memory management).  Device buffers of 256 MiB
  * and more (packed genotypes, tiles, the uploaded .bed) are kept in a per-device
  * cache when released and reused by later allocations of 1 to 1.25 times their size,

@@ -880,3 +880,183 @@ int orc_fit_ai_reml(const double* y, const double* x, int64_t n, int p, int t, i
   free(kpy); free(su); free(ku); free(pk); free(invw_py); free(tmp); free(probes);
   return 0;
 }
+
+
+/* ===================================================================== */
+/* Variance ratio (saige-core/src/glmm/variance_ratio.rs:87-246,         */
+/* saige-cli/src/commands/fit_null.rs:290-373)                            */
+/* ===================================================================== */
+
+/* rand 0.8.5 UniformInt<u32>::sample_single(low, high) -> sample_single_inclusive(low, high-1):
+ * range = high - low, zone = (range << lz) - 1, v = next_u32, accept when the low half of
+ * v * range is <= zone and return low + the high half. */
+uint32_t orc_rng_gen_range_u32(orc_chacha_rng* r, uint32_t low, uint32_t high) {
+  uint32_t range = high - low;
+  uint32_t zone = (range << __builtin_clz(range)) - 1u;
+  for (;;) {
+    uint64_t prod = (uint64_t)orc_rng_next_u32(r) * (uint64_t)range;
+    if ((uint32_t)prod <= zone) return low + (uint32_t)(prod >> 32);
+  }
+}
+
+/* rand 0.8.5 SliceRandom::shuffle: for i = len-1 down to 1, swap(i, gen_index(i+1)) with
+ * gen_index using the u32 range when the bound fits in 32 bits (variance_ratio.rs:116-120). */
+void orc_shuffled_indices(uint64_t seed, int64_t len, int64_t* out) {
+  orc_chacha_rng r;
+  orc_chacha_seed_from_u64(&r, seed, 8);
+  for (int64_t i = 0; i < len; ++i) out[i] = i;
+  for (int64_t i = len - 1; i >= 1; --i) {
+    uint64_t ub = (uint64_t)i + 1;
+    int64_t j = ub <= 0xFFFFFFFFull ? (int64_t)orc_rng_gen_range_u32(&r, 0, (uint32_t)ub)
+                                    : (int64_t)orc_rng_gen_range_u64(&r, 0, ub);
+    int64_t t = out[i];
+    out[i] = out[j];
+    out[j] = t;
+  }
+}
+
+/* variance_ratio.rs:260-272: (sd / mean) / n, infinity for n <= 1 or |mean| < 1e-30. */
+static double vr_cal_cv(const double* v, int n) {
+  if (n <= 1) return INFINITY;
+  double m = 0.0;
+  for (int i = 0; i < n; ++i) m += v[i];
+  m /= (double)n;
+  if (fabs(m) < 1e-30) return INFINITY;
+  double var = 0.0;
+  for (int i = 0; i < n; ++i) var += (v[i] - m) * (v[i] - m);
+  var /= ((double)n - 1.0);
+  return (sqrt(var) / m) / (double)n;
+}
+
+int orc_variance_ratio(const double* dosages, const double* mac, int64_t n_cand, const double* mu,
+                       const double* w, const double tau[2], int t, const double* x, int64_t n,
+                       int p, int kind, const double* grm, int64_t m, int kmode,
+                       const orc_vr_config* cfg, orc_vr_summary* out, double* per_marker_vr,
+                       int64_t* used_idx) {
+  /* fit_null.rs:290-306: XVX = X'WX (dense.rs:227-245), its inverse (inverse_spd:
+   * Cholesky, unit columns), and XVX_inv_XV filled as data[j*n + i]. */
+  double xvx[64 * 64] = {0}, l[64 * 64], inv[64 * 64];
+  for (int j = 0; j < p; ++j)
+    for (int k = j; k < p; ++k) {
+      double s = 0.0;
+      for (int64_t i = 0; i < n; ++i) s += x[(int64_t)j * n + i] * w[i] * x[(int64_t)k * n + i];
+      xvx[j * p + k] = s;
+      xvx[k * p + j] = s;
+    }
+  if (orc_cholesky(xvx, p, l) != 0) return 2;
+  for (int j = 0; j < p; ++j) {
+    double e[64], col[64];
+    for (int k = 0; k < p; ++k) e[k] = k == j ? 1.0 : 0.0;
+    orc_chol_solve(l, p, e, col);
+    for (int k = 0; k < p; ++k) inv[k * p + j] = col[k];  /* inv(k, j) */
+  }
+  double* data = (double*)malloc(sizeof(double) * (size_t)p * (size_t)n);
+  for (int j = 0; j < p; ++j)
+    for (int64_t i = 0; i < n; ++i) {
+      double val = 0.0;
+      for (int k = 0; k < p; ++k) val += inv[j * p + k] * x[(int64_t)k * n + i] * w[i];
+      data[(int64_t)j * n + i] = val;
+    }
+
+  int64_t* order = (int64_t*)malloc(sizeof(int64_t) * (size_t)(n_cand > 0 ? n_cand : 1));
+  orc_shuffled_indices(cfg->seed, n_cand, order);
+  double* g0 = (double*)malloc(sizeof(double) * (size_t)n);
+  double* gt = (double*)malloc(sizeof(double) * (size_t)n);
+  double* sg = (double*)malloc(sizeof(double) * (size_t)n);
+  int n_tested = 0, target = cfg->n_markers;
+  int64_t n_kv = 0;
+  for (int64_t oi = 0; oi < n_cand; ++oi) {
+    const int64_t idx = order[oi];
+    if (mac[idx] < cfg->min_mac) continue;
+    const double* g_raw = dosages + idx * n;
+    /* missing calls -> 2 * af of the called genotypes (see the header) */
+    double s_nm = 0.0;
+    int64_t n_nm = 0;
+    for (int64_t i = 0; i < n; ++i)
+      if (!isnan(g_raw[i])) { s_nm += g_raw[i]; ++n_nm; }
+    const double fill = n_nm > 0 ? 2.0 * (s_nm / (2.0 * (double)n_nm)) : 0.0;
+    double sum = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      g0[i] = isnan(g_raw[i]) ? fill : g_raw[i];
+      sum += g0[i];
+    }
+    const double af = sum / (2.0 * (double)n);
+    if (af > 0.5)
+      for (int64_t i = 0; i < n; ++i) g0[i] = 2.0 - g0[i];
+    double ac = 0.0;
+    for (int64_t i = 0; i < n; ++i) ac += g0[i];
+    if (ac < 1.0) continue;
+    /* X-adjust (variance_ratio.rs:144-151) */
+    double tcoef[64];
+    for (int r = 0; r < p; ++r) tcoef[r] = 0.0;
+    if (cfg->xadjust == 0) {
+      /* DenseMatrix::from_col_major(p, n, data).mat_vec(g0) (dense.rs:35-38, 102-113):
+       * element (r, c) = data[c * p + r], accumulated column by column */
+      for (int64_t c = 0; c < n; ++c) {
+        const double vc = g0[c];
+        for (int r = 0; r < p; ++r) tcoef[r] += data[c * p + r] * vc;
+      }
+    } else {
+      for (int r = 0; r < p; ++r) {
+        double s = 0.0;
+        for (int64_t i = 0; i < n; ++i) s += data[(int64_t)r * n + i] * g0[i];
+        tcoef[r] = s;
+      }
+    }
+    /* x.mat_vec(t) column by column, then g_tilde = g0 - X t */
+    for (int64_t i = 0; i < n; ++i) sg[i] = 0.0;
+    for (int k = 0; k < p; ++k)
+      for (int64_t i = 0; i < n; ++i) sg[i] += x[(int64_t)k * n + i] * tcoef[k];
+    for (int64_t i = 0; i < n; ++i) gt[i] = g0[i] - sg[i];
+    /* Sigma^-1 g_tilde: PcgSolver::new(1e-5, 500), zero start (fit_null.rs:317-342) */
+    int iters = 0, conv = 0;
+    double resid = 0.0;
+    orc_pcg_sigma(NULL, kind, grm, n, m, kmode, w, tau, gt, NULL, 1e-5, 500, sg, &iters, &resid,
+                  &conv);
+    n_kv += iters;
+    double var1 = 0.0;
+    for (int64_t i = 0; i < n; ++i) var1 += gt[i] * sg[i];
+    var1 /= ac;
+    double var2 = 0.0;
+    for (int64_t i = 0; i < n; ++i) {
+      /* variance_ratio.rs:162-180 */
+      const double c = t == ORC_BINARY ? mu[i] * (1.0 - mu[i]) : (t == ORC_SURVIVAL ? mu[i] : 1.0);
+      var2 += c * gt[i] * gt[i] / ac;
+    }
+    if (var2 < 1e-30) continue;
+    per_marker_vr[n_tested] = var1 / var2;
+    if (used_idx) used_idx[n_tested] = idx;
+    ++n_tested;
+    if (n_tested >= target) {
+      if (vr_cal_cv(per_marker_vr, n_tested) <= cfg->ratio_cv_cutoff) break;
+      target += 10;
+    }
+  }
+  free(order); free(g0); free(gt); free(sg); free(data);
+  out->n_kv = n_kv;
+  out->n_markers_used = n_tested;
+  out->n_categories = 0;
+  if (n_tested == 0) return 1;
+  double mean = 0.0;
+  for (int i = 0; i < n_tested; ++i) mean += per_marker_vr[i];
+  out->variance_ratio = mean / (double)n_tested;
+  if (cfg->use_categorical) {
+    /* variance_ratio.rs:276-298 with the default MAC bins */
+    static const double lo[8] = {0.5, 1.5, 2.5, 3.5, 4.5, 5.5, 10.5, 20.5};
+    static const double hi[8] = {1.5, 2.5, 3.5, 4.5, 5.5, 10.5, 20.5, INFINITY};
+    for (int b = 0; b < 8; ++b) {
+      double s = 0.0;
+      int c = 0;
+      for (int i = 0; i < n_tested; ++i) {
+        const double mc = mac[used_idx ? used_idx[i] : 0];
+        if (mc > lo[b] && mc <= hi[b]) { s += per_marker_vr[i]; ++c; }
+      }
+      if (c > 0) {
+        out->cat_upper[out->n_categories] = hi[b];
+        out->cat_vr[out->n_categories] = s / (double)c;
+        ++out->n_categories;
+      }
+    }
+  }
+  return 0;
+}

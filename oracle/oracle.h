@@ -131,6 +131,46 @@ int orc_pcg_sigma(const double* y_unused, int kind, const double* grm, int64_t n
                   const double* x0, double tol, int max_iter, double* x, int* iters,
                   double* resid, int* converged);
 
+/* rand 0.8.5 UniformInt<u32>::sample_single(low, high): 32-bit widening multiply. */
+uint32_t orc_rng_gen_range_u32(orc_chacha_rng* r, uint32_t low, uint32_t high);
+
+/* variance_ratio.rs:116-120: indices 0..len shuffled by rand 0.8.5's
+ * SliceRandom::shuffle with ChaCha8Rng::seed_from_u64(seed). */
+void orc_shuffled_indices(uint64_t seed, int64_t len, int64_t* out);
+
+/* Variance ratio (variance_ratio.rs:87-246 driven as in fit_null.rs:290-373).
+ * dosages: n_cand x n (candidate-major), NaN = missing call; mac per candidate.
+ * mu, w: the fit's final mu and working weights; x: n x p column-major.
+ * xadjust 0 = as fit_null.rs:294-306 builds XVX_inv_XV (a p x n row-major array
+ * read back as column-major), 1 = the projection X (X'WX)^-1 X'W g.
+ * Missing calls are set to 2*af of the called genotypes (saige-rs keeps NaN,
+ * which makes its variance ratio NaN).  per_marker_vr / used_idx (capacity
+ * n_cand) receive the ratios and candidate indices in the order used.
+ * Returns 0, or 1 when no marker is usable ("No markers available ..."). */
+typedef struct {
+  int n_markers;
+  double min_mac;
+  double ratio_cv_cutoff;
+  uint64_t seed;
+  int use_categorical;
+  int xadjust;
+} orc_vr_config;
+
+typedef struct {
+  double variance_ratio;
+  int n_markers_used;
+  int n_categories;
+  double cat_upper[8];
+  double cat_vr[8];
+  int64_t n_kv;
+} orc_vr_summary;
+
+int orc_variance_ratio(const double* dosages, const double* mac, int64_t n_cand, const double* mu,
+                       const double* w, const double tau[2], int trait_type, const double* x,
+                       int64_t n, int p, int kind, const double* grm, int64_t m, int kmode,
+                       const orc_vr_config* cfg, orc_vr_summary* out, double* per_marker_vr,
+                       int64_t* used_idx);
+
 #ifdef __cplusplus
 }
 #endif

@@ -244,3 +244,51 @@ def fit_ai_reml(y, x: np.ndarray, trait: int, kind: int, grm, m: int = 0, kmode:
     return dict(tau=np.array(out.tau[:]), iterations=it, converged=bool(out.converged),
                 log_likelihood=out.log_likelihood, n_kv=out.n_kv, pcg_iters=out.pcg_iters,
                 tau_trace=trace[: 2 * it].reshape(-1, 2), alpha=alpha, mu=mu, eta=eta, w=w)
+
+
+# ---------------------------------------------------------------- variance ratio
+class VrConfig(C.Structure):
+    _fields_ = [("n_markers", C.c_int), ("min_mac", C.c_double), ("ratio_cv_cutoff", C.c_double),
+                ("seed", C.c_uint64), ("use_categorical", C.c_int), ("xadjust", C.c_int)]
+
+
+class VrSummary(C.Structure):
+    _fields_ = [("variance_ratio", C.c_double), ("n_markers_used", C.c_int),
+                ("n_categories", C.c_int), ("cat_upper", C.c_double * 8),
+                ("cat_vr", C.c_double * 8), ("n_kv", C.c_int64)]
+
+
+L.orc_rng_gen_range_u32.restype = C.c_uint32
+L.orc_rng_gen_range_u32.argtypes = [P(ChaChaRng), C.c_uint32, C.c_uint32]
+L.orc_shuffled_indices.argtypes = [C.c_uint64, C.c_int64, _i64]
+L.orc_variance_ratio.restype = C.c_int
+L.orc_variance_ratio.argtypes = [_d, _d, C.c_int64, _d, _d, _d, C.c_int, _d, C.c_int64, C.c_int,
+                                 C.c_int, _d, C.c_int64, C.c_int, P(VrConfig), P(VrSummary), _d,
+                                 _i64]
+
+
+def shuffled_indices(seed: int, length: int) -> np.ndarray:
+    out = np.empty(max(length, 1), dtype=np.int64)
+    L.orc_shuffled_indices(seed, length, out.ctypes.data_as(_i64))
+    return out[:length]
+
+
+def variance_ratio(dosages, mac, mu, w, tau, trait: int, x: np.ndarray, kind: int, grm,
+                   m: int = 0, kmode: int = 0, n_markers=30, min_mac=20.0, cutoff=0.001,
+                   seed=12345, categorical=False, xadjust=0):
+    d = np.ascontiguousarray(dosages, dtype=np.float64)
+    n_cand, n = d.shape
+    p = x.shape[1]
+    xc = np.asfortranarray(x).ravel(order="F").copy()
+    cfg = VrConfig(n_markers, min_mac, cutoff, seed, int(categorical), xadjust)
+    out = VrSummary()
+    vr = np.empty(max(n_cand, 1))
+    used = np.empty(max(n_cand, 1), dtype=np.int64)
+    g = None if grm is None else dp(f64(grm))
+    rc = L.orc_variance_ratio(dp(d), dp(f64(mac)), n_cand, dp(f64(mu)), dp(f64(w)),
+                              dp(f64(tau)), trait, dp(xc), n, p, kind, g, m, kmode,
+                              C.byref(cfg), C.byref(out), dp(vr), used.ctypes.data_as(_i64))
+    k = out.n_markers_used
+    return dict(rc=rc, variance_ratio=out.variance_ratio, n_used=k, per_marker=vr[:k].copy(),
+                used=used[:k].copy(), n_kv=out.n_kv,
+                categorical=[(out.cat_upper[i], out.cat_vr[i]) for i in range(out.n_categories)])

@@ -1,0 +1,111 @@
+"""Variance ratio on the GPU (csaige_b200.estimate_variance_ratio, through the C ABI)
+against the CPU oracle's restatement of variance_ratio.rs:87-246 / fit_null.rs:290-373.
+
+The ratios depend on Sigma^-1 solves to the PCG tolerance (1e-5), so per-marker ratios
+are compared at 1e-4 relative; the marker order and count, which follow from the
+shuffle and the reference's rules, must be equal."""
+import numpy as np
+import pytest
+
+import csaige_b200 as cs
+import oracle_ffi as O
+
+pytestmark = pytest.mark.gpu
+
+MIXED = cs.PREC_MIXED
+FP32 = cs.PREC_FP32
+
+
+def _setup(n=1200, m_grm=500, n_cand=120, seed=5, missing=0.01):
+    spec = cs.CohortSpec(n=n, m=m_grm + n_cand, seed=seed, missing_rate=missing,
+                         prevalence=0.2, h2=0.3, n_covar=2)
+    bed = cs.gen_bed(spec)
+    m = m_grm + n_cand
+    af, mac, nv = O.marker_stats(bed, n, m)
+    gidx = np.arange(m_grm)
+    cidx = np.arange(m_grm, m)
+    grm = cs.OnTheFlyGrm.from_bed(bed, n, m, gidx, af[gidx])
+    dos_g = O.dosages(bed, n, gidx)
+    z = O.standardize(dos_g, af[gidx], 0)
+    cand = O.dosages(bed, n, cidx)  # NaN = missing call
+    y, x = cs.gen_pheno(spec)
+    fit = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cs.AiRemlConfig(max_iter=5))
+    return dict(grm=grm, z=z, m_grm=m_grm, cand=cand, mac=mac[cidx], x=x, mu=fit.mu,
+                w=fit.working_weights, tau=np.array(fit.tau))
+
+
+@pytest.fixture(scope="module")
+def case():
+    return _setup()
+
+
+def _oracle(c, **kw):
+    return O.variance_ratio(c["cand"], c["mac"], c["mu"], c["w"], c["tau"], O.BINARY, c["x"],
+                            O.K_OTF, c["z"], m=c["m_grm"], kmode=0, **kw)
+
+
+@pytest.mark.parametrize("xadjust", [cs.api.VR_XADJUST_REFERENCE, cs.api.VR_XADJUST_PROJECTION])
+@pytest.mark.parametrize("precision", [FP32, MIXED])
+def test_all_candidates_match_oracle(case, xadjust, precision):
+    c = case
+    cfg = cs.VarianceRatioConfig(ratio_cv_cutoff=1e-12, xadjust=xadjust, precision=precision)
+    got = cs.estimate_variance_ratio(c["grm"], c["cand"], c["mac"], c["mu"], c["w"], c["tau"],
+                                     cs.TraitType.Binary, c["x"], cfg)
+    want = _oracle(c, cutoff=1e-12, xadjust=xadjust)
+    assert want["rc"] == 0
+    assert got.n_markers_used == want["n_used"]
+    assert np.array_equal(got.used_idx, want["used"])
+    assert np.allclose(got.per_marker_vr, want["per_marker"], rtol=1e-4, atol=0)
+    assert abs(got.variance_ratio - want["variance_ratio"]) < 1e-4 * abs(want["variance_ratio"])
+
+
+def test_default_stopping_rule_matches_oracle(case):
+    c = case
+    got = cs.estimate_variance_ratio(c["grm"], c["cand"], c["mac"], c["mu"], c["w"], c["tau"],
+                                     cs.TraitType.Binary, c["x"], cs.VarianceRatioConfig())
+    want = _oracle(c)
+    assert got.n_markers_used == want["n_used"] >= 30
+    assert np.array_equal(got.used_idx, want["used"])
+    assert abs(got.variance_ratio - want["variance_ratio"]) < 1e-4 * abs(want["variance_ratio"])
+
+
+@pytest.mark.parametrize("precision", [FP32, MIXED])
+def test_ratios_do_not_depend_on_block_size(case, precision):
+    # each column's PCG recurrence and reductions are independent of its block
+    c = case
+    out = []
+    for block in (7, 64):
+        cfg = cs.VarianceRatioConfig(ratio_cv_cutoff=1e-12, precision=precision, block=block)
+        out.append(cs.estimate_variance_ratio(c["grm"], c["cand"], c["mac"], c["mu"], c["w"],
+                                              c["tau"], cs.TraitType.Binary, c["x"], cfg))
+    assert np.array_equal(out[0].used_idx, out[1].used_idx)
+    assert np.array_equal(out[0].per_marker_vr, out[1].per_marker_vr)
+    assert out[0].n_blocks > out[1].n_blocks
+
+
+def test_ratio_is_one_when_tau_g_is_zero(case):
+    c = case
+    w = c["mu"] * (1 - c["mu"])
+    got = cs.estimate_variance_ratio(c["grm"], c["cand"], c["mac"], c["mu"], w, [1.0, 0.0],
+                                     cs.TraitType.Binary, c["x"], cs.VarianceRatioConfig())
+    assert got.n_markers_used == 30
+    assert np.allclose(got.per_marker_vr, 1.0, rtol=0, atol=1e-9)
+
+
+def test_categorical_ratios_match_oracle(case):
+    c = case
+    cfg = cs.VarianceRatioConfig(ratio_cv_cutoff=1e-12, use_categorical=True)
+    got = cs.estimate_variance_ratio(c["grm"], c["cand"], c["mac"], c["mu"], c["w"], c["tau"],
+                                     cs.TraitType.Binary, c["x"], cfg)
+    want = _oracle(c, cutoff=1e-12, categorical=True)
+    assert len(got.categorical_vr) == len(want["categorical"]) >= 1
+    for (ua, va), (ub, vb) in zip(got.categorical_vr, want["categorical"]):
+        assert ua == ub and abs(va - vb) < 1e-4 * abs(vb)
+
+
+def test_no_usable_candidate_is_an_error(case):
+    c = case
+    with pytest.raises(cs.SaigeError):
+        cs.estimate_variance_ratio(c["grm"], c["cand"][:5], np.zeros(5), c["mu"], c["w"],
+                                   c["tau"], cs.TraitType.Binary, c["x"],
+                                   cs.VarianceRatioConfig())
