@@ -370,6 +370,22 @@ def run_ours(args, world, rank, local):
                        "h2d_bytes_per_step": int(spec.bed_len + y.nbytes + x.nbytes),
                        "d2h_bytes_per_step": int(8 * (p + n + 2 * fast.max_iter)),
                        "tau": [float(fr.ai_reml.tau[0]), float(fr.ai_reml.tau[1])]}
+        # the rest of fit-null (fit_null.rs:290-373): the variance ratio over the VR
+        # candidates, in the same call; reported beside the headline, not in it
+        vcfg = cs.VarianceRatioConfig(precision=cs.PREC_MIXED)
+        t0 = time.perf_counter()
+        fv = cs.fit_null_from_bed(hb, n, m, y, x, cs.TraitType.Binary, fast, variance_ratio=True,
+                                  vr_config=vcfg)
+        wall_vr = time.perf_counter() - t0
+        v = fv.variance_ratio
+        line["variance_ratio"] = {
+            "value": v.variance_ratio, "markers_used": v.n_markers_used,
+            "markers_solved": v.n_solved, "blocks": v.n_blocks, "pcg_iters": int(v.pcg_iters),
+            "n_kv": int(v.n_kv), "device_s": v.seconds,
+            "fit_null_with_vr_wall_s": wall_vr,
+            # the reference solves each used marker alone: its PCG iterations plus the
+            # A*0 product of each solve (decomposition.rs:226)
+            "reference_kv_estimate": int(v.pcg_iters + v.n_solved)}
     # the reference's strategy on the same GPU
     plain_kv = None
     if not args.no_plain and world == 1:

@@ -205,7 +205,8 @@ SIGNATURES = {
     "saige_fit_null_from_bed": (
         C.c_int32,
         [_u8, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _d, _d, C.c_int32, C.c_int32,
-         C.c_double, C.c_double, P(AiRemlConfigC), P(AiRemlSummaryC), _d, _d, _d, _i64, _i64],
+         C.c_double, C.c_double, P(AiRemlConfigC), P(AiRemlSummaryC), _d, _d, _d, _i64, _i64,
+         P(VrConfigC), P(VrSummaryC)],
     ),
     "saige_grm_set_profiling": (C.c_int32, [_vp, C.c_int32]),
     "saige_grm_get_stats": (C.c_int32, [_vp, P(GrmStatsC)]),

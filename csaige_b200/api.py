@@ -553,13 +553,17 @@ class FitNullResult:
     ai_reml: AiRemlResult
     m_grm: int
     m_vr: int
+    variance_ratio: Optional["VarianceRatioResult"] = None
 
 
 def fit_null_from_bed(bed, n_fam: int, m_tot: int, y, x, trait_type: TraitType,
                       config: AiRemlConfig = AiRemlConfig(), sample_idx=None,
-                      min_maf: float = 0.01, max_missing: float = 0.15) -> FitNullResult:
+                      min_maf: float = 0.01, max_missing: float = 0.15,
+                      variance_ratio: bool = False,
+                      vr_config: Optional[VarianceRatioConfig] = None) -> FitNullResult:
     """Marker statistics, QC + VR/GRM split, GRM operator and AI-REML in one call
-    (the genotype part of saige-cli fit_null::run)."""
+    (the genotype part of saige-cli fit_null::run), followed by the variance ratio
+    over the VR candidates when variance_ratio is true (fit_null.rs:290-373)."""
     b = _bed_array(bed)
     yy = _f64(y)
     n = yy.size
@@ -573,17 +577,29 @@ def fit_null_from_bed(bed, n_fam: int, m_tot: int, y, x, trait_type: TraitType,
     mu = np.zeros(n)
     trace = np.full(2 * max(config.max_iter, 1), np.nan)
     mg, mv = C.c_int64(), C.c_int64()
+    vsum = _lib.VrSummaryC()
+    vcfg = None
+    if vr_config is not None:
+        vcfg = vr_config.c()
     check(LIB.saige_fit_null_from_bed(
         b.ctypes.data_as(C.POINTER(C.c_uint8)), b.size, n_fam, m_tot, _i64ptr(sidx), n, _dptr(yy),
         _dptr(xc), p, int(trait_type), min_maf, max_missing, C.byref(cfg), C.byref(out),
-        _dptr(alpha), _dptr(mu), _dptr(trace), C.byref(mg), C.byref(mv)))
+        _dptr(alpha), _dptr(mu), _dptr(trace), C.byref(mg), C.byref(mv),
+        C.byref(vcfg) if vcfg is not None else None,
+        C.byref(vsum) if variance_ratio else None))
     it = out.iterations
     res = AiRemlResult(
         tau=np.array([out.tau[0], out.tau[1]]), iterations=it, converged=bool(out.converged),
         mu=mu, working_weights=np.zeros(0), residuals=yy - mu, eta=np.zeros(0), alpha=alpha,
         log_likelihood=out.log_likelihood, n_kv=out.n_kv, n_kv_launches=out.n_kv_launches,
         pcg_iters=out.pcg_iters, seconds=out.seconds, tau_trace=trace[: 2 * it].reshape(-1, 2))
-    return FitNullResult(res, mg.value, mv.value)
+    vr = None
+    if variance_ratio:
+        cats = [(vsum.cat_upper[i], vsum.cat_vr[i]) for i in range(vsum.n_categories)]
+        vr = VarianceRatioResult(vsum.variance_ratio, cats, vsum.n_markers_used, np.zeros(0),
+                                 np.zeros(0, np.int64), vsum.n_solved, vsum.n_blocks,
+                                 vsum.pcg_iters, vsum.n_kv, vsum.seconds)
+    return FitNullResult(res, mg.value, mv.value, vr)
 
 
 def kernel_launches() -> int:

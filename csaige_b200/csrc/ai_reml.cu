@@ -11,6 +11,7 @@
 
 #include "engine.cuh"
 #include "rng.hpp"
+#include "vr.cuh"
 
 namespace saige {
 
@@ -482,7 +483,8 @@ SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64
                                        double min_maf, double max_missing,
                                        const saige_ai_reml_config* cfg,
                                        saige_ai_reml_summary* out, double* alpha, double* mu,
-                                       double* tau_trace, int64_t* m_grm_out, int64_t* m_vr_out) {
+                                       double* tau_trace, int64_t* m_grm_out, int64_t* m_vr_out,
+                                       const saige_vr_config* vr_cfg, saige_vr_summary* vr_out) {
   try {
     set_error("");
     if (!bed || !y || !x || !out || m_tot <= 0) return fail(SAIGE_EINVAL, "null argument").code;
@@ -520,10 +522,47 @@ SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64
                                        gidx.data(), m_grm, gaf.data(), -1, &h);
     if (rc != SAIGE_OK) return rc;
     tm.mark("grm");
+    // the variance-ratio candidates' packed rows outlive the full .bed
+    VrRows vr_rows;
+    std::vector<double> vr_mac;
+    if (vr_out) {
+      vr_mac.resize((size_t)m_vr);
+      for (int64_t j = 0; j < m_vr; ++j) vr_mac[(size_t)j] = mac[(size_t)vidx[(size_t)j]];
+      Status gs = vr_gather_rows(d_bed.as<uint8_t>(), (n_fam + 3) / 4, vidx.data(), m_vr,
+                                 sample_idx, n, vr_rows, h->stream);
+      if (!gs.ok()) {
+        saige_grm_destroy(h);
+        return gs.code;
+      }
+    }
     d_bed.release();  // the handle holds the packed GRM rows
     tm.mark("free bed");
-    rc = saige_fit_ai_reml(h, y, x, n, p, trait, &c, out, alpha, mu, nullptr, nullptr, tau_trace);
+    std::vector<double> mu_v((size_t)n), w_v((size_t)n);
+    rc = saige_fit_ai_reml(h, y, x, n, p, trait, &c, out, alpha, mu_v.data(), nullptr, w_v.data(),
+                           tau_trace);
     tm.mark("fit");
+    if (mu) memcpy(mu, mu_v.data(), (size_t)n * 8);
+    if (rc == SAIGE_OK && vr_out) {
+      saige_vr_config vc;
+      if (vr_cfg) {
+        vc = *vr_cfg;
+      } else {
+        saige_vr_config_default(&vc);
+        vc.precision = c.precision;
+      }
+      if (m_vr == 0) {
+        // fit_null.rs:352-358: no candidate, variance ratio 1
+        *vr_out = saige_vr_summary{};
+        vr_out->variance_ratio = 1.0;
+      } else {
+        std::lock_guard<std::recursive_mutex> lk(h->mu);
+        cudaSetDevice(h->device);
+        Status vs = vr_from_rows(h, vr_rows, vr_mac.data(), mu_v.data(), w_v.data(), out->tau,
+                                 trait, x, p, &vc, vr_out);
+        rc = vs.code;
+      }
+      tm.mark("vr");
+    }
     saige_grm_destroy(h);
     tm.mark("destroy");
     return rc;

@@ -33,6 +33,7 @@
 #include "engine.cuh"
 #include "kernels_vec.cuh"
 #include "rng.hpp"
+#include "vr.cuh"
 
 namespace saige {
 namespace {
@@ -117,9 +118,9 @@ __global__ void vr_mul_rows_kernel(const double* __restrict__ s, const double* _
   if (i < ld) out[(int64_t)c * ld + i] = s[i] * g[(int64_t)c * ld + i];
 }
 
-// Dosages of the candidate markers straight from a device .bed (codes 00,01,10,11 ->
-// 2, NaN, 1, 0 as plink.rs:170-179), samples in subset order.
-__global__ void vr_bed_decode_kernel(const uint8_t* __restrict__ bed, int64_t bpm,
+// Dosages of candidate markers from packed .bed rows in device memory (codes
+// 00,01,10,11 -> 2, NaN, 1, 0 as plink.rs:170-179), samples in subset order.
+__global__ void vr_bed_decode_kernel(const uint8_t* __restrict__ rows, int64_t bpm,
                                      const int64_t* __restrict__ markers,
                                      const int64_t* __restrict__ sample_idx, int64_t n, int64_t ld,
                                      double* __restrict__ out) {
@@ -127,7 +128,7 @@ __global__ void vr_bed_decode_kernel(const uint8_t* __restrict__ bed, int64_t bp
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t s = sample_idx ? sample_idx[i] : i;
-  const uint8_t byte = bed[3 + markers[c] * bpm + s / 4];
+  const uint8_t byte = rows[markers[c] * bpm + s / 4];
   const int code = (byte >> (2 * (s % 4))) & 3;
   out[(int64_t)c * ld + i] = code == 0 ? 2.0 : (code == 2 ? 1.0 : (code == 3 ? 0.0 : (double)NAN));
 }
@@ -391,6 +392,51 @@ Status vr_run(saige_grm* h, const VrFill& fill, int64_t n_cand, const double* ma
     }
   }
   return Status();
+}
+
+}  // namespace saige
+
+namespace saige {
+
+Status vr_gather_rows(const uint8_t* bed_dev, int64_t bpm, const int64_t* vidx, int64_t m_vr,
+                      const int64_t* sample_idx, int64_t n, VrRows& out, cudaStream_t st) {
+  out.bpm = bpm;
+  out.m = m_vr;
+  out.has_sidx = sample_idx != nullptr;
+  if (m_vr > 0) {
+    SG_TRY(out.rows.reserve((size_t)m_vr * (size_t)bpm));
+    for (int64_t j = 0; j < m_vr; ++j)
+      SG_CUDA(cudaMemcpyAsync(out.rows.as<uint8_t>() + j * bpm, bed_dev + 3 + vidx[j] * bpm,
+                              (size_t)bpm, cudaMemcpyDeviceToDevice, st));
+  }
+  if (sample_idx) {
+    SG_TRY(out.sidx.reserve((size_t)n * sizeof(int64_t)));
+    SG_CUDA(cudaMemcpyAsync(out.sidx.ptr, sample_idx, (size_t)n * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, st));
+  }
+  SG_CUDA(cudaStreamSynchronize(st));
+  return Status();
+}
+
+Status vr_from_rows(saige_grm* h, const VrRows& rows, const double* mac, const double* mu,
+                    const double* w, const double tau[2], int trait, const double* x, int p,
+                    const saige_vr_config* cfg, saige_vr_summary* out) {
+  const int64_t n = h->n, ld = h->n_pad;
+  DevBuf dmarkers;
+  SG_TRY(dmarkers.reserve(256 * sizeof(int64_t)));
+  VrFill fill = [&](const std::vector<int64_t>& cand, double* g, cudaStream_t st) -> Status {
+    SG_CUDA(cudaMemcpyAsync(dmarkers.ptr, cand.data(), cand.size() * sizeof(int64_t),
+                            cudaMemcpyHostToDevice, st));
+    vr_bed_decode_kernel<<<dim3(blocks_for(n), (unsigned)cand.size()), kT, 0, st>>>(
+        rows.rows.as<uint8_t>(), rows.bpm, dmarkers.as<int64_t>(),
+        rows.has_sidx ? rows.sidx.as<int64_t>() : nullptr, n, ld, g);
+    count_launches(1);
+    SG_CUDA(cudaGetLastError());
+    // the host vector of indices must outlive the copy
+    SG_CUDA(cudaStreamSynchronize(st));
+    return Status();
+  };
+  return vr_run(h, fill, rows.m, mac, mu, w, tau, trait, x, p, cfg, out, nullptr, nullptr);
 }
 
 }  // namespace saige

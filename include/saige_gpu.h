@@ -326,13 +326,17 @@ int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x, int64_
  * operator over the GRM markers (pcg.rs:101-122) and fit_ai_reml
  * (ai_reml.rs:86-427).  The .bed is copied to the device once.  Phenotype
  * and covariate parsing stay with the caller (y, x as for saige_fit_ai_reml).
- * m_grm / m_vr (optional) receive the marker split sizes. */
+ * m_grm / m_vr (optional) receive the marker split sizes.  When vr_out is not
+ * NULL the variance ratio over the VR candidates follows the fit as in
+ * fit_null.rs:290-373 (vr_cfg NULL: defaults with the fit's precision; no
+ * candidate gives a ratio of 1). */
 int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
                                 const int64_t* sample_idx, int64_t n, const double* y,
                                 const double* x, int32_t p, int32_t trait, double min_maf,
                                 double max_missing, const saige_ai_reml_config* cfg,
                                 saige_ai_reml_summary* out, double* alpha, double* mu,
-                                double* tau_trace, int64_t* m_grm, int64_t* m_vr);
+                                double* tau_trace, int64_t* m_grm, int64_t* m_vr,
+                                const saige_vr_config* vr_cfg, saige_vr_summary* vr_out);
 
 /* ---------------------------------------------------------------------
  * Instrumentation (the reference logs per-phase times through `tracing`,

@@ -109,3 +109,24 @@ def test_no_usable_candidate_is_an_error(case):
         cs.estimate_variance_ratio(c["grm"], c["cand"][:5], np.zeros(5), c["mu"], c["w"],
                                    c["tau"], cs.TraitType.Binary, c["x"],
                                    cs.VarianceRatioConfig())
+
+
+def test_fit_null_from_bed_variance_ratio_equals_the_steps():
+    # the one-call pipeline (device .bed rows) against the same steps through the API
+    n, m = 1500, 3000
+    spec = cs.CohortSpec(n=n, m=m, seed=17, missing_rate=0.01, prevalence=0.2, h2=0.3,
+                         n_covar=2)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    cfg = cs.AiRemlConfig(max_iter=4)
+    fr = cs.fit_null_from_bed(bed, n, m, y, x, cs.TraitType.Binary, cfg, variance_ratio=True)
+    assert fr.variance_ratio is not None and fr.m_vr > 0
+    af, mac, nv = cs.bed_marker_stats(bed, n, m)
+    gidx, vidx = cs.select_grm_markers(af, mac, nv, n, 0.01, 0.15, 12345)
+    grm = cs.OnTheFlyGrm.from_bed(bed, n, m, gidx, af[gidx])
+    fit = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg)
+    assert np.array_equal(fit.tau, fr.ai_reml.tau)
+    vr = cs.estimate_variance_ratio(grm, O.dosages(bed, n, vidx), mac[vidx], fit.mu,
+                                    fit.working_weights, fit.tau, cs.TraitType.Binary, x)
+    assert vr.n_markers_used == fr.variance_ratio.n_markers_used
+    assert vr.variance_ratio == fr.variance_ratio.variance_ratio
