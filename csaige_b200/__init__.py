@@ -19,7 +19,9 @@ from .api import (  # noqa: F401
     PcgResult,
     PcgSolver,
     SaigePcgConfig,
+    LocoChromResult,
     TraitType,
+    run_loco,
     VarianceRatioConfig,
     VarianceRatioResult,
     estimate_variance_ratio,

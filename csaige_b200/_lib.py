@@ -202,6 +202,11 @@ SIGNATURES = {
         C.c_int32,
         [_vp, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _d, _d, _i64],
     ),
+    "saige_fit_loco": (
+        C.c_int32,
+        [_vp, _i32, C.c_int32, _d, _d, C.c_int64, C.c_int32, C.c_int32, P(AiRemlConfigC),
+         P(AiRemlSummaryC), _d, _d, _d],
+    ),
     "saige_fit_null_from_bed": (
         C.c_int32,
         [_u8, _sz, C.c_int64, C.c_int64, _i64, C.c_int64, _d, _d, C.c_int32, C.c_int32,

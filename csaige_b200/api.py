@@ -376,6 +376,58 @@ def fit_ai_reml(y, x, grm: OnTheFlyGrm, trait_type: TraitType,
         tau_trace=trace[: 2 * it].reshape(-1, 2))
 
 
+@dataclass
+class LocoChromResult:
+    """LocoChromResult (loco.rs:25-39)."""
+    chrom: str
+    tau: np.ndarray
+    mu: np.ndarray
+    residuals: np.ndarray
+    working_weights: np.ndarray
+    alpha: np.ndarray
+    iterations: int = 0
+    converged: bool = False
+    n_kv: int = 0
+    seconds: float = 0.0
+
+
+def run_loco(y, x, grm: OnTheFlyGrm, marker_chroms: Sequence[str], trait_type: TraitType,
+             config: AiRemlConfig = AiRemlConfig()) -> dict:
+    """run_loco (loco.rs:54-117) over the GRM handle's markers: marker_chroms gives the
+    chromosome of each GRM marker; one fit per chromosome (sorted by name, as the
+    reference sorts them) with that chromosome left out of the GRM.  Returns
+    {chrom: LocoChromResult}."""
+    yy = _f64(y)
+    n = yy.size
+    if n != grm.n_samples:
+        raise SaigeError(_lib.EINVAL, "y.len() != n_samples")
+    names = [str(c) for c in marker_chroms]
+    if len(names) != grm.n_markers:
+        raise SaigeError(_lib.EINVAL, "one chromosome per GRM marker is required")
+    chroms = sorted(set(names))
+    code = {c: k for k, c in enumerate(chroms)}
+    mc = np.array([code[c] for c in names], dtype=np.int32)
+    xc, p = _design(x, n)
+    cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
+                             config.n_random_vectors, config.seed, config.precision, config.solve,
+                             config.warm_start, 0)
+    k = len(chroms)
+    outs = (_lib.AiRemlSummaryC * k)()
+    alpha = np.zeros((k, p))
+    mu = np.zeros((k, n))
+    w = np.zeros((k, n))
+    check(LIB.saige_fit_loco(grm._h, mc.ctypes.data_as(C.POINTER(C.c_int32)), k, _dptr(yy),
+                             _dptr(xc), n, p, int(trait_type), C.byref(cfg), outs, _dptr(alpha),
+                             _dptr(mu), _dptr(w)))
+    res = {}
+    for i, c in enumerate(chroms):
+        o = outs[i]
+        res[c] = LocoChromResult(c, np.array([o.tau[0], o.tau[1]]), mu[i].copy(), yy - mu[i],
+                                 w[i].copy(), alpha[i].copy(), o.iterations, bool(o.converged),
+                                 o.n_kv, o.seconds)
+    return res
+
+
 # ---------------------------------------------------------------------------
 # synthetic cohorts
 # ---------------------------------------------------------------------------

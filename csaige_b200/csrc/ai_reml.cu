@@ -477,6 +477,74 @@ SG_API int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x,
   }
 }
 
+// run_loco (saige-core/src/glmm/loco.rs:54-117): one fit_ai_reml per chromosome with
+// K over the markers of the other chromosomes.  The packed tiles are shared: the
+// chromosome's markers are masked out between the two passes of every product and the
+// product is scaled by 1/M_-c, which is the GRM the reference rebuilds from the
+// remaining markers.
+namespace {
+struct MaskGuard {
+  saige_grm* h;
+  explicit MaskGuard(saige_grm* g) : h(g) {}
+  ~MaskGuard() { h->masked = false; }
+};
+}  // namespace
+
+SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t n_chrom,
+                              const double* y, const double* x, int64_t n, int32_t p,
+                              int32_t trait, const saige_ai_reml_config* cfg,
+                              saige_ai_reml_summary* out, double* alpha, double* mu, double* w) {
+  try {
+    set_error("");
+    if (!h || !marker_chrom || !y || !x || !out) return fail(SAIGE_EINVAL, "null argument").code;
+    if (n != h->n) return fail(SAIGE_EINVAL, "y.len() != n_samples").code;
+    if (n_chrom <= 0) return fail(SAIGE_EINVAL, "n_chrom must be positive").code;
+    if (p <= 0 || p > 64) return fail(SAIGE_EINVAL, "p must be in 1..64").code;
+    if (trait < 0 || trait > 2) return fail(SAIGE_EINVAL, "unknown trait type").code;
+    for (int64_t j = 0; j < h->m; ++j)
+      if (marker_chrom[j] < 0 || marker_chrom[j] >= n_chrom)
+        return fail(SAIGE_EINVAL, "marker %lld: chromosome code %d outside 0..%d", (long long)j,
+                    marker_chrom[j], n_chrom - 1).code;
+    saige_ai_reml_config c;
+    if (cfg) c = *cfg;
+    else saige_ai_reml_config_default(&c);
+    std::lock_guard<std::recursive_mutex> lk(h->mu);
+    int prev = -1;
+    cudaGetDevice(&prev);
+    cudaSetDevice(h->device);
+    Status s;
+    {
+      MaskGuard guard(h);
+      s = h->excl.reserve((size_t)h->m_pad);
+      std::vector<uint8_t> ex((size_t)h->m_pad, 0);
+      for (int32_t k = 0; s.ok() && k < n_chrom; ++k) {
+        int64_t active = 0;
+        for (int64_t j = 0; j < h->m; ++j) {
+          ex[(size_t)j] = marker_chrom[j] == k ? 1 : 0;
+          active += ex[(size_t)j] ? 0 : 1;
+        }
+        if (cudaMemcpy(h->excl.ptr, ex.data(), ex.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+          s = fail(SAIGE_ECUDA, "mask upload failed");
+          break;
+        }
+        h->m_active = active;
+        h->masked = true;
+        s = fit_impl(h, y, x, n, p, trait, &c, out + k, alpha ? alpha + (int64_t)k * p : nullptr,
+                     mu ? mu + (int64_t)k * n : nullptr, nullptr, w ? w + (int64_t)k * n : nullptr,
+                     nullptr);
+        h->masked = false;
+      }
+    }
+    if (prev >= 0) cudaSetDevice(prev);
+    return s.code;
+  } catch (const std::bad_alloc&) {
+    return fail(SAIGE_ENOMEM, "host allocation failed").code;
+  } catch (...) {
+    return fail(SAIGE_EINVAL, "unexpected C++ exception").code;
+  }
+}
+
+
 SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
                                        int64_t m_tot, const int64_t* sample_idx, int64_t n,
                                        const double* y, const double* x, int32_t p, int32_t trait,

@@ -317,7 +317,7 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
   SG_TRY(h->v32.reserve((size_t)h->n_pad * sizeof(float)));
   SG_TRY(h->u32.reserve((size_t)h->m_pad * sizeof(float)));
   SG_TRY(h->ypart.reserve((size_t)h->n_splits * h->n_pad * sizeof(float)));
-  const float scale = 1.0f / (float)h->m;
+  const float scale = 1.0f / (float)(h->masked ? h->m_active : h->m);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->profiling) {
     SG_CUDA(cudaEventCreate(&e0));
@@ -332,6 +332,7 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
     SG_CUDA(launch_to_f32(vc, h->n, h->n_pad, h->v32.as<float>(), st));
     SG_CUDA(launch_fp32_zt(h->geno, h->wpr, h->zlut, h->m_pad, h->v32.as<float>(),
                            h->u32.as<float>(), st));
+    if (h->masked) SG_CUDA(mask_rows_f32(h->u32.as<float>(), h->excl.as<uint8_t>(), h->m, st));
     SG_CUDA(launch_fp32_z(h->geno, h->wpr, h->zlut, h->m_pad, h->u32.as<float>(),
                           h->ypart.as<float>(), h->n_splits, st));
     SG_CUDA(launch_fp32_finish(h->ypart.as<float>(), h->n_splits, h->n_pad, h->n, scale, oc, st));
@@ -354,7 +355,7 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
 
 Status grm_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
                    int precision, cudaStream_t st) {
-  if (h->m == 0) {
+  if (h->m == 0 || (h->masked && h->m_active == 0)) {
     // pcg.rs:132-134: no markers -> zero vector
     for (int c = 0; c < q; ++c)
       if (!active || active[c] == kColActive)

@@ -54,6 +54,12 @@ struct saige_grm {
   saige::TcPlan* tc = nullptr;
   // generic workspaces
   saige::DevBuf ws_vec, ws_red, ws_cols, ws_io;
+  // Leave-one-chromosome-out: while `masked`, products skip the markers flagged in
+  // excl (m_pad bytes, 1 = left out) and scale by 1/m_active.  Set and cleared only
+  // inside saige_fit_loco, under mu.
+  bool masked = false;
+  int64_t m_active = 0;
+  saige::DevBuf excl;
   // statistics
   int64_t n_kv = 0, n_kv_launches = 0;
   bool profiling = false;

@@ -960,6 +960,9 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       cudaEvent_t t0 = nullptr, t1 = nullptr;
       SG_TRY(mark(&t0));
       SG_CUDA(launch_tc<false>(grid, a, st));
+      // leave-one-chromosome-out: the left-out markers' rows of u do not enter pass B
+      if (h->masked) SG_CUDA(mask_rows_f64(p->u.as<double>(), h->m_pad, r, h->excl.as<uint8_t>(),
+                                           h->m, st));
       SG_TRY(mark(&t1));
       if (h->profiling) ev_a.emplace_back(t0, t1);
       h->stats.tc_pass_a_launches += 1;
@@ -999,7 +1002,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.out = kp;
       a.out_ld = h->n_pad;
       a.col_map = cmap;
-      a.out_scale = 1.0 / (double)h->m;
+      a.out_scale = 1.0 / (double)(h->masked ? h->m_active : h->m);
       a.err = sc.err;
       a.trace = p->tracing ? p->trace.as<unsigned long long>() : nullptr;
       const unsigned grid = (unsigned)(h->n_pad / kRows);

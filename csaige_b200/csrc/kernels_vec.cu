@@ -366,6 +366,14 @@ __global__ void rademacher_kernel(Key8 key, int64_t n, int64_t ld, int nrv, doub
   }
 }
 
+template <class T>
+__global__ void mask_rows_kernel(T* __restrict__ u, int64_t ld, const uint8_t* __restrict__ excl,
+                                 int64_t m) {
+  const int c = blockIdx.y;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m && excl[i]) u[(int64_t)c * ld + i] = T(0);
+}
+
 __global__ void zero_pad_kernel(double* __restrict__ v, int64_t n, int64_t ld) {
   const int c = blockIdx.y;
   const int64_t i = n + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -506,6 +514,19 @@ cudaError_t rademacher_probes_dev(const uint32_t* key, double* out, int64_t n, i
   const int64_t pad = (ld - n) * nrv;
   const int64_t threads = blocks > pad ? blocks : pad;
   rademacher_kernel<<<(unsigned)ceil_div(threads > 0 ? threads : 1, kT), kT, 0, st>>>(k, n, ld, nrv, out);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t mask_rows_f64(double* u, int64_t ld, int q, const uint8_t* excl, int64_t m,
+                          cudaStream_t st) {
+  mask_rows_kernel<double><<<dim3(g1(m), q), kT, 0, st>>>(u, ld, excl, m);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t mask_rows_f32(float* u, const uint8_t* excl, int64_t m, cudaStream_t st) {
+  mask_rows_kernel<float><<<dim3(g1(m), 1), kT, 0, st>>>(u, m, excl, m);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -77,6 +77,11 @@ cudaError_t div_w(const double* v, const double* w, double* out, int64_t n, cuda
 // stream with the given key (ai_reml.rs:121-130).
 cudaError_t rademacher_probes_dev(const uint32_t* key, double* out, int64_t n, int64_t ld, int nrv,
                                   cudaStream_t st);
+// Rows m with excl[m] != 0 set to zero in q columns (ld apart): markers left out of
+// a leave-one-chromosome-out product.
+cudaError_t mask_rows_f64(double* u, int64_t ld, int q, const uint8_t* excl, int64_t m,
+                          cudaStream_t st);
+cudaError_t mask_rows_f32(float* u, const uint8_t* excl, int64_t m, cudaStream_t st);
 cudaError_t zero_pad(double* v, int64_t n, int64_t ld, int q, cudaStream_t st);
 
 }  // namespace saige

@@ -320,6 +320,18 @@ int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x, int64_
                           saige_ai_reml_summary* out, double* alpha, double* mu, double* eta,
                           double* w, double* tau_trace);
 
+/* run_loco (saige-core/src/glmm/loco.rs:54-117): for each chromosome code k in
+ * 0..n_chrom-1, fit_ai_reml with the GRM over the handle's markers whose
+ * marker_chrom (one code per GRM marker) differs from k.  The handle's packed
+ * genotypes are shared; the chromosome's markers are left out of every product
+ * and the product is scaled by 1/M_-k.  out has n_chrom entries; alpha (n_chrom*p),
+ * mu and w (n_chrom*n) are optional.  The reference visits chromosomes in sorted
+ * name order: give codes in that order. */
+int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t n_chrom,
+                       const double* y, const double* x, int64_t n, int32_t p, int32_t trait,
+                       const saige_ai_reml_config* cfg, saige_ai_reml_summary* out,
+                       double* alpha, double* mu, double* w);
+
 /* The fit-null pipeline of saige-cli/src/commands/fit_null.rs:199-287 from
  * host buffers in one call: marker statistics over the sample subset
  * (plink.rs:237-267), QC and the VR/GRM split (fit_null.rs:209-259), the GRM
