@@ -96,6 +96,36 @@ class VrSummaryC(C.Structure):
     ]
 
 
+class NullModelC(C.Structure):
+    _fields_ = [
+        ("trait", C.c_int32),
+        ("p", C.c_int32),
+        ("n", C.c_int64),
+        ("sample_ids", C.POINTER(C.c_char_p)),
+        ("tau", C.c_double * 2),
+        ("alpha", C.POINTER(C.c_double)),
+        ("mu", C.POINTER(C.c_double)),
+        ("y", C.POINTER(C.c_double)),
+        ("x", C.POINTER(C.c_double)),
+        ("xvx_inv_xv", C.POINTER(C.c_double)),
+        ("variance_ratio", C.c_double),
+        ("vr_n_categories", C.c_int32),
+        ("use_loco", C.c_int32),
+        ("vr_cat_upper", C.POINTER(C.c_double)),
+        ("vr_cat_vr", C.POINTER(C.c_double)),
+        ("vr_n_markers_used", C.c_int64),
+        ("vr_per_marker", C.POINTER(C.c_double)),
+        ("vr_n_per_marker", C.c_int64),
+        ("n_loco", C.c_int32),
+        ("use_sparse_grm", C.c_int32),
+        ("loco_chrom", C.POINTER(C.c_char_p)),
+        ("loco_tau", C.POINTER(C.c_double)),
+        ("loco_mu", C.POINTER(C.c_double)),
+        ("loco_residuals", C.POINTER(C.c_double)),
+        ("n_markers_in_grm", C.c_int64),
+    ]
+
+
 class GrmStatsC(C.Structure):
     _fields_ = [
         ("n_kv", C.c_int64),
@@ -172,6 +202,8 @@ SIGNATURES = {
         [_vp, _vp, _vp, C.c_int64, C.c_int32, C.c_int32, _vp],
     ),
     "saige_release_cached_memory": (C.c_int32, []),
+    "saige_write_null_model": (C.c_int32, [C.c_char_p, P(NullModelC)]),
+    "saige_xvx_inv_xv": (C.c_int32, [_d, _d, C.c_int64, C.c_int32, _d]),
     "saige_vr_config_default": (C.c_int32, [P(VrConfigC)]),
     "saige_vr_marker_order": (C.c_int32, [C.c_uint64, C.c_int64, _i64]),
     "saige_estimate_variance_ratio": (

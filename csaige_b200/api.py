@@ -598,6 +598,169 @@ def _rust_f64(x: float) -> str:
 
 
 # ---------------------------------------------------------------------------
+# the .saige.model file (null_model.rs:17-113, serialization.rs:13-34)
+# ---------------------------------------------------------------------------
+@dataclass
+class NullModel:
+    """NullModel (null_model.rs:17-60)."""
+    trait_type: TraitType
+    sample_ids: list
+    tau: np.ndarray
+    alpha: np.ndarray
+    mu: np.ndarray
+    mu2: np.ndarray
+    residuals: np.ndarray
+    y: np.ndarray
+    x_flat: np.ndarray
+    x_ncols: int
+    xvx_inv_xv_flat: np.ndarray
+    variance_ratio: VarianceRatioResult
+    magic: bytes = b"SGMD"
+    version: int = 1
+    n_samples: int = 0
+    n_covariates: int = 0
+    use_loco: bool = False
+    loco_tau: list = field(default_factory=list)
+    loco_mu: list = field(default_factory=list)
+    loco_residuals: list = field(default_factory=list)
+    use_sparse_grm: bool = False
+    n_markers_in_grm: int = 0
+
+
+def xvx_inv_xv(x, working_weights) -> np.ndarray:
+    """(X'WX)^-1 X'W laid out as fit_null.rs:290-305 fills it: a flat p*n array with
+    element (j, i) at j*n + i.  x is n x p."""
+    xa = np.asarray(x, dtype=np.float64)
+    if xa.ndim == 1:
+        xa = xa[:, None]
+    n, p = xa.shape
+    xc = np.ascontiguousarray(xa.T)
+    out = np.empty(p * n)
+    check(LIB.saige_xvx_inv_xv(_dptr(xc), _dptr(_f64(working_weights, n)), n, p, _dptr(out)))
+    return out
+
+
+def save_model(path, trait_type: TraitType, sample_ids: Sequence[str], tau, alpha, mu, y, x,
+               xvx_inv_xv_flat, vr: VarianceRatioResult, loco: Optional[dict] = None,
+               n_markers_in_grm: int = 0, use_sparse_grm: bool = False) -> None:
+    """save_model(NullModel::new(...)) (serialization.rs:13-17, null_model.rs:71-112):
+    the bincode file saige-rs Step 2 loads.  loco: {chrom: LocoChromResult} (fit_null
+    itself writes none)."""
+    yy = _f64(y)
+    n = yy.size
+    xa = np.asarray(x, dtype=np.float64)
+    if xa.ndim == 1:
+        xa = xa[:, None]
+    p = xa.shape[1]
+    keep = []  # owners of the buffers the struct points to
+
+    def dp(a):
+        a = np.ascontiguousarray(a, dtype=np.float64)
+        keep.append(a)
+        return _dptr(a)
+
+    def sp(strs):
+        arr = (C.c_char_p * max(len(strs), 1))(*[str(t).encode() for t in strs])
+        keep.append(arr)
+        return C.cast(arr, C.POINTER(C.c_char_p))
+
+    m = _lib.NullModelC()
+    m.trait = int(trait_type)
+    m.p = p
+    m.n = n
+    m.sample_ids = sp(list(sample_ids))
+    if len(sample_ids) != n:
+        raise SaigeError(_lib.EINVAL, "one sample id per sample is required")
+    m.tau[0], m.tau[1] = float(tau[0]), float(tau[1])
+    m.alpha = dp(_f64(alpha, p))
+    m.mu = dp(_f64(mu, n))
+    m.y = dp(yy)
+    m.x = dp(np.ascontiguousarray(xa.T).ravel())
+    m.xvx_inv_xv = dp(_f64(xvx_inv_xv_flat, p * n))
+    m.variance_ratio = vr.variance_ratio
+    m.vr_n_categories = len(vr.categorical_vr)
+    m.vr_cat_upper = dp(np.array([c[0] for c in vr.categorical_vr] or [0.0]))
+    m.vr_cat_vr = dp(np.array([c[1] for c in vr.categorical_vr] or [0.0]))
+    m.vr_n_markers_used = vr.n_markers_used
+    per = np.asarray(vr.per_marker_vr, dtype=np.float64)
+    m.vr_per_marker = dp(per if per.size else np.zeros(1))
+    m.vr_n_per_marker = per.size
+    loco = loco or {}
+    chroms = list(loco.keys())
+    m.use_loco = 1 if chroms else 0
+    m.n_loco = len(chroms)
+    m.loco_chrom = sp(chroms)
+    m.loco_tau = dp(np.array([loco[c].tau for c in chroms]).ravel() if chroms else np.zeros(1))
+    m.loco_mu = dp(np.array([loco[c].mu for c in chroms]).ravel() if chroms else np.zeros(1))
+    m.loco_residuals = dp(np.array([loco[c].residuals for c in chroms]).ravel()
+                          if chroms else np.zeros(1))
+    m.use_sparse_grm = int(use_sparse_grm)
+    m.n_markers_in_grm = n_markers_in_grm
+    check(LIB.saige_write_null_model(str(path).encode(), C.byref(m)))
+
+
+class _Reader:
+    def __init__(self, data: bytes):
+        self.d, self.o = memoryview(data), 0
+
+    def take(self, k):
+        if self.o + k > len(self.d):
+            raise ValueError("truncated model file")
+        b = self.d[self.o:self.o + k]
+        self.o += k
+        return b
+
+    def u8(self):
+        return self.take(1)[0]
+
+    def u32(self):
+        return int.from_bytes(self.take(4), "little")
+
+    def u64(self):
+        return int.from_bytes(self.take(8), "little")
+
+    def f64(self):
+        return float(np.frombuffer(self.take(8), dtype="<f8")[0])
+
+    def vec(self):
+        k = self.u64()
+        return np.frombuffer(self.take(8 * k), dtype="<f8").copy()
+
+    def str(self):
+        return bytes(self.take(self.u64())).decode()
+
+
+def load_model(path) -> NullModel:
+    """load_model (serialization.rs:20-34): bincode decode, then the magic check."""
+    r = _Reader(open(path, "rb").read())
+    magic = bytes(r.take(4))
+    version = r.u32()
+    trait = TraitType(r.u32())
+    ids = [r.str() for _ in range(r.u64())]
+    n_samples, n_cov = r.u64(), r.u64()
+    tau = np.array([r.f64(), r.f64()])
+    alpha, mu, mu2, resid, y, x = r.vec(), r.vec(), r.vec(), r.vec(), r.vec(), r.vec()
+    x_ncols = r.u64()
+    xvx = r.vec()
+    vr_val = r.f64()
+    cats = [(r.f64(), r.f64()) for _ in range(r.u64())]
+    n_used = r.u64()
+    per = r.vec()
+    use_loco = bool(r.u8())
+    loco_tau = [(r.str(), (r.f64(), r.f64())) for _ in range(r.u64())]
+    loco_mu = [(r.str(), r.vec()) for _ in range(r.u64())]
+    loco_res = [(r.str(), r.vec()) for _ in range(r.u64())]
+    sparse = bool(r.u8())
+    n_grm = r.u64()
+    if magic != b"SGMD":
+        raise ValueError(f"Invalid model file: expected magic bytes b'SGMD', got {magic!r}")
+    vr = VarianceRatioResult(vr_val, cats, n_used, per, np.zeros(0, np.int64))
+    return NullModel(trait, ids, tau, alpha, mu, mu2, resid, y, x, x_ncols, xvx, vr, magic,
+                     version, n_samples, n_cov, use_loco, loco_tau, loco_mu, loco_res, sparse,
+                     n_grm)
+
+
+# ---------------------------------------------------------------------------
 # whole fit-null from host buffers, instrumentation
 # ---------------------------------------------------------------------------
 @dataclass
@@ -652,6 +815,32 @@ def fit_null_from_bed(bed, n_fam: int, m_tot: int, y, x, trait_type: TraitType,
                                  np.zeros(0, np.int64), vsum.n_solved, vsum.n_blocks,
                                  vsum.pcg_iters, vsum.n_kv, vsum.seconds)
     return FitNullResult(res, mg.value, mv.value, vr)
+
+
+def _with_extension(prefix, ext: str) -> str:
+    """std::path::Path::with_extension: replace (or add) the last component's extension."""
+    import os
+    head, tail = os.path.split(str(prefix))
+    dot = tail.rfind(".")
+    stem = tail[:dot] if dot > 0 else tail
+    return os.path.join(head, f"{stem}.{ext}")
+
+
+def save_fit_null(prefix, result: FitNullResult, trait_type: TraitType, sample_ids, y, x) -> tuple:
+    """The files fit_null::run writes (fit_null.rs:376-399): <prefix>.varianceRatio.txt and
+    <prefix>.saige.model, from a fit_null_from_bed result with its variance ratio.  The
+    working weights are max(V(mu), 1e-30) (family.rs:55-66)."""
+    if result.variance_ratio is None:
+        raise SaigeError(_lib.EINVAL, "the result holds no variance ratio")
+    mu = result.ai_reml.mu
+    w = np.maximum(mu * (1 - mu) if trait_type != TraitType.Quantitative
+                   else np.ones_like(mu), 1e-30)
+    vr_path = _with_extension(prefix, "varianceRatio.txt")
+    model_path = _with_extension(prefix, "saige.model")
+    write_variance_ratio_file(result.variance_ratio, vr_path)
+    save_model(model_path, trait_type, sample_ids, result.ai_reml.tau, result.ai_reml.alpha, mu,
+               y, x, xvx_inv_xv(x, w), result.variance_ratio)
+    return model_path, vr_path
 
 
 def kernel_launches() -> int:

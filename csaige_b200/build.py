@@ -30,6 +30,7 @@ SOURCES = [
     "kernels_tc.cu",
     "noalloc.cu",
     "vr.cu",
+    "model.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -163,6 +163,48 @@ int32_t saige_estimate_variance_ratio(saige_grm* h, const double* dosages, const
                                       saige_vr_summary* out, double* per_marker_vr,
                                       int64_t* used_idx);
 
+/* ---------------------------------------------------------------------
+ * The .saige.model file (saige-core/src/model/null_model.rs:17-113,
+ * serialization.rs:13-17): NullModel as bincode 1.3.3 serialises it
+ * ------------------------------------------------------------------- */
+/* The fields of NullModel that the caller supplies; mu2 and the residuals are
+ * computed as NullModel::new does (null_model.rs:83-88).  Arrays are read only. */
+typedef struct saige_null_model {
+  int32_t trait;                  /* SAIGE_TRAIT_* (the TraitType variant index) */
+  int32_t p;                      /* covariates including the intercept (x_ncols) */
+  int64_t n;                      /* samples */
+  const char* const* sample_ids;  /* n UTF-8 strings, model order */
+  double tau[2];
+  const double* alpha;            /* p */
+  const double* mu;               /* n */
+  const double* y;                /* n */
+  const double* x;                /* n x p, column-major */
+  const double* xvx_inv_xv;       /* p x n as fit_null.rs:294-305 fills it (data[j*n + i]) */
+  double variance_ratio;          /* VarianceRatioResult */
+  int32_t vr_n_categories;
+  int32_t use_loco;
+  const double* vr_cat_upper;     /* vr_n_categories */
+  const double* vr_cat_vr;
+  int64_t vr_n_markers_used;
+  const double* vr_per_marker;    /* vr_n_per_marker (may be NULL: empty) */
+  int64_t vr_n_per_marker;
+  int32_t n_loco;                 /* per-chromosome entries (0 as fit_null writes them) */
+  int32_t use_sparse_grm;
+  const char* const* loco_chrom;  /* n_loco */
+  const double* loco_tau;         /* 2 * n_loco */
+  const double* loco_mu;          /* n_loco * n */
+  const double* loco_residuals;   /* n_loco * n */
+  int64_t n_markers_in_grm;       /* 0 as NullModel::new leaves it */
+} saige_null_model;
+
+/* save_model (serialization.rs:13-17): writes path (.saige.model). Host only. */
+int32_t saige_write_null_model(const char* path, const saige_null_model* model);
+
+/* XVX_inv_XV of fit_null.rs:290-305 on the host: XVX = X'WX, its inverse by
+ * Cholesky unit-column solves, out[j*n + i] = sum_k inv(j,k) x(i,k) w(i)
+ * (x n x p column-major, out p*n doubles). Host only. */
+int32_t saige_xvx_inv_xv(const double* x, const double* w, int64_t n, int32_t p, double* out);
+
 /* No counterpart in the reference (memory management).  Device buffers of 256 MiB
  * and more (packed genotypes, tiles, the uploaded .bed) are kept in a per-device
  * cache when released and reused by later allocations of 1 to 1.25 times their size,

@@ -130,3 +130,19 @@ def test_fit_null_from_bed_variance_ratio_equals_the_steps():
                                     fit.working_weights, fit.tau, cs.TraitType.Binary, x)
     assert vr.n_markers_used == fr.variance_ratio.n_markers_used
     assert vr.variance_ratio == fr.variance_ratio.variance_ratio
+
+
+def test_fit_null_outputs_written_and_read_back(tmp_path):
+    n, m = 800, 1500
+    spec = cs.CohortSpec(n=n, m=m, seed=29, prevalence=0.2, h2=0.3, n_covar=2)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    fr = cs.fit_null_from_bed(bed, n, m, y, x, cs.TraitType.Binary, cs.AiRemlConfig(max_iter=3),
+                              variance_ratio=True)
+    ids = [f"s{i}" for i in range(n)]
+    model_path, vr_path = cs.save_fit_null(tmp_path / "example", fr, cs.TraitType.Binary, ids,
+                                           y, x)
+    mdl = cs.load_model(model_path)
+    assert np.array_equal(mdl.tau, fr.ai_reml.tau)
+    assert mdl.variance_ratio.variance_ratio == fr.variance_ratio.variance_ratio
+    assert open(vr_path).read().endswith(" null 1\n")
