@@ -59,6 +59,15 @@ CPU_SAMPLE_MARKERS = 32768
 TC_READ_PER_MARKER_ROW = {"A": 922.8e6 / 18048, "B": 928.5e6 / 18048}
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# Explicit GRM (create-sparse-grm) workload: an FP64 SYRK over all sample pairs, so
+# its size is set by N^2 M / 2 products; N = 32,768 and M = 8,192 give 4.4e12.
+EXPLICIT_GRM = dict(n=32_768, m=8_192, min_maf=0.01, cutoff=0.125)
+# The CPU sample for it: the oracle's compute_dense_grm (reference loop order, all
+# host threads) on N = 4,096 and M = 1,024 of the same cohort.
+EXPLICIT_GRM_CPU = dict(n=4_096, m=1_024)
+# Nominal FP64 pipe of a B200: 148 SMs x 64 FP64 lanes per clock (no measured figure
+# exists for it; the clock is the one sampled during the runs).
+FP64_LANES_PER_SM, N_SMS = 64, 148
 
 
 def parse_args():
@@ -69,6 +78,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-strategy fit")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-explicit-grm", action="store_true",
+                    help="skip the create-sparse-grm workload")
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--m", type=int, default=WORKLOAD["m"])
     return ap.parse_args()
@@ -212,6 +223,61 @@ class CpuSample:
         return (f"OnTheFlyGrm::mat_vec arithmetic (f32, per-thread fold) on {self.markers} of "
                 f"{m_full} markers x {self.n} samples, extrapolated x{m_full / self.markers:.1f} "
                 f"per product and x{kv_fit} products per fit (reference strategy count)")
+
+
+def explicit_grm_block(cs, gpu_index: int) -> dict:
+    """compute_sparse_grm (saige-core/src/grm/sparse.rs:18-66) from host .bed bytes to
+    the sorted sparse triplets, on EXPLICIT_GRM; kernel time from the library's CUDA
+    events, e2e from the call's own clock; the CPU oracle on a bounded sample."""
+    g = EXPLICIT_GRM
+    spec = cs.CohortSpec(n=g["n"], m=g["m"], seed=WORKLOAD["seed"], sib_frac=WORKLOAD["sib_frac"],
+                         cousin_frac=WORKLOAD["cousin_frac"],
+                         missing_rate=WORKLOAD["missing_rate"])
+    bed = cs.gen_bed(spec)
+    out = {"workload": (f"create-sparse-grm: N={g['n']} samples, M={g['m']} markers "
+                        f"(the fit-null cohort generator), min_maf {g['min_maf']}, "
+                        f"cutoff {g['cutoff']}, host .bed in, sorted triplets out")}
+    with ClockSampler(gpu_index) as clk:
+        for arith, key in ((cs.GRM_ARITH_REFERENCE, "reference_arith"),
+                           (cs.GRM_ARITH_FMA, "fma_arith")):
+            ks, tot = [], []
+            for rep in range(4):  # the first is a warm-up
+                sp, used = cs.compute_sparse_grm(bed, g["n"], g["m"], g["min_maf"], g["cutoff"],
+                                                 arith=arith)
+                if rep:
+                    ks.append(sp.info.kernel_seconds)
+                    tot.append(sp.info.total_seconds)
+            k = statistics.median(ks)
+            out[key] = {"kernel_s": k, "e2e_s": statistics.median(tot),
+                        "terms_per_s": sp.info.terms / k}
+    c = clk.summary()
+    mhz = c["sm_mhz"] or c["sm_max_mhz"] or 1965.0
+    peak_ops = N_SMS * FP64_LANES_PER_SM * mhz * 1e6
+    # reference arithmetic: a DMUL and a DADD per product; FMA: one DFMA
+    out["reference_arith"]["fp64_pipe_frac"] = 2 * out["reference_arith"]["terms_per_s"] / peak_ops
+    out["fma_arith"]["fp64_pipe_frac"] = out["fma_arith"]["terms_per_s"] / peak_ops
+    out.update({"terms": sp.info.terms, "n_markers_used": int(used), "nnz": int(sp.vals.size),
+                "fp64_peak": f"nominal {N_SMS} SMs x {FP64_LANES_PER_SM} lanes at {mhz:.0f} MHz",
+                "clocks": c, "parity": "reference_arith bit-identical to the oracle (tests)"})
+    # CPU: the oracle in the reference's loop order on a bounded sample
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_ffi as O
+    cg = EXPLICIT_GRM_CPU
+    cbed = cs.gen_bed(cs.CohortSpec(n=cg["n"], m=cg["m"], seed=WORKLOAD["seed"],
+                                    sib_frac=WORKLOAD["sib_frac"],
+                                    cousin_frac=WORKLOAD["cousin_frac"],
+                                    missing_rate=WORKLOAD["missing_rate"]))
+    times = []
+    for _ in range(2):
+        t0 = time.perf_counter()
+        _, cu = O.dense_grm_bed(cbed, cg["n"], cg["m"], g["min_maf"])
+        times.append(time.perf_counter() - t0)
+    rate = cg["n"] * (cg["n"] + 1) / 2 * cu / min(times)
+    out["cpu_baseline"] = {"terms_per_s": rate, "cores": os.cpu_count(), "kind": "port",
+                           "sample": f"oracle compute_dense_grm on N={cg['n']}, M={cg['m']}",
+                           "extrapolated_s": sp.info.terms / rate}
+    out["speedup_e2e_vs_cpu"] = out["cpu_baseline"]["extrapolated_s"] / out["reference_arith"]["e2e_s"]
+    return out
 
 
 def run_reference(args, rank):
@@ -411,6 +477,8 @@ def run_ours(args, world, rank, local):
         line["cpu_baseline"] = {
             "value": per_kv * kv_fit, "unit": "s", "cores": smp.threads, "kind": "port",
             "sample": smp.describe(m, kv_fit), "sec_per_kv": per_kv}
+    if rank == 0 and world == 1 and not args.no_explicit_grm:
+        line["explicit_grm"] = explicit_grm_block(cs, local)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

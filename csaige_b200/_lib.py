@@ -67,6 +67,26 @@ class AiRemlSummaryC(C.Structure):
     ]
 
 
+class ExplicitGrmConfigC(C.Structure):
+    _fields_ = [
+        ("min_maf", C.c_double),
+        ("relatedness_cutoff", C.c_double),
+        ("arith", C.c_int32),
+        ("device", C.c_int32),
+        ("reserved", C.c_int32 * 4),
+    ]
+
+
+class ExplicitGrmInfoC(C.Structure):
+    _fields_ = [
+        ("n_markers_used", C.c_int64),
+        ("nnz", C.c_int64),
+        ("kernel_seconds", C.c_double),
+        ("total_seconds", C.c_double),
+        ("terms", C.c_double),
+    ]
+
+
 class VrConfigC(C.Structure):
     _fields_ = [
         ("n_markers", C.c_int32),
@@ -204,6 +224,36 @@ SIGNATURES = {
     "saige_release_cached_memory": (C.c_int32, []),
     "saige_write_null_model": (C.c_int32, [C.c_char_p, P(NullModelC)]),
     "saige_xvx_inv_xv": (C.c_int32, [_d, _d, C.c_int64, C.c_int32, _d]),
+    "saige_explicit_grm_config_default": (C.c_int32, [P(ExplicitGrmConfigC)]),
+    "saige_dense_grm_from_bed": (
+        C.c_int32,
+        [_u8, C.c_size_t, C.c_int64, C.c_int64, _i64, C.c_int64, P(ExplicitGrmConfigC), _d,
+         P(ExplicitGrmInfoC)],
+    ),
+    "saige_sparse_grm_from_bed": (
+        C.c_int32,
+        [_u8, C.c_size_t, C.c_int64, C.c_int64, _i64, C.c_int64, P(ExplicitGrmConfigC),
+         P(_vp), P(ExplicitGrmInfoC)],
+    ),
+    "saige_grm_from_dosages": (
+        C.c_int32,
+        [_d, _d, C.c_int64, C.c_int64, P(ExplicitGrmConfigC), _d, P(ExplicitGrmInfoC)],
+    ),
+    "saige_sparse_grm_from_dosages": (
+        C.c_int32,
+        [_d, _d, C.c_int64, C.c_int64, P(ExplicitGrmConfigC), P(_vp), P(ExplicitGrmInfoC)],
+    ),
+    "saige_sparse_grm_n": (C.c_int64, [_vp]),
+    "saige_sparse_grm_nnz": (C.c_int64, [_vp]),
+    "saige_sparse_grm_n_markers": (C.c_int64, [_vp]),
+    "saige_sparse_grm_get": (C.c_int32, [_vp, P(C.c_int32), P(C.c_int32), _d]),
+    "saige_sparse_grm_free": (None, [_vp]),
+    "saige_sparse_grm_from_triplets": (
+        C.c_int32,
+        [C.c_int64, C.c_int64, P(C.c_int32), P(C.c_int32), _d, C.c_int64, P(_vp)],
+    ),
+    "saige_write_sparse_grm": (
+        C.c_int32, [_vp, P(C.c_char_p), C.c_int64, C.c_char_p, C.c_char_p]),
     "saige_vr_config_default": (C.c_int32, [P(VrConfigC)]),
     "saige_vr_marker_order": (C.c_int32, [C.c_uint64, C.c_int64, _i64]),
     "saige_estimate_variance_ratio": (

@@ -31,6 +31,7 @@ SOURCES = [
     "noalloc.cu",
     "vr.cu",
     "model.cu",
+    "grm_explicit.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -138,7 +138,7 @@ void DevBuf::release() {
 // ---------------------------------------------------------------------------
 // device selection
 // ---------------------------------------------------------------------------
-static Status pick_device(int32_t want, int* dev) {
+Status pick_device(int32_t want, int* dev) {
   int count = 0;
   cudaError_t e = cudaGetDeviceCount(&count);
   if (e != cudaSuccess || count == 0) {
@@ -253,7 +253,7 @@ static void grm_free(saige_grm* h) {
   delete h;
 }
 
-static Status check_bed_header(const uint8_t* hdr, size_t bed_len, int64_t n_fam, int64_t m_tot) {
+Status check_bed_header(const uint8_t* hdr, size_t bed_len, int64_t n_fam, int64_t m_tot) {
   if (bed_len < 3) return fail(SAIGE_EBED, "Bed file too small");
   if (hdr[0] != 0x6C || hdr[1] != 0x1B) return fail(SAIGE_EBED, "Invalid PLINK bed file magic number");
   if (hdr[2] != 0x01)
@@ -265,7 +265,7 @@ static Status check_bed_header(const uint8_t* hdr, size_t bed_len, int64_t n_fam
   return Status();
 }
 
-static Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam,
+Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam,
                            std::vector<int32_t>& out, bool& identity) {
   identity = true;
   if (n <= 0) return fail(SAIGE_EINVAL, "n must be positive");
@@ -288,7 +288,7 @@ static Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam,
 }
 
 // Gather rows of a device-resident .bed into the handle (or count only).
-static Status bed_gather_dev(const uint8_t* bed_dev, int64_t n_fam, const std::vector<int64_t>& rows,
+Status bed_gather_dev(const uint8_t* bed_dev, int64_t n_fam, const std::vector<int64_t>& rows,
                              const std::vector<int32_t>& sidx, bool identity, int64_t n,
                              uint32_t* geno_out, int64_t wpr, int64_t* counts_dev,
                              cudaStream_t st) {

@@ -34,6 +34,19 @@ void release_cached_blocks();
 
 struct TcPlan;  // tensor-core path state (kernels_tc.cu)
 
+// Selects (want >= 0) or checks (want < 0: the current) device; fails unless it is sm_100.
+Status pick_device(int32_t want, int* dev);
+// PLINK .bed magic, SNP-major mode and size (plink.rs:80-98).
+Status check_bed_header(const uint8_t* hdr, size_t bed_len, int64_t n_fam, int64_t m_tot);
+// Validates a sample subset (NULL = all n_fam samples in order).
+Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam, std::vector<int32_t>& out,
+                    bool& identity);
+// Gathers .bed rows (device-resident .bed) into packed rows of wpr words and/or
+// per-row {alt count, missing count}; synchronises the stream.
+Status bed_gather_dev(const uint8_t* bed_dev, int64_t n_fam, const std::vector<int64_t>& rows,
+                      const std::vector<int32_t>& sidx, bool identity, int64_t n,
+                      uint32_t* geno_out, int64_t wpr, int64_t* counts_dev, cudaStream_t st);
+
 }  // namespace saige
 
 struct saige_grm {

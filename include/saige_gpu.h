@@ -417,6 +417,94 @@ int32_t saige_grm_reset_stats(saige_grm* h);
 int64_t saige_kernel_launches(void);
 
 /* ---------------------------------------------------------------------
+ * Explicit GRM: replaces compute_dense_grm (saige-core/src/grm/dense.rs:22-112),
+ * compute_grm_from_dosages (dense.rs:115-186), compute_sparse_grm
+ * (grm/sparse.rs:18-66), compute_sparse_grm_from_dosages (sparse.rs:69-98) and
+ * write_sparse_grm (saige-geno/src/sparse_grm_io.rs:73-115), the steps of the
+ * create-sparse-grm command (saige-cli/src/commands/create_sparse_grm.rs:37-71).
+ *
+ * K_ij = (1/M) sum over the M used markers of z_i z_j, each entry one f64 sum in
+ * marker order.  SAIGE_GRM_ARITH_REFERENCE rounds each product and each sum as
+ * the reference does, so K is bit-identical to it; SAIGE_GRM_ARITH_FMA fuses them
+ * (twice the FP64 rate, last-bit differences).
+ * ------------------------------------------------------------------- */
+#define SAIGE_GRM_ARITH_REFERENCE 0
+#define SAIGE_GRM_ARITH_FMA 1
+
+typedef struct {
+  double min_maf;            /* .bed entry points: markers with af < min_maf or
+                                af > 1 - min_maf are skipped (dense.rs:37-39)      */
+  double relatedness_cutoff; /* sparse: keep i == j or |K_ij| >= cutoff            */
+  int32_t arith;             /* SAIGE_GRM_ARITH_*                                  */
+  int32_t device;            /* CUDA device, -1 = current                          */
+  int32_t reserved[4];
+} saige_explicit_grm_config;
+
+typedef struct {
+  int64_t n_markers_used;    /* M (the usize dense.rs:22 returns)                  */
+  int64_t nnz;               /* sparse: stored entries (upper triangle with the
+                                diagonal); dense: n * n                            */
+  double kernel_seconds;     /* the GRM kernel, CUDA events on the call's stream   */
+  double total_seconds;      /* the whole call, host copies included               */
+  double terms;              /* n (n + 1) / 2 * M products summed                  */
+} saige_explicit_grm_info;
+
+/* Sparse GRM result: the upper triangle with the diagonal, sorted by row then
+ * column (the entries write_sparse_grm lists). */
+typedef struct saige_sparse_grm saige_sparse_grm;
+
+/* min_maf 0.01, relatedness_cutoff 0.125 (the command's defaults), reference
+ * arithmetic, current device. */
+int32_t saige_explicit_grm_config_default(saige_explicit_grm_config* cfg);
+
+/* compute_dense_grm on a PLINK .bed (3-byte header + m_tot rows of ceil(n_fam/4)
+ * bytes) over all n_fam samples (sample_idx NULL, n = n_fam) or sample_idx[0..n).
+ * af as MarkerData::compute_af (saige-geno/src/traits.rs:42-54).  out: n x n
+ * (symmetric: row- and column-major agree).  All zeros when no marker is used. */
+int32_t saige_dense_grm_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                 int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                 const saige_explicit_grm_config* cfg, double* out,
+                                 saige_explicit_grm_info* info);
+
+/* compute_sparse_grm: the same K thresholded (sparse.rs:36-53).  *out is freed
+ * with saige_sparse_grm_free. */
+int32_t saige_sparse_grm_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
+                                  int64_t m_tot, const int64_t* sample_idx, int64_t n,
+                                  const saige_explicit_grm_config* cfg, saige_sparse_grm** out,
+                                  saige_explicit_grm_info* info);
+
+/* compute_grm_from_dosages: dosages m x n (row j = marker j, NaN = missing), af[m]
+ * as given; markers with 2 af (1 - af) < 1e-10 are skipped; min_maf is not used.
+ * m == 0 is the 0 x 0 matrix (out not written). */
+int32_t saige_grm_from_dosages(const double* dosages, const double* af, int64_t n, int64_t m,
+                               const saige_explicit_grm_config* cfg, double* out,
+                               saige_explicit_grm_info* info);
+
+/* compute_sparse_grm_from_dosages. */
+int32_t saige_sparse_grm_from_dosages(const double* dosages, const double* af, int64_t n,
+                                      int64_t m, const saige_explicit_grm_config* cfg,
+                                      saige_sparse_grm** out, saige_explicit_grm_info* info);
+
+int64_t saige_sparse_grm_n(const saige_sparse_grm* g);
+int64_t saige_sparse_grm_nnz(const saige_sparse_grm* g);
+int64_t saige_sparse_grm_n_markers(const saige_sparse_grm* g);
+/* Copies the nnz entries (0-based rows and columns). */
+int32_t saige_sparse_grm_get(const saige_sparse_grm* g, int32_t* rows, int32_t* cols,
+                             double* vals);
+void saige_sparse_grm_free(saige_sparse_grm* g);
+/* A sparse GRM from upper-triangle entries sorted by row, then column (0-based),
+ * e.g. to write one read back from a file.  No reference counterpart. */
+int32_t saige_sparse_grm_from_triplets(int64_t n, int64_t nnz, const int32_t* rows,
+                                       const int32_t* cols, const double* vals,
+                                       int64_t n_markers_used, saige_sparse_grm** out);
+
+/* write_sparse_grm: sample IDs one per line to ids_path, then the MatrixMarket
+ * "coordinate real symmetric" header, "n n nnz" and 1-based "i j value" lines
+ * with ten decimals to mtx_path. */
+int32_t saige_write_sparse_grm(const saige_sparse_grm* g, const char* const* sample_ids,
+                               int64_t n_ids, const char* mtx_path, const char* ids_path);
+
+/* ---------------------------------------------------------------------
  * Synthetic cohorts (seeded; no counterpart in the reference — test and
  * benchmark input).  Deterministic functions of the spec: the host and the
  * device generator produce identical bytes.

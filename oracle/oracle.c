@@ -1060,3 +1060,83 @@ int orc_variance_ratio(const double* dosages, const double* mac, int64_t n_cand,
   }
   return 0;
 }
+
+/* ===================================================================== */
+/* Explicit GRM (saige-core/src/grm/dense.rs)                             */
+/* ===================================================================== */
+
+/* The accumulation of dense.rs:66-86 / :147-163 and the scaling of :89-102 /
+ * :165-177, in the reference's loop order: row i keeps row_vals[j - i] for
+ * j >= i and adds gi * z_j for every used marker in turn, so each K_ij (i <= j)
+ * is one f64 sum over the markers in order (multiply, then add); the result is
+ * multiplied by 1/n_used and mirrored. */
+static void orc_grm_accumulate(const double* z, int64_t n, int64_t n_used, double* out) {
+  const double scale = n_used > 0 ? 1.0 / (double)n_used : 0.0;
+#pragma omp parallel
+  {
+    double* row_vals = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
+#pragma omp for schedule(dynamic, 4)
+    for (int64_t i = 0; i < n; ++i) {
+      const int64_t len = n - i;
+      for (int64_t k = 0; k < len; ++k) row_vals[k] = 0.0;
+      for (int64_t mk = 0; mk < n_used; ++mk) {
+        const double* zk = z + mk * n;
+        const double gi = zk[i];
+        for (int64_t k = 0; k < len; ++k) row_vals[k] += gi * zk[i + k];
+      }
+      for (int64_t k = 0; k < len; ++k) {
+        const double v = n_used > 0 ? row_vals[k] * scale : 0.0;
+        out[i * n + i + k] = v;
+        out[(i + k) * n + i] = v;
+      }
+    }
+    free(row_vals);
+  }
+}
+
+/* dense.rs:46-58 / :129-140: standardise one marker; returns 0 when skipped. */
+static int orc_grm_std_marker(const double* d, int64_t n, double af, double* z) {
+  const double var = 2.0 * af * (1.0 - af);
+  if (var < 1e-10) return 0;
+  const double sd = sqrt(var);
+  const double mean = 2.0 * af;
+  for (int64_t i = 0; i < n; ++i) {
+    const double di = isnan(d[i]) ? mean : d[i];
+    z[i] = (di - mean) / sd;
+  }
+  return 1;
+}
+
+int orc_dense_grm_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                      const int64_t* sample_idx, int64_t n, double min_maf, double* out,
+                      int64_t* n_used) {
+  const int64_t bpm = (n_fam + 3) / 4;
+  if (bed_len < 3 || (int64_t)bed_len < 3 + bpm * m_tot) return -1;
+  if (bed[0] != 0x6C || bed[1] != 0x1B || bed[2] != 0x01) return -1;
+  double* z = (double*)malloc(sizeof(double) * (size_t)(m_tot > 0 ? m_tot : 1) * (size_t)n);
+  double* d = (double*)malloc(sizeof(double) * (size_t)n);
+  int64_t used = 0;
+  for (int64_t j = 0; j < m_tot; ++j) {
+    double af, mac;
+    int64_t nv;
+    orc_read_marker(bed, bpm, n_fam, j, sample_idx, n, d);
+    orc_compute_af(d, n, &af, &mac, &nv);
+    if (af < min_maf || af > 1.0 - min_maf) continue; /* dense.rs:37-39 */
+    used += orc_grm_std_marker(d, n, af, z + used * n);
+  }
+  orc_grm_accumulate(z, n, used, out);
+  *n_used = used;
+  free(d);
+  free(z);
+  return 0;
+}
+
+void orc_grm_from_dosages(const double* dosages, const double* af, int64_t n, int64_t m,
+                          double* out, int64_t* n_used) {
+  double* z = (double*)malloc(sizeof(double) * (size_t)(m > 0 ? m : 1) * (size_t)n);
+  int64_t used = 0;
+  for (int64_t j = 0; j < m; ++j) used += orc_grm_std_marker(dosages + j * n, n, af[j], z + used * n);
+  orc_grm_accumulate(z, n, used, out);
+  *n_used = used;
+  free(z);
+}

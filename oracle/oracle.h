@@ -171,6 +171,21 @@ int orc_variance_ratio(const double* dosages, const double* mac, int64_t n_cand,
                        const orc_vr_config* cfg, orc_vr_summary* out, double* per_marker_vr,
                        int64_t* used_idx);
 
+/* ---- explicit GRM (saige-core/src/grm/dense.rs, grm/sparse.rs) -------- */
+/* compute_dense_grm (dense.rs:22-112): markers of the .bed (all n_fam
+ * samples, or sample_idx[0..n)) whose af (traits.rs:42-54) is within
+ * [min_maf, 1 - min_maf] and whose 2 af (1 - af) is at least 1e-10, z =
+ * (d - 2 af) / sqrt(2 af (1 - af)) with a missing call at the mean (z = 0),
+ * K_ij = (sum over markers in file order of z_i * z_j, f64 multiply then add)
+ * * (1 / n_used); all zeros when no marker is used.  out: n x n. */
+int orc_dense_grm_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                      const int64_t* sample_idx, int64_t n, double min_maf, double* out,
+                      int64_t* n_used);
+/* compute_grm_from_dosages (dense.rs:115-186): dosages m x n (row per marker,
+ * NaN = missing), af as given, only the 2 af (1 - af) < 1e-10 skip. */
+void orc_grm_from_dosages(const double* dosages, const double* af, int64_t n, int64_t m,
+                          double* out, int64_t* n_used);
+
 #ifdef __cplusplus
 }
 #endif

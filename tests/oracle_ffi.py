@@ -292,3 +292,64 @@ def variance_ratio(dosages, mac, mu, w, tau, trait: int, x: np.ndarray, kind: in
     return dict(rc=rc, variance_ratio=out.variance_ratio, n_used=k, per_marker=vr[:k].copy(),
                 used=used[:k].copy(), n_kv=out.n_kv,
                 categorical=[(out.cat_upper[i], out.cat_vr[i]) for i in range(out.n_categories)])
+
+
+# ---- explicit GRM (saige-core/src/grm/dense.rs, grm/sparse.rs) -------------
+L.orc_dense_grm_bed.argtypes = [P(C.c_uint8), C.c_size_t, C.c_int64, C.c_int64, _i64, C.c_int64,
+                                C.c_double, _d, _i64]
+L.orc_grm_from_dosages.argtypes = [_d, _d, C.c_int64, C.c_int64, _d, _i64]
+
+
+def dense_grm_bed(bed: np.ndarray, n_fam: int, m_tot: int, min_maf=0.01, sample_idx=None):
+    """compute_dense_grm (dense.rs:22-112): (K n x n, n_markers_used)."""
+    sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
+    n = n_fam if sidx is None else sidx.size
+    out = np.empty((n, n))
+    used = np.zeros(1, dtype=np.int64)
+    rc = L.orc_dense_grm_bed(bed.ctypes.data_as(P(C.c_uint8)), bed.size, n_fam, m_tot, ip(sidx), n,
+                             min_maf, dp(out), ip(used))
+    if rc != 0:
+        raise ValueError("malformed bed")
+    return out, int(used[0])
+
+
+def grm_from_dosages(dos: np.ndarray, af):
+    """compute_grm_from_dosages (dense.rs:115-186); m == 0 gives a 0 x 0 matrix."""
+    dos = f64(dos)
+    m, n = dos.shape
+    if m == 0:
+        return np.zeros((0, 0)), 0
+    out = np.empty((n, n))
+    used = np.zeros(1, dtype=np.int64)
+    L.orc_grm_from_dosages(dp(dos), dp(f64(af)), n, m, dp(out), ip(used))
+    return out, int(used[0])
+
+
+def sparse_from_dense(k: np.ndarray, cutoff: float):
+    """sparse.rs:36-53 thresholding, stored as the writer lists it
+    (sparse_grm_io.rs:92-107): upper triangle with the diagonal, row-major,
+    (rows, cols, vals) 0-based."""
+    n = k.shape[0]
+    iu, ju = np.triu_indices(n)
+    v = k[iu, ju]
+    keep = (iu == ju) | (np.abs(v) >= cutoff)
+    return iu[keep].astype(np.int32), ju[keep].astype(np.int32), v[keep]
+
+
+def sparse_grm_text(n: int, rows, cols, vals) -> str:
+    """The .sparseGRM.mtx text write_sparse_grm produces (sparse_grm_io.rs:73-115);
+    Rust's {:.10} and C's %.10f both print the exact decimal value rounded."""
+    lines = ["%%MatrixMarket matrix coordinate real symmetric", f"{n} {n} {len(vals)}"]
+    lines += ["%d %d %.10f" % (i + 1, j + 1, v) for i, j, v in zip(rows, cols, vals)]
+    return "\n".join(lines) + "\n"
+
+
+def gen_f64(rng: ChaChaRng) -> float:
+    """rand 0.8 Standard for f64: the top 53 bits of next_u64, times 2^-53."""
+    return (L.orc_rng_next_u64(C.byref(rng)) >> 11) * (1.0 / (1 << 53))
+
+
+def chacha8(seed: int) -> ChaChaRng:
+    r = ChaChaRng()
+    L.orc_chacha_seed_from_u64(C.byref(r), seed, 8)
+    return r
