@@ -80,6 +80,11 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-explicit-grm", action="store_true",
                     help="skip the create-sparse-grm workload")
+    ap.add_argument("--explicit-grm-only", action="store_true",
+                    help="run only the create-sparse-grm workload and print its block")
+    ap.add_argument("--grm-n", type=int, default=EXPLICIT_GRM["n"])
+    ap.add_argument("--grm-m", type=int, default=EXPLICIT_GRM["m"])
+    ap.add_argument("--grm-reps", type=int, default=4, help="runs per arithmetic, first untimed")
     ap.add_argument("--n", type=int, default=WORKLOAD["n"])
     ap.add_argument("--m", type=int, default=WORKLOAD["m"])
     return ap.parse_args()
@@ -225,11 +230,12 @@ class CpuSample:
                 f"per product and x{kv_fit} products per fit (reference strategy count)")
 
 
-def explicit_grm_block(cs, gpu_index: int) -> dict:
+def explicit_grm_block(cs, gpu_index: int, n: int, m: int, reps: int = 4,
+                       cpu: bool = True) -> dict:
     """compute_sparse_grm (saige-core/src/grm/sparse.rs:18-66) from host .bed bytes to
     the sorted sparse triplets, on EXPLICIT_GRM; kernel time from the library's CUDA
     events, e2e from the call's own clock; the CPU oracle on a bounded sample."""
-    g = EXPLICIT_GRM
+    g = dict(EXPLICIT_GRM, n=n, m=m)
     spec = cs.CohortSpec(n=g["n"], m=g["m"], seed=WORKLOAD["seed"], sib_frac=WORKLOAD["sib_frac"],
                          cousin_frac=WORKLOAD["cousin_frac"],
                          missing_rate=WORKLOAD["missing_rate"])
@@ -241,7 +247,7 @@ def explicit_grm_block(cs, gpu_index: int) -> dict:
         for arith, key in ((cs.GRM_ARITH_REFERENCE, "reference_arith"),
                            (cs.GRM_ARITH_FMA, "fma_arith")):
             ks, tot = [], []
-            for rep in range(4):  # the first is a warm-up
+            for rep in range(max(reps, 2)):  # the first is a warm-up
                 sp, used = cs.compute_sparse_grm(bed, g["n"], g["m"], g["min_maf"], g["cutoff"],
                                                  arith=arith)
                 if rep:
@@ -259,6 +265,8 @@ def explicit_grm_block(cs, gpu_index: int) -> dict:
     out.update({"terms": sp.info.terms, "n_markers_used": int(used), "nnz": int(sp.vals.size),
                 "fp64_peak": f"nominal {N_SMS} SMs x {FP64_LANES_PER_SM} lanes at {mhz:.0f} MHz",
                 "clocks": c, "parity": "reference_arith bit-identical to the oracle (tests)"})
+    if not cpu:
+        return out
     # CPU: the oracle in the reference's loop order on a bounded sample
     sys.path.insert(0, str(ROOT / "tests"))
     import oracle_ffi as O
@@ -478,7 +486,8 @@ def run_ours(args, world, rank, local):
             "value": per_kv * kv_fit, "unit": "s", "cores": smp.threads, "kind": "port",
             "sample": smp.describe(m, kv_fit), "sec_per_kv": per_kv}
     if rank == 0 and world == 1 and not args.no_explicit_grm:
-        line["explicit_grm"] = explicit_grm_block(cs, local)
+        line["explicit_grm"] = explicit_grm_block(cs, local, args.grm_n, args.grm_m,
+                                                  args.grm_reps)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -490,6 +499,15 @@ def main():
     world, rank, local = dist_setup()
     if args.impl == "reference":
         run_reference(args, rank)
+        return
+    if args.explicit_grm_only:
+        if rank == 0:
+            import torch
+
+            import csaige_b200 as cs
+            torch.cuda.set_device(local)
+            print(json.dumps(explicit_grm_block(cs, local, args.grm_n, args.grm_m, args.grm_reps,
+                                                cpu=False)), flush=True)
         return
     run_ours(args, world, rank, local)
 

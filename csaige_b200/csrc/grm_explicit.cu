@@ -47,9 +47,9 @@ constexpr int kT = 128;    // samples per tile side
 constexpr int kKc = 32;    // markers per shared-memory stage
 constexpr int kThr = 256;  // 16 x 16 threads, 8 x 8 entries each
 constexpr int kWordsSide = kT / 16;
-constexpr size_t kSmemBytes = (size_t)2 * kKc * kT * sizeof(double)   // z, both sides
-                              + (size_t)kKc * 4 * sizeof(double)       // z table of the stage
-                              + (size_t)2 * kKc * kWordsSide * 4;      // packed words
+constexpr size_t kSmemBytes = 2 * ((size_t)2 * kKc * kT * sizeof(double)   // z, both sides
+                                   + (size_t)kKc * 4 * sizeof(double)       // z table
+                                   + (size_t)2 * kKc * kWordsSide * 4);     // packed words
 
 struct SyrkArgs {
   const uint32_t* geno = nullptr;  // packed rows (m_pad x wpr words), or
@@ -78,10 +78,17 @@ __device__ __forceinline__ int code_shift(int e) {
 
 template <bool kPacked, bool kFma, bool kSparse>
 __global__ void __launch_bounds__(kThr, 1) grm_syrk_kernel(const SyrkArgs a) {
+  // Two stages in flight: while the threads multiply stage c out of zs[c & 1], each
+  // k-step also decodes 1/32 of stage c + 1 into zs[(c + 1) & 1], from the packed
+  // words stored (before the previous barrier) in sraw[(c + 1) & 1]; the words of
+  // stage c + 2 are loaded into registers at the start of stage c.  One barrier per
+  // stage separates every write of a buffer from its reads.
   extern __shared__ __align__(16) double smem[];
-  double* zs = smem;                   // [side][k][s], side 0 = rows i, 1 = columns j
-  double* slut = zs + 2 * kKc * kT;    // [k][code]
-  uint32_t* sraw = reinterpret_cast<uint32_t*>(slut + kKc * 4);  // [side][k][word]
+  double* zs = smem;                       // [buf][side][k][s], side 0 = rows i, 1 = columns j
+  double* slut = zs + 2 * 2 * kKc * kT;    // [buf][k][code]
+  uint32_t* sraw = reinterpret_cast<uint32_t*>(slut + 2 * kKc * 4);  // [buf][side][k][word]
+  constexpr int kZ = 2 * kKc * kT;         // doubles per z buffer
+  constexpr int kRaw = 2 * kKc * kWordsSide;
   const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
   const int2 tile = a.tiles[blockIdx.x];
   const int64_t i0 = (int64_t)tile.x * kT, j0 = (int64_t)tile.y * kT;
@@ -89,11 +96,11 @@ __global__ void __launch_bounds__(kThr, 1) grm_syrk_kernel(const SyrkArgs a) {
 
   uint32_t wreg0 = 0, wreg1 = 0;
   double lreg = 0.0;
-  // Packed source: thread t holds word v = t and v = t + 256 of the stage,
-  // v = (side * kKc + k) * 8 + w.
-  auto fetch = [&](int c) {
+  // Packed source: thread t loads words v = t and v = t + 256 of stage q,
+  // v = (side * kKc + k) * 8 + w, and table entry t of it (t < 128).
+  auto fetch = [&](int q) {
     if constexpr (kPacked) {
-      const int64_t row0 = (int64_t)c * kKc;
+      const int64_t row0 = (int64_t)q * kKc;
       {
         const int v = tid, side = v >> 8, k = (v >> 3) & (kKc - 1), w = v & 7;
         wreg0 = __ldg(a.geno + (row0 + k) * a.wpr + (side ? j0 : i0) / 16 + w);
@@ -105,32 +112,27 @@ __global__ void __launch_bounds__(kThr, 1) grm_syrk_kernel(const SyrkArgs a) {
       if (tid < kKc * 4) lreg = __ldg(a.lut + row0 * 4 + tid);
     }
   };
-  // Fills zs with stage c.  Every thread reaches the first barrier only after its
-  // reads of zs for the previous stage, so the decode may overwrite it.
-  auto stage = [&](int c) {
+  auto store_raw = [&](int q) {
     if constexpr (kPacked) {
-      sraw[tid] = wreg0;
-      sraw[tid + kThr] = wreg1;
-      if (tid < kKc * 4) slut[tid] = lreg;
-      __syncthreads();
-#pragma unroll 4
-      for (int it = 0; it < 2 * kKc * kT / kThr; ++it) {
-        const int v = tid + it * kThr;  // side = v >> 12, k = (v >> 7) & 31, s = v & 127
-        const int k = (v >> 7) & (kKc - 1), s = v & (kT - 1);
-        const uint32_t word = sraw[(v >> 7) * kWordsSide + (s >> 4)];
-        zs[v] = slut[k * 4 + ((word >> code_shift(s & 15)) & 3u)];
-      }
-    } else {
-      __syncthreads();
-      const int64_t row0 = (int64_t)c * kKc;
-#pragma unroll 4
-      for (int it = 0; it < 2 * kKc * kT / kThr; ++it) {
-        const int v = tid + it * kThr;
-        const int side = v >> 12, k = (v >> 7) & (kKc - 1), s = v & (kT - 1);
-        zs[v] = __ldg(a.z + (row0 + k) * a.ldz + (side ? j0 : i0) + s);
-      }
+      uint32_t* r = sraw + (q & 1) * kRaw;
+      r[tid] = wreg0;
+      r[tid + kThr] = wreg1;
+      if (tid < kKc * 4) slut[(q & 1) * kKc * 4 + tid] = lreg;
     }
-    __syncthreads();
+  };
+  // Decode slice `it` (0..31) of stage q: entry v = tid + 256 it of its z buffer,
+  // v = (side * kKc + k) * kT + s.
+  auto decode = [&](int q, int it) {
+    const int v = tid + it * kThr;
+    const int k = (v >> 7) & (kKc - 1), s = v & (kT - 1);
+    double* z = zs + (q & 1) * kZ;
+    if constexpr (kPacked) {
+      const uint32_t word = sraw[(q & 1) * kRaw + (v >> 7) * kWordsSide + (s >> 4)];
+      z[v] = slut[(q & 1) * kKc * 4 + k * 4 + ((word >> code_shift(s & 15)) & 3u)];
+    } else {
+      const int side = v >> 12;
+      z[v] = __ldg(a.z + ((int64_t)q * kKc + k) * a.ldz + (side ? j0 : i0) + s);
+    }
   };
 
   double acc[8][8];
@@ -139,12 +141,21 @@ __global__ void __launch_bounds__(kThr, 1) grm_syrk_kernel(const SyrkArgs a) {
 #pragma unroll
     for (int q = 0; q < 8; ++q) acc[r][q] = 0.0;
 
+  // prologue: stage 0 decoded, the words of stage 1 in shared memory
   fetch(0);
-  stage(0);
+  store_raw(0);
+  if (nch > 1) fetch(1);
+  __syncthreads();
+#pragma unroll 4
+  for (int it = 0; it < kKc; ++it) decode(0, it);
+  if (nch > 1) store_raw(1);
+  __syncthreads();
+
   for (int c = 0; c < nch; ++c) {
-    if (c + 1 < nch) fetch(c + 1);
-    const double* zi = zs + ty;
-    const double* zj = zs + kKc * kT + tx;
+    const bool next = c + 1 < nch;
+    if (c + 2 < nch) fetch(c + 2);
+    const double* zi = zs + (c & 1) * kZ + ty;
+    const double* zj = zs + (c & 1) * kZ + kKc * kT + tx;
 #pragma unroll 2
     for (int k = 0; k < kKc; ++k) {
       double x[8], y[8];
@@ -152,6 +163,7 @@ __global__ void __launch_bounds__(kThr, 1) grm_syrk_kernel(const SyrkArgs a) {
       for (int r = 0; r < 8; ++r) x[r] = zi[k * kT + 16 * r];
 #pragma unroll
       for (int q = 0; q < 8; ++q) y[q] = zj[k * kT + 16 * q];
+      if (next) decode(c + 1, k);
 #pragma unroll
       for (int r = 0; r < 8; ++r)
 #pragma unroll
@@ -162,7 +174,9 @@ __global__ void __launch_bounds__(kThr, 1) grm_syrk_kernel(const SyrkArgs a) {
             acc[r][q] = __dadd_rn(acc[r][q], __dmul_rn(x[r], y[q]));
         }
     }
-    if (c + 1 < nch) stage(c + 1);
+    // sraw[c & 1] was last read while stage c was decoded, before the previous barrier
+    if (c + 2 < nch) store_raw(c + 2);
+    __syncthreads();
   }
 
   const bool diag = tile.x == tile.y;
