@@ -78,6 +78,8 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-strategy fit")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--warm", choices=["previous", "recycled", "learned"], default="recycled",
+                    help="PCG start of the fast configuration")
     ap.add_argument("--no-explicit-grm", action="store_true",
                     help="skip the create-sparse-grm workload")
     ap.add_argument("--explicit-grm-only", action="store_true",
@@ -358,8 +360,9 @@ def run_ours(args, world, rank, local):
     torch.cuda.synchronize()
     torch.cuda.empty_cache()
 
-    fast = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
-                           warm_start=cs.WARM_PREVIOUS)
+    warm = {"previous": cs.WARM_PREVIOUS, "recycled": cs.WARM_RECYCLED,
+            "learned": cs.WARM_LEARNED}[args.warm]
+    fast = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK, warm_start=warm)
     for _ in range(args.warmup):
         cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, fast)
     grm.reset_stats()
@@ -427,7 +430,7 @@ def run_ours(args, world, rank, local):
         "n_kv_launches": int(last.n_kv_launches), "wall_s_per_step": wall / args.steps,
         "gpu_launches": int(launches), "roofline": roof, "clocks": clk.summary(),
         "markers_grm": int(m_grm), "markers_vr": int(len(vidx)),
-        "fast_config": "MIXED + block PCG + previous-iterate warm start",
+        "fast_config": f"MIXED + block PCG + {args.warm} warm start",
     }
 
     # end to end through the host-buffer C ABI

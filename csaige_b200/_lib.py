@@ -26,7 +26,7 @@ STATUS_NAMES = {
 PREC_FP32, PREC_MIXED = 0, 1
 TRAIT_BINARY, TRAIT_QUANTITATIVE, TRAIT_SURVIVAL = 0, 1, 2
 SOLVE_SINGLE, SOLVE_BLOCK = 0, 1
-WARM_ZERO, WARM_PREVIOUS, WARM_LEARNED = 0, 1, 2
+WARM_ZERO, WARM_PREVIOUS, WARM_LEARNED, WARM_RECYCLED = 0, 1, 2, 3
 
 
 class SaigeError(RuntimeError):

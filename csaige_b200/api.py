@@ -34,6 +34,7 @@ SOLVE_BLOCK = _lib.SOLVE_BLOCK
 WARM_ZERO = _lib.WARM_ZERO
 WARM_PREVIOUS = _lib.WARM_PREVIOUS
 WARM_LEARNED = _lib.WARM_LEARNED
+WARM_RECYCLED = _lib.WARM_RECYCLED
 
 
 class TraitType(enum.IntEnum):

@@ -32,6 +32,7 @@ SOURCES = [
     "vr.cu",
     "model.cu",
     "grm_explicit.cu",
+    "warm.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

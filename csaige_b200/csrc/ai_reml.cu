@@ -12,6 +12,7 @@
 #include "engine.cuh"
 #include "rng.hpp"
 #include "vr.cuh"
+#include "warm.cuh"
 
 namespace saige {
 
@@ -60,7 +61,7 @@ struct Fit {
   // device vectors
   double *y, *x, *eta, *mu, *w, *wmax, *d, *ytil;
   double *rhs, *sol;      // n_pad x q each: [ytil | X | U], [Sinv ytil | Sinv X | Sinv U]
-  double *ku, *pu, *tmpq; // n_pad x nrv
+  double *kxu, *ku, *pu, *tmpq; // K [X | U] (n_pad x (p + nrv)); ku = its U part; n_pad x nrv
   double *py, *kpy, *pk, *invw_py, *pw, *pk_raw, *pw_raw;
   double *dsmall;         // small device scratch (coefficients, dot results)
   double *partial;
@@ -88,10 +89,13 @@ Status coldots(Fit& f, const double* a, const double* b, int q, std::vector<doub
 }
 
 // PCG of Sigma = tau0 W^-1 + tau1 K on q columns of b into x (x0 optional).
-Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const double tau[2]) {
+Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const double tau[2],
+             const double* ax0 = nullptr, double* r_out = nullptr) {
   PcgRun run;
   run.b = b;
   run.x0 = x0;
+  run.ax0 = x0 ? ax0 : nullptr;
+  run.r_out = r_out;
   run.wv = f.wmax;
   run.d = f.d;
   run.tau0 = tau[0];
@@ -128,6 +132,184 @@ Status copy_cols(Fit& f, const double* src, double* dst, int q) {
   return Status();
 }
 
+// ---- recycled starts -------------------------------------------------------
+// A start x0 = V g with Sigma x0 = (Sigma V) g known needs no GRM product for its
+// residual.  V holds vectors whose Sigma-image is known without a product of its
+// own: X and the probes U (K X and K U come from one launch per fit), the block
+// solutions of the previous iteration and the previous AI solutions (their K-images
+// ride in the K Py launch, whose cost hardly grows with the column count), and, for
+// the AI solves, this iteration's block solutions (Sigma x = b - r exactly).
+// g solves the Galerkin system (V' Sigma V) g = V' b, the start of least
+// Sigma-norm error in span V; the solve is then an ordinary PCG from x0.
+struct Recycle {
+  int mb_max = 0, nk = 0;
+  DevBuf mem;                           // one block (large blocks are cached)
+  double *v, *av, *x0, *ax0, *br;       // basis, images (+ b), start, its image, block r
+  double *kin, *kout;                   // [Py | X*_t | pk' | pw'] and its K-image
+  double *gam, *gpart, *gout;
+  bool have_ksol = false;               // kout holds K X*_t of the previous iteration
+  bool have_kpk = false, have_kpw = false;  // K of the previous AI solutions is in kout
+  int at_pk = 0, at_pw = 0;                  // their columns in kout
+  int64_t fallbacks = 0;
+};
+
+Status recycle_init(Fit& f, Recycle& rc) {
+  const size_t ld = (size_t)f.ld, q = (size_t)f.q;
+  rc.mb_max = 2 * f.q + 1;
+  rc.nk = f.q + 3;
+  const size_t mb = (size_t)rc.mb_max, nk = (size_t)rc.nk;
+  const size_t ncol = mb + (mb + q) + 3 * q + 2 * nk;
+  const size_t nsmall = mb * q + gram_partial_doubles(f.n, (int)mb, (int)(mb + q)) + mb * (mb + q);
+  SG_TRY(rc.mem.reserve((ncol * ld + nsmall) * 8));
+  double* b = rc.mem.as<double>();
+  SG_CUDA(cudaMemsetAsync(b, 0, ncol * ld * 8, f.st));  // padding rows stay zero
+  rc.v = b;                 b += mb * ld;
+  rc.av = b;                b += (mb + q) * ld;
+  rc.x0 = b;                b += q * ld;
+  rc.ax0 = b;               b += q * ld;
+  rc.br = b;                b += q * ld;
+  rc.kin = b;               b += nk * ld;
+  rc.kout = b;              b += nk * ld;
+  rc.gam = b;               b += mb * q;
+  rc.gout = b;              b += mb * (mb + q);
+  rc.gpart = b;
+  return Status();
+}
+
+// Coefficients g (mb x q, row-major) of (V' A V) g = V' B from the Gram block
+// gall = V' [A V | B] (mb x (mb + q)): Jacobi-scaled, with the smallest ridge
+// (relative 1e-12 .. 1e-6) under which the Cholesky factorisation succeeds.
+bool galerkin_coeffs(const std::vector<double>& gall, int mb, int q, std::vector<double>& gam) {
+  const int w = mb + q;
+  std::vector<double> s((size_t)mb), a((size_t)mb * mb), l;
+  for (int i = 0; i < mb; ++i) {
+    const double d = gall[(size_t)i * w + i];
+    s[(size_t)i] = (d > 0.0 && std::isfinite(d)) ? 1.0 / sqrt(d) : 0.0;
+  }
+  bool ok = false;
+  for (double ridge : {1e-12, 1e-10, 1e-8, 1e-6}) {
+    for (int i = 0; i < mb; ++i)
+      for (int j = 0; j < mb; ++j) {
+        double v = 0.5 * (gall[(size_t)i * w + j] + gall[(size_t)j * w + i]) * s[(size_t)i] *
+                   s[(size_t)j];
+        if (i == j) v = (s[(size_t)i] > 0.0 ? v : 1.0) + ridge;
+        a[(size_t)i * mb + j] = v;
+      }
+    if (cholesky(a, mb, l)) {
+      ok = true;
+      break;
+    }
+  }
+  if (!ok) return false;
+  gam.assign((size_t)mb * q, 0.0);
+  std::vector<double> rhs((size_t)mb), y((size_t)mb);
+  for (int c = 0; c < q; ++c) {
+    for (int i = 0; i < mb; ++i) rhs[(size_t)i] = s[(size_t)i] * gall[(size_t)i * w + mb + c];
+    chol_solve(l, mb, rhs.data(), y.data());
+    for (int i = 0; i < mb; ++i) {
+      const double g = s[(size_t)i] * y[(size_t)i];
+      if (!std::isfinite(g)) return false;
+      gam[(size_t)i * q + c] = g;
+    }
+  }
+  return true;
+}
+
+// With rc.v[0..mb) and rc.av[0..mb) filled and b (q columns) at rc.av[mb..mb+q):
+// x0 = V g into rc.x0 and Sigma x0 into rc.ax0; ok = false when the projected system
+// cannot be factorised (no start).
+Status galerkin_start(Fit& f, Recycle& rc, int mb, int q, bool& ok) {
+  const int64_t ld = f.ld;
+  SG_CUDA(gram(rc.v, mb, rc.av, mb + q, f.n, ld, rc.gpart, rc.gout, f.st));
+  std::vector<double> gall((size_t)mb * (mb + q)), gam;
+  SG_CUDA(cudaMemcpyAsync(gall.data(), rc.gout, gall.size() * 8, cudaMemcpyDeviceToHost, f.st));
+  SG_CUDA(cudaStreamSynchronize(f.st));
+  ok = galerkin_coeffs(gall, mb, q, gam);
+  if (!ok) {
+    ++rc.fallbacks;
+    return Status();
+  }
+  SG_CUDA(cudaMemcpyAsync(rc.gam, gam.data(), gam.size() * 8, cudaMemcpyHostToDevice, f.st));
+  SG_CUDA(combo(rc.v, mb, rc.gam, q, rc.x0, false, f.n, ld, f.st));
+  SG_CUDA(combo(rc.av, mb, rc.gam, q, rc.ax0, false, f.n, ld, f.st));
+  return Status();
+}
+
+// k basis columns x with K-images kx, and their images under the current Sigma,
+// at column `at` of rc.v / rc.av.
+Status basis_cols(Fit& f, Recycle& rc, int at, const double* x, const double* kx, int k,
+                  const double tau[2]) {
+  const int64_t ld = f.ld;
+  SG_TRY(copy_cols(f, x, rc.v + (size_t)at * ld, k));
+  SG_CUDA(sigma_image(x, kx, f.wmax, tau[0], tau[1], rc.av + (size_t)at * ld, f.n, ld, k, f.st));
+  return Status();
+}
+
+// The block solve of one iteration from the recycled start: basis [X | U] and the
+// previous iteration's block solutions (f.sol on entry).  Leaves the final residual
+// in rc.br.
+Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const double tau[2]) {
+  const int64_t ld = f.ld;
+  int mb = 0;
+  SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
+  mb += f.p + f.nrv;
+  if (rc.have_ksol) {
+    SG_TRY(basis_cols(f, rc, mb, f.sol, rc.kout + ld, f.q, tau));
+    mb += f.q;
+  }
+  SG_TRY(copy_cols(f, f.rhs, rc.av + (size_t)mb * ld, f.q));
+  bool ok = false;
+  SG_TRY(galerkin_start(f, rc, mb, f.q, ok));
+  if (ok) return solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br);
+  return solve(f, f.rhs, f.sol, x0_prev, f.q, tau, nullptr, rc.br);
+}
+
+// K Py, and in the same launch K X*_t (this iteration's block solutions, for the next
+// block start) and K of the previous AI solutions pk', pw' (for this iteration's AI
+// starts).  Writes f.kpy.
+Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw) {
+  const int64_t ld = f.ld;
+  SG_TRY(copy_cols(f, f.py, rc.kin, 1));
+  SG_TRY(copy_cols(f, f.sol, rc.kin + ld, f.q));
+  int k = 1 + f.q;
+  const int at_pk = k;
+  if (with_pk) SG_TRY(copy_cols(f, f.pk_raw, rc.kin + (size_t)k++ * ld, 1));
+  const int at_pw = k;
+  if (with_pw) SG_TRY(copy_cols(f, f.pw_raw, rc.kin + (size_t)k++ * ld, 1));
+  SG_TRY(grm_product(f.h, rc.kin, rc.kout, k, nullptr, f.cfg->precision, f.st));
+  SG_TRY(copy_cols(f, rc.kout, f.kpy, 1));
+  rc.have_ksol = true;
+  rc.have_kpk = with_pk;
+  rc.have_kpw = with_pw;
+  rc.at_pk = at_pk;
+  rc.at_pw = at_pw;
+  return Status();
+}
+
+// One AI solve Sigma x = b (one column) from a recycled start over this iteration's
+// block solutions (image b_block - r_block), [X | U] and the previous solution of the
+// same system (x on entry, K-image at kprev when have).
+Status ai_solve_recycled(Fit& f, Recycle& rc, const double* b, double* x, const double* kprev,
+                         bool have, const double tau[2]) {
+  const int64_t ld = f.ld;
+  int mb = 0;
+  SG_TRY(copy_cols(f, f.sol, rc.v, f.q));
+  SG_CUDA(sub_cols(f.rhs, rc.br, rc.av, f.n, ld, f.q, f.st));
+  mb += f.q;
+  SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
+  mb += f.p + f.nrv;
+  if (have) {
+    SG_TRY(basis_cols(f, rc, mb, x, kprev, 1, tau));
+    mb += 1;
+  }
+  SG_TRY(copy_cols(f, b, rc.av + (size_t)mb * ld, 1));
+  bool ok = false;
+  SG_TRY(galerkin_start(f, rc, mb, 1, ok));
+  if (ok) return solve(f, b, x, rc.x0, 1, tau, rc.ax0, nullptr);
+  if (have) SG_TRY(copy_cols(f, x, rc.x0, 1));
+  return solve(f, b, x, have ? rc.x0 : nullptr, 1, tau);
+}
+
 }  // namespace
 
 }  // namespace saige
@@ -154,6 +336,8 @@ SG_API void saige_ai_reml_config_default(saige_ai_reml_config* c) {
 // fit print the wall time of each phase (device synchronised at each mark) to stderr.
 struct PhaseTimer {
   bool on = false;
+  const int64_t* launches = nullptr;  // GRM product launches, reported per phase when set
+  int64_t l0 = 0;
   std::chrono::steady_clock::time_point t0;
   PhaseTimer() {
     const char* e = getenv("SAIGE_TIMING");
@@ -164,8 +348,10 @@ struct PhaseTimer {
     if (!on) return;
     cudaDeviceSynchronize();
     const auto t1 = std::chrono::steady_clock::now();
-    fprintf(stderr, "[saige timing] %-10s %8.2f ms\n", what,
-            std::chrono::duration<double, std::milli>(t1 - t0).count());
+    const int64_t l = launches ? *launches : 0;
+    fprintf(stderr, "[saige timing] %-10s %8.2f ms  %lld GRM launches\n", what,
+            std::chrono::duration<double, std::milli>(t1 - t0).count(), (long long)(l - l0));
+    l0 = l;
     t0 = t1;
   }
 };
@@ -175,6 +361,8 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
                        double* alpha_out, double* mu_out, double* eta_out, double* w_out,
                        double* tau_trace) {
   PhaseTimer tm;
+  tm.launches = &h->n_kv_launches;
+  tm.l0 = h->n_kv_launches;
   Fit f;
   f.h = h;
   f.st = h->stream;
@@ -189,7 +377,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   const size_t q = (size_t)f.q, nrv = (size_t)f.nrv, pp = (size_t)p;
   const size_t cols[] = {1, pp, 1, 1, 1, 1, 1, 1,  // y, x, eta, mu, w, wmax, d, ytil
                          q, q,                     // rhs, sol
-                         nrv, nrv, nrv,            // ku, pu, tmpq
+                         pp + nrv, nrv, nrv,       // kxu, pu, tmpq
                          1, 1, 1, 1, 1, 1, 1};     // py, kpy, pk, invw_py, pw, pk_raw, pw_raw
   size_t nvec = 0;
   for (size_t c : cols) nvec += c;
@@ -210,7 +398,8 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   f.y = take(1); f.x = take(pp); f.eta = take(1); f.mu = take(1); f.w = take(1);
   f.wmax = take(1); f.d = take(1); f.ytil = take(1);
   f.rhs = take(q); f.sol = take(q);
-  f.ku = take(nrv); f.pu = take(nrv); f.tmpq = take(nrv);
+  f.kxu = take(pp + nrv); f.pu = take(nrv); f.tmpq = take(nrv);
+  f.ku = f.kxu + pp * ld;
   f.py = take(1); f.kpy = take(1); f.pk = take(1); f.invw_py = take(1); f.pw = take(1);
   f.pk_raw = take(1); f.pw_raw = take(1);
   if (base != vec_end || ci != sizeof(cols) / sizeof(cols[0])) std::abort();
@@ -264,9 +453,16 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   SG_CUDA(cudaMemcpy2DAsync(f.rhs + ld, (size_t)ld * 8, f.x, (size_t)ld * 8, (size_t)ld * 8,
                             (size_t)p, cudaMemcpyDeviceToDevice, f.st));
   // K u is the same every iteration (K and the probes are fixed): one block product.
+  // Recycled starts also use K X, from the same launch (X and U are adjacent in rhs).
   tm.mark("  irls");
-  SG_TRY(grm_product(h, U, f.ku, f.nrv, nullptr, cfg->precision, f.st));
+  const bool recyc = cfg->warm_start == SAIGE_WARM_RECYCLED || cfg->warm_start == SAIGE_WARM_LEARNED;
+  if (recyc)
+    SG_TRY(grm_product(h, f.rhs + ld, f.kxu, p + f.nrv, nullptr, cfg->precision, f.st));
+  else
+    SG_TRY(grm_product(h, U, f.ku, f.nrv, nullptr, cfg->precision, f.st));
   tm.mark("  Ku");
+  Recycle rc;
+  if (recyc) SG_TRY(recycle_init(f, rc));
 
   const bool fix_tau_e = trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL;
   double tau[2] = {1.0, 0.0};
@@ -286,7 +482,9 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     if (warm && f.have_prev)
       SG_CUDA(cudaMemcpyAsync(prev.ptr, f.sol, (size_t)ld * f.q * 8, cudaMemcpyDeviceToDevice, f.st));
     const double* x0 = (warm && f.have_prev) ? prev.as<double>() : nullptr;
-    if (cfg->solve == SAIGE_SOLVE_BLOCK) {
+    if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
+      SG_TRY(block_solve_recycled(f, rc, x0, tau));
+    } else if (cfg->solve == SAIGE_SOLVE_BLOCK) {
       SG_TRY(solve(f, f.rhs, f.sol, x0, f.q, tau));
     } else {
       // one solve per right-hand side, in the reference's order
@@ -295,6 +493,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
                      x0 ? x0 + (size_t)c * ld : nullptr, 1, tau));
     }
     f.have_prev = true;
+    tm.mark("  block");
 
     // X' Sigma^-1 X and X' Sigma^-1 y (ai_reml.rs:189-205)
     std::vector<double> dxs, dxy;
@@ -315,7 +514,11 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     // P y = Sinv y - SinvX alpha; YPAPY = Py' K Py (ai_reml.rs:221-232)
     SG_TRY(copy_cols(f, SinvY, f.py, 1));
     SG_CUDA(sub_combo(f.py, 1, SinvX, p, f.dsmall, n, ld, f.st));
-    SG_TRY(grm_product(h, f.py, f.kpy, 1, nullptr, cfg->precision, f.st));
+    if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK)
+      SG_TRY(kpy_recycled(f, rc, f.have_prev_pk, !fix_tau_e && f.have_prev_pw));
+    else
+      SG_TRY(grm_product(h, f.py, f.kpy, 1, nullptr, cfg->precision, f.st));
+    tm.mark("  kpy");
     std::vector<double> r1;
     SG_TRY(coldots(f, f.py, f.kpy, 1, r1));
     const double ypapy = r1[0];
@@ -332,9 +535,15 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
 
     // AI = (K P y)' P (K P y) (ai_reml.rs:263-273)
     // warm start from the previous iteration's unprojected solution
-    if (warm && f.have_prev_pk) SG_TRY(copy_cols(f, f.pk_raw, f.pw, 1));
-    SG_TRY(solve(f, f.kpy, f.pk_raw, (warm && f.have_prev_pk) ? f.pw : nullptr, 1, tau));
+    if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
+      SG_TRY(ai_solve_recycled(f, rc, f.kpy, f.pk_raw, rc.kout + (size_t)rc.at_pk * ld,
+                               rc.have_kpk, tau));
+    } else {
+      if (warm && f.have_prev_pk) SG_TRY(copy_cols(f, f.pk_raw, f.pw, 1));
+      SG_TRY(solve(f, f.kpy, f.pk_raw, (warm && f.have_prev_pk) ? f.pw : nullptr, 1, tau));
+    }
     f.have_prev_pk = true;
+    tm.mark("  ai solve");
     SG_TRY(copy_cols(f, f.pk_raw, f.pk, 1));
     SG_TRY(p_project(f, f.pk, f.kpy, 1, l));
     SG_TRY(coldots(f, f.kpy, f.pk, 1, r1));
@@ -352,8 +561,13 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
       SG_CUDA(div_w(f.py, f.w, f.invw_py, n, f.st));
       SG_TRY(coldots(f, f.py, f.invw_py, 1, r1));
       score_e = r1[0] - trace_w;
-      if (warm && f.have_prev_pw) SG_TRY(copy_cols(f, f.pw_raw, f.tmpq, 1));
-      SG_TRY(solve(f, f.invw_py, f.pw_raw, (warm && f.have_prev_pw) ? f.tmpq : nullptr, 1, tau));
+      if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
+        SG_TRY(ai_solve_recycled(f, rc, f.invw_py, f.pw_raw, rc.kout + (size_t)rc.at_pw * ld,
+                                 rc.have_kpw, tau));
+      } else {
+        if (warm && f.have_prev_pw) SG_TRY(copy_cols(f, f.pw_raw, f.tmpq, 1));
+        SG_TRY(solve(f, f.invw_py, f.pw_raw, (warm && f.have_prev_pw) ? f.tmpq : nullptr, 1, tau));
+      }
       f.have_prev_pw = true;
       SG_TRY(copy_cols(f, f.pw_raw, f.pw, 1));
       SG_TRY(p_project(f, f.pw, f.invw_py, 1, l));

@@ -401,11 +401,15 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
   PcgScratch s;
   SG_TRY(pcg_scratch(h, q, s));
   std::vector<int32_t> state((size_t)q, kColActive);
-  const double* ax0 = nullptr;
-  if (run.x0) {
+  // With tau1 = 0 the operator is tau0 W^-1 (or tau0 W): tau1 K v contributes only
+  // zeros, so no GRM product is formed and K v reads as 0.
+  const bool no_k = run.tau1 == 0.0;
+  if (no_k) SG_CUDA(cudaMemsetAsync(s.kp, 0, (size_t)ld * q * sizeof(double), st));
+  const double* ax0 = run.x0 ? run.ax0 : nullptr;
+  if (run.x0 && !run.ax0) {
     // r = b - A x0 (decomposition.rs:225-227)
     SG_CUDA(cudaMemsetAsync(s.cols.state, 0, (size_t)q * sizeof(int32_t), st));
-    SG_TRY(grm_product(h, run.x0, s.kp, q, nullptr, run.precision, st));
+    if (!no_k) SG_TRY(grm_product(h, run.x0, s.kp, q, nullptr, run.precision, st));
     if (run.w_inverse)
       SG_CUDA(pcg_apply(run.x0, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
                         s.partial, st));
@@ -428,7 +432,7 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
       bool any = false;
       for (int c = 0; c < q; ++c) any |= state[(size_t)c] == kColActive;
       if (!any) break;
-      SG_TRY(grm_product(h, s.p, s.kp, q, state.data(), run.precision, st));
+      if (!no_k) SG_TRY(grm_product(h, s.p, s.kp, q, state.data(), run.precision, st));
       if (run.w_inverse)
         SG_CUDA(pcg_apply(s.p, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
                           s.partial, st));
@@ -439,6 +443,9 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
                        s.partial, s.small, st));
     }
   }
+  if (run.r_out)
+    SG_CUDA(cudaMemcpyAsync(run.r_out, s.r, (size_t)ld * q * sizeof(double),
+                            cudaMemcpyDeviceToDevice, st));
   std::vector<double> rr((size_t)q);
   run.iters.assign((size_t)q, 0);
   run.state = state;

@@ -90,6 +90,7 @@ struct PcgRun {
   // inputs (device, ld = n_pad)
   const double* b = nullptr;
   const double* x0 = nullptr;
+  const double* ax0 = nullptr; // Sigma x0 when the caller knows it (no product for r0)
   const double* wv = nullptr;  // wmax (fit-null form) or w (score-test form)
   const double* d = nullptr;   // Jacobi diagonal
   double tau0 = 1.0, tau1 = 0.0;
@@ -101,6 +102,7 @@ struct PcgRun {
   bool force_step = false;     // warm starts: at least one CG step per column
   // outputs
   double* x = nullptr;         // device n_pad x q
+  double* r_out = nullptr;     // optional: the final residual b - Sigma x (device n_pad x q)
   std::vector<int32_t> iters, state;
   std::vector<double> resid;
   int64_t total_iters = 0;

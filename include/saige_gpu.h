@@ -322,7 +322,12 @@ int32_t saige_solve_mixed_model_pcg(saige_grm* h, const double tau[2], const dou
 
 #define SAIGE_WARM_ZERO 0     /* x0 = 0 (the reference)                        */
 #define SAIGE_WARM_PREVIOUS 1 /* previous AI-REML iteration's solution         */
-#define SAIGE_WARM_LEARNED 2  /* MLP-predicted start, previous as fallback      */
+#define SAIGE_WARM_LEARNED 2  /* recycled start plus a learned correction (MLP
+                                 trained on the fit's own solves), used when it
+                                 validates; the recycled start otherwise        */
+#define SAIGE_WARM_RECYCLED 3 /* Galerkin start over vectors whose Sigma-image
+                                 needs no GRM product: X, the probes, the
+                                 previous solutions (block solve only)          */
 
 typedef struct {
   int32_t max_iter;         /* AiRemlConfig::max_iter (ai_reml.rs:22-51), 30     */
