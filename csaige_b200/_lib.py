@@ -50,7 +50,7 @@ class AiRemlConfigC(C.Structure):
         ("precision", C.c_int32),
         ("solve", C.c_int32),
         ("warm_start", C.c_int32),
-        ("reserved", C.c_int32),
+        ("precond", C.c_int32),
     ]
 
 
@@ -64,6 +64,10 @@ class AiRemlSummaryC(C.Structure):
         ("n_kv_launches", C.c_int64),
         ("pcg_iters", C.c_int64),
         ("seconds", C.c_double),
+        ("learned_trainings", C.c_int32),
+        ("learned_uses", C.c_int32),
+        ("learned_r2", C.c_double),
+        ("learned_seconds", C.c_double),
     ]
 
 
@@ -224,6 +228,13 @@ SIGNATURES = {
     "saige_release_cached_memory": (C.c_int32, []),
     "saige_write_null_model": (C.c_int32, [C.c_char_p, P(NullModelC)]),
     "saige_xvx_inv_xv": (C.c_int32, [_d, _d, C.c_int64, C.c_int32, _d]),
+    "saige_mlp_param_count": (C.c_int32, []),
+    "saige_mlp_initial_params": (C.c_int32, [C.c_uint64, P(C.c_float)]),
+    "saige_mlp_eval": (C.c_int32, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64,
+                                   P(C.c_float), P(C.c_float), _d, C.c_int32]),
+    "saige_mlp_train": (C.c_int32, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64,
+                                    C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_int32, _d, _d,
+                                    _d, C.c_int32]),
     "saige_explicit_grm_config_default": (C.c_int32, [P(ExplicitGrmConfigC)]),
     "saige_dense_grm_from_bed": (
         C.c_int32,

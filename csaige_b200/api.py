@@ -35,6 +35,8 @@ WARM_ZERO = _lib.WARM_ZERO
 WARM_PREVIOUS = _lib.WARM_PREVIOUS
 WARM_LEARNED = _lib.WARM_LEARNED
 WARM_RECYCLED = _lib.WARM_RECYCLED
+PRECOND_UNIT = 0    # 1 / (tau0 / w + tau1): diag K taken as 1 (ai_reml.rs:142-164)
+PRECOND_DIAG_K = 1  # 1 / (tau0 / w + tau1 K_ii) with the exact diagonal
 
 
 class TraitType(enum.IntEnum):
@@ -319,6 +321,7 @@ class AiRemlConfig:
     precision: int = PREC_FP32
     solve: int = SOLVE_SINGLE
     warm_start: int = WARM_ZERO
+    precond: int = PRECOND_UNIT
 
 
 @dataclass
@@ -337,6 +340,10 @@ class AiRemlResult:
     pcg_iters: int = 0
     seconds: float = 0.0
     tau_trace: np.ndarray = field(default_factory=lambda: np.zeros((0, 2)))
+    learned_trainings: int = 0
+    learned_uses: int = 0
+    learned_r2: float = 0.0
+    learned_seconds: float = 0.0
 
 
 def _design(x, n: int) -> tuple[np.ndarray, int]:
@@ -358,7 +365,7 @@ def fit_ai_reml(y, x, grm: OnTheFlyGrm, trait_type: TraitType,
     xc, p = _design(x, n)
     cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
                              config.n_random_vectors, config.seed, config.precision, config.solve,
-                             config.warm_start, 0)
+                             config.warm_start, config.precond)
     out = _lib.AiRemlSummaryC()
     alpha = np.zeros(p)
     mu = np.zeros(n)
@@ -374,7 +381,9 @@ def fit_ai_reml(y, x, grm: OnTheFlyGrm, trait_type: TraitType,
         mu=mu, working_weights=w, residuals=yy - mu, eta=eta, alpha=alpha,
         log_likelihood=out.log_likelihood, n_kv=out.n_kv, n_kv_launches=out.n_kv_launches,
         pcg_iters=out.pcg_iters, seconds=out.seconds,
-        tau_trace=trace[: 2 * it].reshape(-1, 2))
+        tau_trace=trace[: 2 * it].reshape(-1, 2), learned_trainings=out.learned_trainings,
+        learned_uses=out.learned_uses, learned_r2=out.learned_r2,
+        learned_seconds=out.learned_seconds)
 
 
 @dataclass
@@ -411,7 +420,7 @@ def run_loco(y, x, grm: OnTheFlyGrm, marker_chroms: Sequence[str], trait_type: T
     xc, p = _design(x, n)
     cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
                              config.n_random_vectors, config.seed, config.precision, config.solve,
-                             config.warm_start, 0)
+                             config.warm_start, config.precond)
     k = len(chroms)
     outs = (_lib.AiRemlSummaryC * k)()
     alpha = np.zeros((k, p))
@@ -787,7 +796,7 @@ def fit_null_from_bed(bed, n_fam: int, m_tot: int, y, x, trait_type: TraitType,
     sidx = None if sample_idx is None else np.ascontiguousarray(sample_idx, dtype=np.int64)
     cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
                              config.n_random_vectors, config.seed, config.precision, config.solve,
-                             config.warm_start, 0)
+                             config.warm_start, config.precond)
     out = _lib.AiRemlSummaryC()
     alpha = np.zeros(p)
     mu = np.zeros(n)

@@ -33,6 +33,7 @@ SOURCES = [
     "model.cu",
     "grm_explicit.cu",
     "warm.cu",
+    "mlp.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

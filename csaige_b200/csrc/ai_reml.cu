@@ -12,6 +12,7 @@
 #include "engine.cuh"
 #include "rng.hpp"
 #include "vr.cuh"
+#include "mlp.cuh"
 #include "warm.cuh"
 
 namespace saige {
@@ -151,12 +152,45 @@ struct Recycle {
   bool have_kpk = false, have_kpw = false;  // K of the previous AI solutions is in kout
   int at_pk = 0, at_pw = 0;                  // their columns in kout
   int64_t fallbacks = 0;
+  // learned correction (SAIGE_WARM_LEARNED): an MLP trained on the change of the
+  // block solutions between iterations predicts the next change; the prediction joins
+  // the next block basis, its K-image from the K Py launch
+  bool learned = false;
+  Mlp mlp;
+  DevBuf lmem;
+  float *F0 = nullptr, *F1 = nullptr, *T = nullptr, *yhat = nullptr;
+  double *xprev = nullptr, *delta = nullptr, *bnext = nullptr, *wnext = nullptr, *scales = nullptr;
+  const double* diagk = nullptr;
+  bool have_F = false, have_delta = false;
+  int at_delta = 0, trainings = 0, uses = 0;
+  double r2 = 0.0, seconds = 0.0;
 };
 
-Status recycle_init(Fit& f, Recycle& rc) {
+// Held-out R^2 at or above which the prediction joins the basis.
+constexpr double kLearnR2Min = 0.25;
+
+Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint64_t seed) {
   const size_t ld = (size_t)f.ld, q = (size_t)f.q;
-  rc.mb_max = 2 * f.q + 1;
-  rc.nk = f.q + 3;
+  rc.learned = learned;
+  rc.diagk = diagk;
+  rc.mb_max = learned ? 3 * f.q + 1 : 2 * f.q + 1;
+  rc.nk = learned ? 2 * f.q + 3 : f.q + 3;
+  if (learned) {
+    const size_t nq = (size_t)f.n * q;
+    SG_TRY(rc.lmem.reserve(nq * (2 * kMlpIn + 2) * 4 + (3 * q + 1) * ld * 8 + (2 * q + 8) * 8 + 64));
+    char* c = rc.lmem.as<char>();
+    rc.xprev = reinterpret_cast<double*>(c);
+    rc.delta = rc.xprev + q * ld;
+    rc.bnext = rc.delta + q * ld;
+    rc.wnext = rc.bnext + q * ld;
+    rc.scales = rc.wnext + ld;
+    rc.F0 = reinterpret_cast<float*>(rc.scales + 2 * q + 8);
+    rc.F1 = rc.F0 + nq * kMlpIn;
+    rc.T = rc.F1 + nq * kMlpIn;
+    rc.yhat = rc.T + nq;
+    SG_CUDA(cudaMemsetAsync(rc.xprev, 0, (3 * q + 1) * ld * 8, f.st));
+    SG_TRY(mlp_init(rc.mlp, seed, f.st));
+  }
   const size_t mb = (size_t)rc.mb_max, nk = (size_t)rc.nk;
   const size_t ncol = mb + (mb + q) + 3 * q + 2 * nk;
   const size_t nsmall = mb * q + gram_partial_doubles(f.n, (int)mb, (int)(mb + q)) + mb * (mb + q);
@@ -257,6 +291,12 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
     SG_TRY(basis_cols(f, rc, mb, f.sol, rc.kout + ld, f.q, tau));
     mb += f.q;
   }
+  if (rc.have_delta) {
+    // the learned prediction of this iteration's change of the solutions
+    SG_TRY(basis_cols(f, rc, mb, rc.delta, rc.kout + (size_t)rc.at_delta * ld, f.q, tau));
+    mb += f.q;
+    ++rc.uses;
+  }
   SG_TRY(copy_cols(f, f.rhs, rc.av + (size_t)mb * ld, f.q));
   bool ok = false;
   SG_TRY(galerkin_start(f, rc, mb, f.q, ok));
@@ -267,7 +307,10 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
 // K Py, and in the same launch K X*_t (this iteration's block solutions, for the next
 // block start) and K of the previous AI solutions pk', pw' (for this iteration's AI
 // starts).  Writes f.kpy.
-Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw) {
+Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k);
+
+Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw, int trait,
+                    const double tau[2]) {
   const int64_t ld = f.ld;
   SG_TRY(copy_cols(f, f.py, rc.kin, 1));
   SG_TRY(copy_cols(f, f.sol, rc.kin + ld, f.q));
@@ -276,6 +319,7 @@ Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw) {
   if (with_pk) SG_TRY(copy_cols(f, f.pk_raw, rc.kin + (size_t)k++ * ld, 1));
   const int at_pw = k;
   if (with_pw) SG_TRY(copy_cols(f, f.pw_raw, rc.kin + (size_t)k++ * ld, 1));
+  if (rc.learned) SG_TRY(learn_step(f, rc, trait, tau, k));
   SG_TRY(grm_product(f.h, rc.kin, rc.kout, k, nullptr, f.cfg->precision, f.st));
   SG_TRY(copy_cols(f, rc.kout, f.kpy, 1));
   rc.have_ksol = true;
@@ -283,6 +327,67 @@ Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw) {
   rc.have_kpw = with_pw;
   rc.at_pk = at_pk;
   rc.at_pw = at_pw;
+  return Status();
+}
+
+// Learned correction, at the K Py point of an iteration (block solutions X*_t in
+// f.sol, the weights of the next iteration computable from the updated mu):
+//  1. with the features of the previous iteration, fit the MLP to the change
+//     X*_t - X*_{t-1} (per-column RMS scaled) and measure its held-out R^2;
+//  2. form this iteration's features;
+//  3. when the R^2 is at least kLearnR2Min, predict the next change and append it to
+//     the K launch (column k on), so that the next block start may use it.
+Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k) {
+  const auto t0 = std::chrono::steady_clock::now();
+  const int64_t ld = f.ld, n = f.n;
+  const int q = f.q;
+  std::vector<double> sc((size_t)(2 * q + 2)), dd;
+  if (rc.have_F) {
+    SG_CUDA(sub_cols(f.sol, rc.xprev, rc.x0, n, ld, q, f.st));
+    SG_TRY(coldots(f, rc.x0, rc.x0, q, dd));
+    for (int c = 0; c < q; ++c) sc[(size_t)c] = sqrt(dd[(size_t)c] / (double)n);
+    SG_CUDA(cudaMemcpyAsync(rc.scales, sc.data(), (size_t)q * 8, cudaMemcpyHostToDevice, f.st));
+    SG_CUDA(learn_targets(f.sol, rc.xprev, rc.scales, n, ld, q, rc.T, f.st));
+    SG_TRY(mlp_train(rc.mlp, rc.F0, rc.T, n, q, rc.trainings == 0 ? 200 : 100, 32768, 3e-3f, 8,
+                     f.st));
+    double mse = 0.0, tms = 0.0;
+    SG_TRY(mlp_validate(rc.mlp, rc.F0, rc.T, n, q, 8, &mse, &tms, f.st));
+    rc.r2 = tms > 0.0 ? 1.0 - mse / tms : 0.0;
+    ++rc.trainings;
+  }
+  // features of this iteration: x = X*_t, b = [ytil | X | U], bnext = next [ytil | X | U]
+  SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, rc.wnext, rc.bnext, n, f.st));
+  SG_TRY(copy_cols(f, f.rhs + ld, rc.bnext + ld, q - 1));
+  std::vector<double> a, b, u, w;
+  SG_TRY(coldots(f, f.sol, f.sol, q, a));
+  SG_TRY(coldots(f, f.rhs, f.rhs, q, b));
+  SG_TRY(coldots(f, f.ku, f.ku, 2, u));
+  SG_TRY(coldots(f, f.w, f.w, 1, w));
+  for (int c = 0; c < q; ++c) {
+    sc[(size_t)c] = sqrt(a[(size_t)c] / (double)n);
+    sc[(size_t)(q + c)] = sqrt(b[(size_t)c] / (double)n);
+  }
+  sc[(size_t)(2 * q)] = sqrt(u[0] / (double)n);
+  sc[(size_t)(2 * q + 1)] = sqrt(u[1] / (double)n);
+  const double wr = sqrt(w[0] / (double)n);
+  const double dmean = 1.0 / (tau[0] / (wr > 1e-30 ? wr : 1e-30) + tau[1]);
+  SG_CUDA(cudaMemcpyAsync(rc.scales, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice, f.st));
+  SG_CUDA(learn_features(f.sol, f.rhs, rc.bnext, f.w, rc.wnext, rc.diagk, f.ku, f.ku + ld,
+                         rc.scales, tau[0], tau[1], dmean, n, ld, q, rc.F1, f.st));
+  rc.have_delta = false;
+  if (rc.trainings > 0 && rc.r2 >= kLearnR2Min) {
+    SG_TRY(mlp_forward(rc.mlp, rc.F1, n * q, rc.yhat, f.st));
+    SG_CUDA(learn_to_cols(rc.yhat, n, ld, q, rc.delta, f.st));
+    SG_TRY(copy_cols(f, rc.delta, rc.kin + (size_t)k * ld, q));
+    rc.at_delta = k;
+    k += q;
+    rc.have_delta = true;
+  }
+  SG_TRY(copy_cols(f, f.sol, rc.xprev, q));
+  std::swap(rc.F0, rc.F1);
+  rc.have_F = true;
+  SG_CUDA(cudaStreamSynchronize(f.st));
+  rc.seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   return Status();
 }
 
@@ -329,7 +434,7 @@ SG_API void saige_ai_reml_config_default(saige_ai_reml_config* c) {
   c->precision = SAIGE_PREC_FP32;
   c->solve = SAIGE_SOLVE_SINGLE;
   c->warm_start = SAIGE_WARM_ZERO;
-  c->reserved = 0;
+  c->precond = SAIGE_PRECOND_UNIT;
 }
 
 // With SAIGE_TIMING=1 in the environment, saige_fit_null_from_bed and the AI-REML
@@ -360,6 +465,10 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
                        int32_t trait, const saige_ai_reml_config* cfg, saige_ai_reml_summary* out,
                        double* alpha_out, double* mu_out, double* eta_out, double* w_out,
                        double* tau_trace) {
+  if (cfg->warm_start < SAIGE_WARM_ZERO || cfg->warm_start > SAIGE_WARM_RECYCLED)
+    return fail(SAIGE_EINVAL, "unknown warm_start %d", cfg->warm_start);
+  if (cfg->precond != SAIGE_PRECOND_UNIT && cfg->precond != SAIGE_PRECOND_DIAG_K)
+    return fail(SAIGE_EINVAL, "unknown precond %d", cfg->precond);
   PhaseTimer tm;
   tm.launches = &h->n_kv_launches;
   tm.l0 = h->n_kv_launches;
@@ -461,8 +570,17 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   else
     SG_TRY(grm_product(h, U, f.ku, f.nrv, nullptr, cfg->precision, f.st));
   tm.mark("  Ku");
+  // exact diag K: the DIAG_K preconditioner and a feature of the learned start (K8)
+  const bool learned = cfg->warm_start == SAIGE_WARM_LEARNED && cfg->solve == SAIGE_SOLVE_BLOCK;
+  DevBuf diagk;
+  if (cfg->precond == SAIGE_PRECOND_DIAG_K || learned) {
+    SG_TRY(diagk.reserve((size_t)ld * 8));
+    SG_CUDA(cudaMemsetAsync(diagk.ptr, 0, (size_t)ld * 8, f.st));
+    SG_TRY(grm_diag(h, diagk.as<double>(), f.st));
+  }
+  const double* pre_diag = cfg->precond == SAIGE_PRECOND_DIAG_K ? diagk.as<double>() : nullptr;
   Recycle rc;
-  if (recyc) SG_TRY(recycle_init(f, rc));
+  if (recyc) SG_TRY(recycle_init(f, rc, learned, diagk.as<double>(), cfg->seed));
 
   const bool fix_tau_e = trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL;
   double tau[2] = {1.0, 0.0};
@@ -477,7 +595,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   for (int iter = 0; iter < cfg->max_iter; ++iter) {
     n_iter = iter + 1;
     SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, f.ytil, n, f.st));
-    SG_CUDA(sigma_diag(f.w, tau[0], tau[1], f.wmax, f.d, n, f.st));
+    SG_CUDA(sigma_diag(f.w, tau[0], tau[1], f.wmax, f.d, n, f.st, pre_diag));
     SG_CUDA(cudaMemcpyAsync(f.rhs, f.ytil, (size_t)ld * 8, cudaMemcpyDeviceToDevice, f.st));
     if (warm && f.have_prev)
       SG_CUDA(cudaMemcpyAsync(prev.ptr, f.sol, (size_t)ld * f.q * 8, cudaMemcpyDeviceToDevice, f.st));
@@ -515,7 +633,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     SG_TRY(copy_cols(f, SinvY, f.py, 1));
     SG_CUDA(sub_combo(f.py, 1, SinvX, p, f.dsmall, n, ld, f.st));
     if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK)
-      SG_TRY(kpy_recycled(f, rc, f.have_prev_pk, !fix_tau_e && f.have_prev_pw));
+      SG_TRY(kpy_recycled(f, rc, f.have_prev_pk, !fix_tau_e && f.have_prev_pw, trait, tau));
     else
       SG_TRY(grm_product(h, f.py, f.kpy, 1, nullptr, cfg->precision, f.st));
     tm.mark("  kpy");
@@ -659,6 +777,10 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   out->n_kv_launches = h->n_kv_launches - kl0;
   out->pcg_iters = f.pcg_iters;
   out->seconds = ms * 1e-3;
+  out->learned_trainings = rc.trainings;
+  out->learned_uses = rc.uses;
+  out->learned_r2 = rc.r2;
+  out->learned_seconds = rc.seconds;
   return Status();
 }
 

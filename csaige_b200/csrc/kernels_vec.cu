@@ -241,11 +241,12 @@ __global__ void pcg_p_kernel(double* __restrict__ p, const double* __restrict__ 
 }
 
 __global__ void sigma_diag_kernel(const double* __restrict__ w, double tau0, double tau1,
-                                  double* __restrict__ wmax, double* __restrict__ d, int64_t n) {
+                                  const double* __restrict__ diagk, double* __restrict__ wmax,
+                                  double* __restrict__ d, int64_t n) {
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const double wm = w[i] > 1e-30 ? w[i] : 1e-30;
-  const double dg = tau0 / wm + tau1;
+  const double dg = diagk ? tau0 / wm + tau1 * diagk[i] : tau0 / wm + tau1;
   wmax[i] = wm;
   d[i] = fabs(dg) > 1e-30 ? dg : 1.0;
 }
@@ -459,8 +460,8 @@ cudaError_t pcg_step(double* x, double* r, double* z, double* p, const double* a
 }
 
 cudaError_t sigma_diag(const double* w, double tau0, double tau1, double* wmax, double* d,
-                       int64_t n, cudaStream_t st) {
-  sigma_diag_kernel<<<g1(n), kT, 0, st>>>(w, tau0, tau1, wmax, d, n);
+                       int64_t n, cudaStream_t st, const double* diagk) {
+  sigma_diag_kernel<<<g1(n), kT, 0, st>>>(w, tau0, tau1, diagk, wmax, d, n);
   count_launches(1);
   return cudaGetLastError();
 }

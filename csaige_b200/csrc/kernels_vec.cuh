@@ -53,9 +53,10 @@ cudaError_t pcg_step(double* x, double* r, double* z, double* p, const double* a
                      double* partial, double* scratch2q, cudaStream_t st);
 
 // Elementwise helpers for the AI-REML loop.
-// Jacobi diagonal of fit-null: wmax = max(w,1e-30), d = tau0/wmax + tau1 (1 when |d| <= 1e-30).
+// Jacobi diagonal of fit-null: wmax = max(w,1e-30), d = tau0/wmax + tau1 (1 when |d| <= 1e-30);
+// with diagk, d = tau0/wmax + tau1 diagk[i].
 cudaError_t sigma_diag(const double* w, double tau0, double tau1, double* wmax, double* d,
-                       int64_t n, cudaStream_t st);
+                       int64_t n, cudaStream_t st, const double* diagk = nullptr);
 // Jacobi diagonal of solve_mixed_model_pcg: d = tau0 w + tau1.
 cudaError_t sigma_diag_w(const double* w, double tau0, double tau1, double* d, int64_t n,
                          cudaStream_t st);

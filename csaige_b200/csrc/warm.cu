@@ -105,6 +105,55 @@ __global__ void sub_cols_kernel(const double* __restrict__ a, const double* __re
   out[c * ld + i] = a[c * ld + i] - b[c * ld + i];
 }
 
+// scales: sx[q], sb[q], sk0, sk1
+__global__ void learn_features_kernel(const double* __restrict__ x, const double* __restrict__ b,
+                                      const double* __restrict__ bnext,
+                                      const double* __restrict__ w,
+                                      const double* __restrict__ wnext,
+                                      const double* __restrict__ diagk,
+                                      const double* __restrict__ ku0,
+                                      const double* __restrict__ ku1,
+                                      const double* __restrict__ scales, double tau0, double tau1,
+                                      double dmean, int64_t n, int64_t ld, int q,
+                                      float* __restrict__ F) {
+  const int c = blockIdx.y;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t e = (int64_t)c * n + i, a = (int64_t)c * ld + i;
+  const double sx = scales[c], sb = scales[q + c], sk0 = scales[2 * q], sk1 = scales[2 * q + 1];
+  const double wi = w[i] > 1e-30 ? w[i] : 1e-30, wn = wnext[i] > 1e-30 ? wnext[i] : 1e-30;
+  const double d = 1.0 / (tau0 / wi + tau1);
+  float4 f0, f1;
+  f0.x = (float)(sx > 0.0 ? x[a] / sx : 0.0);
+  f0.y = (float)(sb > 0.0 ? b[a] / sb : 0.0);
+  f0.z = (float)(sb > 0.0 ? (bnext[a] - b[a]) / sb : 0.0);
+  f0.w = (float)log(wn / wi);
+  f1.x = (float)(d / dmean - 1.0);
+  f1.y = (float)(diagk[i] - 1.0);
+  f1.z = (float)(sk0 > 0.0 ? ku0[i] / sk0 : 0.0);
+  f1.w = (float)(sk1 > 0.0 ? ku1[i] / sk1 : 0.0);
+  reinterpret_cast<float4*>(F + e * 8)[0] = f0;
+  reinterpret_cast<float4*>(F + e * 8)[1] = f1;
+}
+
+__global__ void learn_targets_kernel(const double* __restrict__ x1, const double* __restrict__ x0,
+                                     const double* __restrict__ s, int64_t n, int64_t ld,
+                                     float* __restrict__ T) {
+  const int c = blockIdx.y;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int64_t a = (int64_t)c * ld + i;
+  T[(int64_t)c * n + i] = (float)(s[c] > 0.0 ? (x1[a] - x0[a]) / s[c] : 0.0);
+}
+
+__global__ void learn_to_cols_kernel(const float* __restrict__ y, int64_t n, int64_t ld,
+                                     double* __restrict__ out) {
+  const int c = blockIdx.y;
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  out[(int64_t)c * ld + i] = (double)y[(int64_t)c * n + i];
+}
+
 // Sample i per thread: sum over markers of z^2 (codes 00 -> 2, 10 -> 1, 11 -> 0,
 // 01 missing -> 0), in the device word layout of the packed rows.
 __global__ void grm_diag_kernel(const uint32_t* __restrict__ geno, int64_t wpr,
@@ -170,6 +219,31 @@ cudaError_t sub_cols(const double* a, const double* b, double* out, int64_t n, i
                      cudaStream_t st) {
   if (q <= 0) return cudaSuccess;
   sub_cols_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)q), 256, 0, st>>>(a, b, out, n, ld);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t learn_features(const double* x, const double* b, const double* bnext, const double* w,
+                           const double* wnext, const double* diagk, const double* ku0,
+                           const double* ku1, const double* scales, double tau0, double tau1,
+                           double dmean, int64_t n, int64_t ld, int q, float* F, cudaStream_t st) {
+  learn_features_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)q), 256, 0, st>>>(
+      x, b, bnext, w, wnext, diagk, ku0, ku1, scales, tau0, tau1, dmean, n, ld, q, F);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t learn_targets(const double* x1, const double* x0, const double* s, int64_t n,
+                          int64_t ld, int q, float* T, cudaStream_t st) {
+  learn_targets_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)q), 256, 0, st>>>(x1, x0, s, n,
+                                                                                     ld, T);
+  count_launches(1);
+  return cudaGetLastError();
+}
+
+cudaError_t learn_to_cols(const float* y, int64_t n, int64_t ld, int q, double* out,
+                          cudaStream_t st) {
+  learn_to_cols_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)q), 256, 0, st>>>(y, n, ld, out);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -30,6 +30,22 @@ cudaError_t sigma_image(const double* v, const double* kv, const double* wmax, d
 cudaError_t sub_cols(const double* a, const double* b, double* out, int64_t n, int64_t ld, int q,
                      cudaStream_t st);
 
+// Learned start: features of example e = c * n + i (sample i, column c) for the
+// prediction of the next solution change, 8 floats each:
+//   x[i,c] / sx[c], b[i,c] / sb[c], (bnext[i,c] - b[i,c]) / sb[c], log(wnext[i] / w[i]),
+//   d[i] / dmean - 1, diagk[i] - 1, ku0[i] / sk0, ku1[i] / sk1
+// (x, b, bnext: ld apart; d the Jacobi scale 1 / (tau0 / w + tau1)).
+cudaError_t learn_features(const double* x, const double* b, const double* bnext, const double* w,
+                           const double* wnext, const double* diagk, const double* ku0,
+                           const double* ku1, const double* scales, double tau0, double tau1,
+                           double dmean, int64_t n, int64_t ld, int q, float* F, cudaStream_t st);
+// T[c*n + i] = (x1[i,c] - x0[i,c]) / s[c]
+cudaError_t learn_targets(const double* x1, const double* x0, const double* s, int64_t n,
+                          int64_t ld, int q, float* T, cudaStream_t st);
+// out[:, c] = y[c*n + i] (double columns, ld apart; padding rows left as they are)
+cudaError_t learn_to_cols(const float* y, int64_t n, int64_t ld, int q, double* out,
+                          cudaStream_t st);
+
 // diag K (n values): (1/M') sum over the markers in the product (the LOCO mask
 // honoured) of z_im^2, z from the handle's 2p and 1/s in f64 (K8; the diagonal
 // SAIGE's C++ computes in Get_Diagof_StdGeno).

@@ -322,6 +322,13 @@ int32_t saige_solve_mixed_model_pcg(saige_grm* h, const double tau[2], const dou
 
 #define SAIGE_WARM_ZERO 0     /* x0 = 0 (the reference)                        */
 #define SAIGE_WARM_PREVIOUS 1 /* previous AI-REML iteration's solution         */
+/* Jacobi preconditioner of the fit-null PCG.  UNIT: 1 / (tau0 / w + tau1), the
+ * saige-rs form that takes diag K = 1 (ai_reml.rs:142-164); DIAG_K: 1 / (tau0 / w +
+ * tau1 K_ii) with the exact diagonal, as SAIGE's C++ does (SAIGE_fitGLMM_fast.cpp:
+ * 2037-2080, Get_Diagof_StdGeno :642-680). */
+#define SAIGE_PRECOND_UNIT 0
+#define SAIGE_PRECOND_DIAG_K 1
+
 #define SAIGE_WARM_LEARNED 2  /* recycled start plus a learned correction (MLP
                                  trained on the fit's own solves), used when it
                                  validates; the recycled start otherwise        */
@@ -339,7 +346,7 @@ typedef struct {
   int32_t precision;        /* SAIGE_PREC_*                                      */
   int32_t solve;            /* SAIGE_SOLVE_*                                     */
   int32_t warm_start;       /* SAIGE_WARM_*                                      */
-  int32_t reserved;
+  int32_t precond;          /* SAIGE_PRECOND_*                                   */
 } saige_ai_reml_config;
 
 typedef struct {
@@ -351,6 +358,10 @@ typedef struct {
   int64_t n_kv_launches;   /* GRM product launches (a block counts once)     */
   int64_t pcg_iters;       /* sum over solves of PCG iterations              */
   double seconds;          /* device wall time of the fit                    */
+  int32_t learned_trainings; /* SAIGE_WARM_LEARNED: training rounds of the MLP  */
+  int32_t learned_uses;      /* block solves whose start used its prediction   */
+  double learned_r2;         /* held-out R^2 of the last training round        */
+  double learned_seconds;    /* time spent on features, training, inference    */
 } saige_ai_reml_summary;
 
 /* Fill cfg with AiRemlConfig::default() (ai_reml.rs:39-51) and the
@@ -508,6 +519,31 @@ int32_t saige_sparse_grm_from_triplets(int64_t n, int64_t nnz, const int32_t* ro
  * with ten decimals to mtx_path. */
 int32_t saige_write_sparse_grm(const saige_sparse_grm* g, const char* const* sample_ids,
                                int64_t n_ids, const char* mtx_path, const char* ids_path);
+
+/* ---------------------------------------------------------------------
+ * The MLP of the learned PCG start (SAIGE_WARM_LEARNED; no reference
+ * counterpart).  8 inputs, three tanh layers of 64, a linear output; BF16
+ * weights in the forward pass, FP32 arithmetic and FP32 master weights.
+ * Parameter layout: W1[64][8], b1[64], W2[64][64], b2[64], W3[64][64], b3[64],
+ * w4[64], b4.  These entry points expose the network's own kernels so that
+ * they can be checked against a CPU reference.
+ * ------------------------------------------------------------------- */
+int32_t saige_mlp_param_count(void);
+/* The initial weights the fit uses for a seed (uniform +-1/sqrt(fan_in)). */
+int32_t saige_mlp_initial_params(uint64_t seed, float* params);
+/* n_ex examples of 8 features (row-major): out[e] = MLP(features[e]) (may be NULL);
+ * grad (may be NULL) = gradient of mean_e (out[e] - targets[e])^2 with respect to
+ * params (through the BF16 rounding); sse (may be NULL) = sum_e (out[e] - targets[e])^2. */
+int32_t saige_mlp_eval(const float* params, const float* features, const float* targets,
+                       int64_t n_ex, float* out, float* grad, double* sse, int32_t device);
+/* Trains params in place with the fit's trainer: steps Adam steps (lr) on
+ * mini-batches of batch examples from e = c * n + i (q columns of n samples),
+ * samples i % holdout == 0 held out; held-out mean squared error before and after
+ * and the held-out mean squared target. */
+int32_t saige_mlp_train(float* params, const float* features, const float* targets, int64_t n,
+                        int32_t q, int32_t steps, int32_t batch, float lr, int32_t holdout,
+                        double* val_mse_before, double* val_mse_after, double* val_target_ms,
+                        int32_t device);
 
 /* ---------------------------------------------------------------------
  * Synthetic cohorts (seeded; no counterpart in the reference — test and

@@ -55,3 +55,36 @@ def test_recycled_fit_matches_oracle():
     o = O.fit_ai_reml(c["y"], c["x"], O.QUANTITATIVE, O.K_EXPLICIT, O.grm_explicit(z), max_iter=30,
                       tol=1e-5)
     assert np.allclose(rec.tau, o["tau"], rtol=1e-3, atol=0)
+
+
+def test_learned_start_same_fit_and_reports_its_gain(capsys):
+    # a quantitative trait to a tight AI-REML tolerance: several iterations, so the MLP
+    # is trained on the fit's own solves and its prediction can join the start
+    trait = cs.TraitType.Quantitative
+    c = _cohort(trait, n=4000, m=3000, seed=11)
+    zero = _fit(c, trait, cs.WARM_ZERO, tol=1e-4)
+    rec = _fit(c, trait, cs.WARM_RECYCLED, tol=1e-4)
+    lrn = _fit(c, trait, cs.WARM_LEARNED, tol=1e-4)
+    assert lrn.iterations == zero.iterations >= 4
+    assert np.allclose(lrn.tau, zero.tau, rtol=1e-4, atol=0)
+    assert np.allclose(lrn.alpha, zero.alpha, rtol=1e-4, atol=1e-6)
+    assert lrn.learned_trainings == lrn.iterations - 1
+    assert 0.0 < lrn.learned_r2 <= 1.0
+    with capsys.disabled():
+        print(f"\n[learned start] iterations {lrn.iterations}: launches zero {zero.n_kv_launches}, "
+              f"recycled {rec.n_kv_launches}, learned {lrn.n_kv_launches} "
+              f"(prediction used in {lrn.learned_uses} block solves, held-out R^2 "
+              f"{lrn.learned_r2:.3f}, {lrn.learned_seconds * 1e3:.1f} ms in the MLP); "
+              f"PCG iterations recycled {rec.pcg_iters}, learned {lrn.pcg_iters}")
+
+
+def test_diag_k_preconditioner_same_fit():
+    trait = cs.TraitType.Binary
+    c = _cohort(trait, n=2000, m=1500, seed=13)
+    unit = _fit(c, trait, cs.WARM_PREVIOUS)
+    grm = cs.OnTheFlyGrm.from_bed(c["bed"], c["n"], c["m"], c["g"], c["af"][c["g"]],
+                                  precision=cs.PREC_MIXED)
+    cfg = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
+                          warm_start=cs.WARM_PREVIOUS, precond=cs.PRECOND_DIAG_K)
+    dk = cs.fit_ai_reml(c["y"], c["x"], grm, trait, cfg)
+    assert np.allclose(dk.tau, unit.tau, rtol=1e-4, atol=0)
