@@ -80,6 +80,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--warm", choices=["previous", "recycled", "learned"], default="recycled",
                     help="PCG start of the fast configuration")
+    ap.add_argument("--no-learned", action="store_true",
+                    help="skip the learned-versus-recycled start comparison")
     ap.add_argument("--no-explicit-grm", action="store_true",
                     help="skip the create-sparse-grm workload")
     ap.add_argument("--explicit-grm-only", action="store_true",
@@ -463,6 +465,26 @@ def run_ours(args, world, rank, local):
             # the reference solves each used marker alone: its PCG iterations plus the
             # A*0 product of each solve (decomposition.rs:226)
             "reference_kv_estimate": int(v.pcg_iters + v.n_solved)}
+    # the learned start against the recycled one on the same cohort, to an AI-REML
+    # tolerance tight enough for several iterations (the default 0.02 stops after the
+    # first iteration with tau1 > 0, before the network has a transition to learn from)
+    if not args.no_learned and world == 1:
+        cmp_ = {}
+        for name, wmode in (("recycled", cs.WARM_RECYCLED), ("learned", cs.WARM_LEARNED)):
+            cfg_l = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
+                                    warm_start=wmode, tol=1e-4)
+            r = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg_l)
+            cmp_[name] = {"seconds": r.seconds, "ai_reml_iterations": int(r.iterations),
+                          "n_kv_launches": int(r.n_kv_launches), "pcg_iters": int(r.pcg_iters),
+                          "tau": [float(r.tau[0]), float(r.tau[1])]}
+            if wmode == cs.WARM_LEARNED:
+                cmp_[name].update({"trainings": int(r.learned_trainings),
+                                   "prediction_used": int(r.learned_uses),
+                                   "held_out_r2": float(r.learned_r2),
+                                   "mlp_seconds": float(r.learned_seconds)})
+        cmp_["launches_saved"] = cmp_["recycled"]["n_kv_launches"] - cmp_["learned"]["n_kv_launches"]
+        cmp_["config"] = "same cohort, AiRemlConfig tol 1e-4, MIXED, block PCG"
+        line["learned_vs_recycled"] = cmp_
     # the reference's strategy on the same GPU
     plain_kv = None
     if not args.no_plain and world == 1:

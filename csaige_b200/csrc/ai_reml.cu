@@ -348,7 +348,7 @@ Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k) {
     for (int c = 0; c < q; ++c) sc[(size_t)c] = sqrt(dd[(size_t)c] / (double)n);
     SG_CUDA(cudaMemcpyAsync(rc.scales, sc.data(), (size_t)q * 8, cudaMemcpyHostToDevice, f.st));
     SG_CUDA(learn_targets(f.sol, rc.xprev, rc.scales, n, ld, q, rc.T, f.st));
-    SG_TRY(mlp_train(rc.mlp, rc.F0, rc.T, n, q, rc.trainings == 0 ? 200 : 100, 32768, 3e-3f, 8,
+    SG_TRY(mlp_train(rc.mlp, rc.F0, rc.T, n, q, rc.trainings == 0 ? 100 : 50, 32768, 3e-3f, 8,
                      f.st));
     double mse = 0.0, tms = 0.0;
     SG_TRY(mlp_validate(rc.mlp, rc.F0, rc.T, n, q, 8, &mse, &tms, f.st));
@@ -384,7 +384,9 @@ Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k) {
     rc.have_delta = true;
   }
   SG_TRY(copy_cols(f, f.sol, rc.xprev, q));
-  std::swap(rc.F0, rc.F1);
+  // the training features stay in F0 (the captured training graph reads them there)
+  SG_CUDA(cudaMemcpyAsync(rc.F0, rc.F1, (size_t)n * q * kMlpIn * sizeof(float),
+                          cudaMemcpyDeviceToDevice, f.st));
   rc.have_F = true;
   SG_CUDA(cudaStreamSynchronize(f.st));
   rc.seconds += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

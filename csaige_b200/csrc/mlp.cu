@@ -109,9 +109,11 @@ __device__ __forceinline__ float forward_one(SmemW w, float* a0, float* a1, floa
   return y;
 }
 
+// Logical example j: e = j when holdout == 0; otherwise the held-out examples only,
+// j = c * nh + h with nh = ceil(n / holdout), e = c * n + h * holdout.
 __global__ void __launch_bounds__(kFwdThreads)
     mlp_forward_kernel(const uint16_t* __restrict__ wbf, const float* __restrict__ F, int64_t n_ex,
-                       float* __restrict__ out) {
+                       int64_t n, int holdout, float* __restrict__ out) {
   extern __shared__ __align__(16) float smem[];
   const SmemW w = carve_w(smem);
   float* act = smem + kSmemWFloats;  // a0 [IN][T], a1/a2 ping-pong [H][T]
@@ -121,10 +123,12 @@ __global__ void __launch_bounds__(kFwdThreads)
   load_w(wbf, w);
   __syncthreads();
   const int t = threadIdx.x;
+  const int64_t nh = holdout > 0 ? (n + holdout - 1) / holdout : 0;
   for (int64_t base = (int64_t)blockIdx.x * kFwdThreads; base < n_ex;
        base += (int64_t)gridDim.x * kFwdThreads) {
-    const int64_t e = base + t;
-    if (e < n_ex) {
+    const int64_t j = base + t;
+    if (j < n_ex) {
+      const int64_t e = holdout > 0 ? (j / nh) * n + (j % nh) * holdout : j;
       const float4 f0 = *reinterpret_cast<const float4*>(F + e * IN);
       const float4 f1 = *reinterpret_cast<const float4*>(F + e * IN + 4);
       const float f[8] = {f0.x, f0.y, f0.z, f0.w, f1.x, f1.y, f1.z, f1.w};
@@ -137,7 +141,7 @@ __global__ void __launch_bounds__(kFwdThreads)
       float y = w.b4[0];
 #pragma unroll 8
       for (int k = 0; k < H; ++k) y += w.w4[k] * a1[k * kFwdThreads + t];
-      out[e] = y;
+      out[j] = y;
     }
   }
 }
@@ -356,15 +360,17 @@ __global__ void mlp_to_bf16_kernel(const float* __restrict__ w, uint16_t* __rest
   if (p < kMlpParams) wbf[p] = __bfloat16_as_ushort(__float2bfloat16_rn(w[p]));
 }
 
-// Held-out squared error and squared target (examples with sample index % holdout == 0).
+// Held-out squared error and squared target: y[j] is the output of held-out example j
+// (see mlp_forward_kernel), T the targets of all examples.
 __global__ void mlp_val_kernel(const float* __restrict__ y, const float* __restrict__ Tg,
-                               int64_t n_ex, int64_t n, int holdout, double* __restrict__ part) {
+                               int64_t n_out, int64_t n, int holdout, double* __restrict__ part) {
   __shared__ double sh[2][8];
+  const int64_t nh = (n + holdout - 1) / holdout;
   double se = 0.0, st = 0.0;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n_ex;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    if (((e % n) % holdout) != 0) continue;
-    const double d = (double)y[e] - (double)Tg[e];
+  for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < n_out;
+       j += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t e = (j / nh) * n + (j % nh) * holdout;
+    const double d = (double)y[j] - (double)Tg[e];
     se += d * d;
     st += (double)Tg[e] * (double)Tg[e];
   }
@@ -420,18 +426,15 @@ int64_t batch_stride(int64_t n_ex) {
   return 1;
 }
 
-// Scratch of one training configuration: per-block partials.
-struct GradScratch {
-  DevBuf part, lpart;
-  int blocks = 0;
-};
-Status grad_scratch(GradScratch& g, int blocks) {
-  if (g.blocks >= blocks) return Status();
-  SG_TRY(g.part.reserve((size_t)blocks * kMlpParams * sizeof(float)));
-  SG_TRY(g.lpart.reserve((size_t)blocks * sizeof(double)));
-  g.blocks = blocks;
+Status mlp_partials(Mlp& m, int blocks) {
+  if (m.part_blocks >= blocks) return Status();
+  SG_TRY(m.part.reserve((size_t)blocks * kMlpParams * sizeof(float)));
+  SG_TRY(m.lpart.reserve((size_t)blocks * sizeof(double)));
+  m.part_blocks = blocks;
   return Status();
 }
+
+constexpr int kGraphSteps = 25;
 
 }  // namespace
 
@@ -502,7 +505,7 @@ Status mlp_forward(const Mlp& m, const float* F, int64_t n_ex, float* out, cudaS
   if (n_ex <= 0) return Status();
   SG_CUDA(set_smem_attrs());
   const int64_t blocks = std::min<int64_t>(ceil_div(n_ex, kFwdThreads), 148 * 8);
-  mlp_forward_kernel<<<(unsigned)blocks, kFwdThreads, kFwdSmem, st>>>(m.wbf, F, n_ex, out);
+  mlp_forward_kernel<<<(unsigned)blocks, kFwdThreads, kFwdSmem, st>>>(m.wbf, F, n_ex, n_ex, 0, out);
   count_launches(1);
   SG_CHECK_LAUNCH();
   return Status();
@@ -512,13 +515,14 @@ Status mlp_grad(Mlp& m, const float* F, const float* T, const int64_t* idx, int6
                 cudaStream_t st) {
   SG_CUDA(set_smem_attrs());
   const int blocks = (int)ceil_div(std::max<int64_t>(n_ex, 1), kTrainThreads);
-  GradScratch g;
-  SG_TRY(grad_scratch(g, blocks));
+  DevBuf part, lpart;
+  SG_TRY(part.reserve((size_t)blocks * kMlpParams * sizeof(float)));
+  SG_TRY(lpart.reserve((size_t)blocks * sizeof(double)));
   const float scale = 1.0f / (float)std::max<int64_t>(n_ex, 1);
   mlp_grad_kernel<<<(unsigned)blocks, kTrainThreads, kTrainSmem, st>>>(
       m.wbf, F, T, idx, n_ex, n_ex, nullptr, 0, 0, std::max<int64_t>(n_ex, 1), 0, scale,
-      g.part.as<float>(), g.lpart.as<double>());
-  mlp_sum_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(g.part.as<float>(), g.lpart.as<double>(),
+      part.as<float>(), lpart.as<double>());
+  mlp_sum_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(part.as<float>(), lpart.as<double>(),
                                                           blocks, m.grad, m.loss);
   count_launches(2);
   SG_CHECK_LAUNCH();
@@ -533,46 +537,69 @@ Status mlp_train(Mlp& m, const float* F, const float* T, int64_t n, int q, int s
   const int64_t n_ex = n * q;
   const int blocks = std::min<int>(kTrainBlocksMax, (int)ceil_div(batch, kTrainThreads));
   const int64_t slots = (int64_t)blocks * kTrainThreads;
-  const int64_t stride = batch_stride(n_ex);
-  GradScratch g;
-  SG_TRY(grad_scratch(g, blocks));
-  const float scale = 1.0f / (float)slots;
-  // the step loop as one graph: grad pass, Adam, step counter
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  SG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-  for (int s = 0; s < steps; ++s) {
-    mlp_grad_kernel<<<(unsigned)blocks, kTrainThreads, kTrainSmem, st>>>(
-        m.wbf, F, T, nullptr, n_ex, slots, m.step, slots, stride, n, holdout, scale,
-        g.part.as<float>(), g.lpart.as<double>());
-    mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(g.part.as<float>(), blocks, m.master,
-                                                             m.wbf, m.m1, m.m2, m.step, lr);
-    mlp_step_kernel<<<1, 1, 0, st>>>(m.step);
+  const int per = std::min(steps, kGraphSteps);
+  const bool same = m.graph && m.graph_key[0] == F && m.graph_key[1] == T && m.graph_n == n &&
+                    m.graph_q == q && m.graph_batch == batch && m.graph_holdout == holdout &&
+                    m.graph_lr == lr && m.graph_steps == per;
+  if (!same) {
+    if (m.graph) {
+      cudaGraphExecDestroy(m.graph);
+      m.graph = nullptr;
+    }
+    SG_TRY(mlp_partials(m, blocks));
+    const int64_t stride = batch_stride(n_ex);
+    const float scale = 1.0f / (float)slots;
+    // the step loop as one graph: grad pass, Adam, step counter
+    cudaGraph_t graph = nullptr;
+    SG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int s = 0; s < per; ++s) {
+      mlp_grad_kernel<<<(unsigned)blocks, kTrainThreads, kTrainSmem, st>>>(
+          m.wbf, F, T, nullptr, n_ex, slots, m.step, slots, stride, n, holdout, scale,
+          m.part.as<float>(), m.lpart.as<double>());
+      mlp_adam_kernel<<<(kMlpParams + 255) / 256, 256, 0, st>>>(m.part.as<float>(), blocks,
+                                                               m.master, m.wbf, m.m1, m.m2, m.step,
+                                                               lr);
+      mlp_step_kernel<<<1, 1, 0, st>>>(m.step);
+    }
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    if (ce != cudaSuccess)
+      return fail(SAIGE_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce));
+    const cudaError_t ie = cudaGraphInstantiate(&m.graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      m.graph = nullptr;
+      return fail(SAIGE_ECUDA, "graph instantiation failed: %s", cudaGetErrorString(ie));
+    }
+    m.graph_key[0] = F;
+    m.graph_key[1] = T;
+    m.graph_n = n;
+    m.graph_q = q;
+    m.graph_batch = batch;
+    m.graph_holdout = holdout;
+    m.graph_lr = lr;
+    m.graph_steps = per;
   }
-  const cudaError_t ce = cudaStreamEndCapture(st, &graph);
-  if (ce != cudaSuccess) return fail(SAIGE_ECUDA, "graph capture failed: %s", cudaGetErrorString(ce));
-  cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e == cudaSuccess) e = cudaGraphLaunch(exec, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (exec) cudaGraphExecDestroy(exec);
-  cudaGraphDestroy(graph);
-  if (e != cudaSuccess) return fail(SAIGE_ECUDA, "MLP training graph: %s", cudaGetErrorString(e));
-  count_launches(3 * steps);
-  m.trained_steps += steps;
+  const int launches = (int)ceil_div(steps, per);
+  for (int l = 0; l < launches; ++l) SG_CUDA(cudaGraphLaunch(m.graph, st));
+  count_launches(3 * per * launches);
+  m.trained_steps += (int64_t)per * launches;
   return Status();
 }
 
 Status mlp_validate(Mlp& m, const float* F, const float* T, int64_t n, int q, int holdout,
                     double* mse, double* target_ms, cudaStream_t st) {
-  const int64_t n_ex = n * q;
+  const int64_t nh = (n + holdout - 1) / holdout, n_out = nh * q;
   DevBuf y, part;
-  SG_TRY(y.reserve((size_t)n_ex * sizeof(float)));
-  const int blocks = (int)std::min<int64_t>(ceil_div(n_ex, 256), 1024);
+  SG_TRY(y.reserve((size_t)n_out * sizeof(float)));
+  const int blocks = (int)std::min<int64_t>(ceil_div(n_out, 256), 1024);
   SG_TRY(part.reserve((size_t)blocks * 2 * sizeof(double)));
-  SG_TRY(mlp_forward(m, F, n_ex, y.as<float>(), st));
-  mlp_val_kernel<<<(unsigned)blocks, 256, 0, st>>>(y.as<float>(), T, n_ex, n, holdout,
+  SG_CUDA(set_smem_attrs());
+  const int64_t fb = std::min<int64_t>(ceil_div(n_out, kFwdThreads), 148 * 8);
+  mlp_forward_kernel<<<(unsigned)fb, kFwdThreads, kFwdSmem, st>>>(m.wbf, F, n_out, n, holdout,
+                                                                 y.as<float>());
+  mlp_val_kernel<<<(unsigned)blocks, 256, 0, st>>>(y.as<float>(), T, n_out, n, holdout,
                                                    part.as<double>());
-  count_launches(1);
+  count_launches(2);
   SG_CHECK_LAUNCH();
   std::vector<double> h((size_t)blocks * 2);
   SG_CUDA(cudaMemcpyAsync(h.data(), part.ptr, h.size() * 8, cudaMemcpyDeviceToHost, st));
@@ -582,11 +609,8 @@ Status mlp_validate(Mlp& m, const float* F, const float* T, int64_t n, int q, in
     se += h[(size_t)2 * b];
     stt += h[(size_t)2 * b + 1];
   }
-  int64_t cnt = 0;
-  for (int64_t i = 0; i < n; i += holdout) ++cnt;
-  cnt *= q;
-  *mse = cnt ? se / (double)cnt : 0.0;
-  *target_ms = cnt ? stt / (double)cnt : 0.0;
+  *mse = n_out ? se / (double)n_out : 0.0;
+  *target_ms = n_out ? stt / (double)n_out : 0.0;
   return Status();
 }
 

@@ -26,6 +26,16 @@ constexpr int kMlpParams = kMlpB4 + 1;
 
 struct Mlp {
   DevBuf mem;
+  DevBuf part, lpart;         // per-block gradient partials of the training pass
+  int part_blocks = 0;
+  cudaGraphExec_t graph = nullptr;  // captured training steps (see mlp_train)
+  const void* graph_key[2] = {nullptr, nullptr};
+  int64_t graph_n = 0;
+  int graph_q = 0, graph_batch = 0, graph_holdout = 0, graph_steps = 0;
+  float graph_lr = 0.f;
+  ~Mlp() {
+    if (graph) cudaGraphExecDestroy(graph);
+  }
   float* master = nullptr;    // FP32 weights
   uint16_t* wbf = nullptr;    // BF16 copy used by the forward passes
   float* grad = nullptr;      // gradient accumulator
@@ -50,7 +60,8 @@ Status mlp_grad(Mlp& m, const float* F, const float* T, const int64_t* idx, int6
 
 // steps Adam steps (lr, betas 0.9/0.999) on mini-batches of `batch` examples drawn
 // from the training examples (every example whose sample index i = e % n has
-// i % holdout != 0); the steps run as one captured CUDA graph.
+// i % holdout != 0).  The steps run as launches of one captured CUDA graph of up to
+// 25 steps, kept in m and reused while F, T and the sizes stay the same.
 Status mlp_train(Mlp& m, const float* F, const float* T, int64_t n, int q, int steps, int batch,
                  float lr, int holdout, cudaStream_t st);
 
