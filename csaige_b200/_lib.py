@@ -310,6 +310,7 @@ SIGNATURES = {
     "saige_grm_get_stats": (C.c_int32, [_vp, P(GrmStatsC)]),
     "saige_grm_reset_stats": (C.c_int32, [_vp]),
     "saige_kernel_launches": (C.c_int64, []),
+    "saige_tc_autotune_trials": (C.c_int64, []),
     "saige_gen_bed": (C.c_int32, [P(CohortSpecC), _vp, C.c_int32]),
     "saige_gen_pheno": (C.c_int32, [P(CohortSpecC), _d, _d]),
 }

@@ -10,6 +10,7 @@
 #include <vector>
 
 #include "engine.cuh"
+#include "kernels.cuh"
 #include "rng.hpp"
 #include "vr.cuh"
 #include "mlp.cuh"
@@ -883,6 +884,86 @@ SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t
 }
 
 
+// Uploads the .bed into d_bed.  From pinned host memory the upload runs in marker
+// chunks on a copy stream and each chunk's allele and missing counts (K1) run as soon
+// as it has landed, so that the counts hide under the PCIe transfer; af, mac and
+// n_valid then follow traits.rs:42-54 from the exact counts (counted = true).  From
+// pageable memory it is one copy and counted = false.
+static Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                               const int64_t* sample_idx, int64_t n, DevBuf& d_bed,
+                               std::vector<double>& af, std::vector<double>& mac,
+                               std::vector<int64_t>& nv, bool& counted) {
+  counted = false;
+  cudaPointerAttributes attr{};
+  const bool pinned =
+      cudaPointerGetAttributes(&attr, bed) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();
+  if (!pinned) {
+    SG_CUDA(cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice));
+    return Status();
+  }
+  SG_TRY(check_bed_header(bed, bed_len, n_fam, m_tot));
+  std::vector<int32_t> sidx;
+  bool identity = true;
+  SG_TRY(check_subset(sample_idx, n, n_fam, sidx, identity));
+  const int64_t bpm = (n_fam + 3) / 4;
+  struct Streams {
+    cudaStream_t c = nullptr, k = nullptr;
+    std::vector<cudaEvent_t> ev;
+    ~Streams() {
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+      if (c) cudaStreamDestroy(c);
+      if (k) cudaStreamDestroy(k);
+    }
+  } ss;
+  SG_CUDA(cudaStreamCreateWithFlags(&ss.c, cudaStreamNonBlocking));
+  SG_CUDA(cudaStreamCreateWithFlags(&ss.k, cudaStreamNonBlocking));
+  constexpr int kChunks = 16;
+  const int64_t per = ceil_div(m_tot, kChunks);
+  DevBuf d_rows, d_sidx, d_cnt;
+  std::vector<int64_t> rows((size_t)m_tot);
+  for (int64_t j = 0; j < m_tot; ++j) rows[(size_t)j] = j;
+  SG_TRY(d_rows.reserve((size_t)m_tot * 8));
+  SG_TRY(d_cnt.reserve((size_t)m_tot * 2 * 8));
+  SG_CUDA(cudaMemcpyAsync(d_rows.ptr, rows.data(), (size_t)m_tot * 8, cudaMemcpyHostToDevice, ss.k));
+  const int32_t* sp = nullptr;
+  if (!identity) {
+    SG_TRY(d_sidx.reserve(sidx.size() * 4));
+    SG_CUDA(cudaMemcpyAsync(d_sidx.ptr, sidx.data(), sidx.size() * 4, cudaMemcpyHostToDevice, ss.k));
+    sp = d_sidx.as<int32_t>();
+  }
+  uint8_t* dst = d_bed.as<uint8_t>();
+  for (int64_t j0 = 0; j0 < m_tot; j0 += per) {
+    const int64_t j1 = std::min(m_tot, j0 + per);
+    const size_t lo = j0 == 0 ? 0 : (size_t)(3 + j0 * bpm);
+    const size_t hi = j1 == m_tot ? bed_len : (size_t)(3 + j1 * bpm);
+    SG_CUDA(cudaMemcpyAsync(dst + lo, bed + lo, hi - lo, cudaMemcpyHostToDevice, ss.c));
+    cudaEvent_t e = nullptr;
+    SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    ss.ev.push_back(e);
+    SG_CUDA(cudaEventRecord(e, ss.c));
+    SG_CUDA(cudaStreamWaitEvent(ss.k, e, 0));
+    SG_CUDA(launch_bed_gather(dst, bpm, d_rows.as<int64_t>() + j0, j1 - j0, sp, n, nullptr, 0,
+                              d_cnt.as<int64_t>() + 2 * j0, ss.k));
+  }
+  std::vector<int64_t> cnt((size_t)m_tot * 2);
+  SG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost, ss.k));
+  SG_CUDA(cudaStreamSynchronize(ss.k));
+  SG_CUDA(cudaStreamSynchronize(ss.c));
+  for (int64_t j = 0; j < m_tot; ++j) {
+    const int64_t alt = cnt[(size_t)(2 * j)], miss = cnt[(size_t)(2 * j + 1)];
+    const int64_t valid = n - miss;
+    // traits.rs:42-54, the same f64 operations on the same exact integers
+    const double sum = (double)alt;
+    af[(size_t)j] = valid > 0 ? sum / (2.0 * (double)valid) : 0.0;
+    const double other = 2.0 * (double)valid - sum;
+    mac[(size_t)j] = sum < other ? sum : other;
+    nv[(size_t)j] = valid;
+  }
+  counted = true;
+  return Status();
+}
+
 SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
                                        int64_t m_tot, const int64_t* sample_idx, int64_t n,
                                        const double* y, const double* x, int32_t p, int32_t trait,
@@ -904,15 +985,19 @@ SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64
     Status s = d_bed.reserve(bed_len);
     if (!s.ok()) return s.code;
     tm.mark("alloc bed");
-    if (cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice) != cudaSuccess)
-      return fail(SAIGE_ECUDA, "bed upload failed: %s", cudaGetErrorString(cudaGetLastError())).code;
-    tm.mark("upload");
     std::vector<double> af((size_t)m_tot), mac((size_t)m_tot);
     std::vector<int64_t> nv((size_t)m_tot);
-    int32_t rc = saige_bed_marker_stats_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx,
-                                            n, af.data(), mac.data(), nv.data());
-    if (rc != SAIGE_OK) return rc;
-    tm.mark("counts");
+    int32_t rc = SAIGE_OK;
+    bool counted = false;
+    s = upload_and_count(bed, bed_len, n_fam, m_tot, sample_idx, n, d_bed, af, mac, nv, counted);
+    if (!s.ok()) return s.code;
+    tm.mark(counted ? "upload+counts" : "upload");
+    if (!counted) {
+      rc = saige_bed_marker_stats_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx, n,
+                                      af.data(), mac.data(), nv.data());
+      if (rc != SAIGE_OK) return rc;
+      tm.mark("counts");
+    }
     std::vector<int64_t> gidx((size_t)m_tot), vidx((size_t)m_tot);
     int64_t m_grm = 0, m_vr = 0;
     rc = saige_select_grm_markers(af.data(), mac.data(), nv.data(), m_tot, n, min_maf, max_missing,

@@ -608,6 +608,8 @@ SG_API int32_t saige_grm_reset_stats(saige_grm* h) {
 
 SG_API int64_t saige_kernel_launches(void) { return launches_total(); }
 
+SG_API int64_t saige_tc_autotune_trials(void) { return tc_autotune_trials(); }
+
 SG_API int32_t saige_release_cached_memory(void) {
   SG_GUARD_BEGIN
   release_cached_blocks();

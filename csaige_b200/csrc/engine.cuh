@@ -18,7 +18,7 @@ namespace saige {
 // reserve() reuses a cached block of the same device of 1 to 1.25 times the size,
 // so that repeated fits of one cohort shape do not map and unmap tens of GB each
 // time.  release_cached_blocks() hands the cache back to the driver.
-constexpr size_t kCacheMinBytes = (size_t)256 << 20;
+constexpr size_t kCacheMinBytes = (size_t)16 << 20;
 
 struct DevBuf {
   void* ptr = nullptr;

@@ -42,8 +42,11 @@
 #include <math.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
+#include <mutex>
 #include <vector>
 
 #include "kernels.cuh"
@@ -875,10 +878,136 @@ static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
   if (a.sa < 2 || (a.sa & 1) || a.sa > kMaxSA || a.sl < 2 || a.sl > kMaxSL || a.sub < 1 ||
       a.sub > 4)
     return cudaErrorInvalidValue;
-  tc_grm_kernel<kPassB><<<grid, kThreads, tc_smem_bytes(a.ng, kPassB), st>>>(a);
+  const size_t smem = tc_fixed_bytes() + (size_t)a.sl * plan_l_stage(a.ng, kPassB, a.sub);
+  if (smem > kSmemBudget) return cudaErrorInvalidValue;
+  tc_grm_kernel<kPassB><<<grid, kThreads, smem, st>>>(a);
   count_launches(1);
   return cudaGetLastError();
 }
+
+// ---- ring-shape autotuner ----------------------------------------------------
+// The ring shape (sub-stages per load stage, load-ring depth, TMEM operand slots)
+// does not change a product's result — the sums are exact integers and the epilogue
+// is per element — only its speed.  The first launch of each (pass, ng, grid, nk)
+// in the process times every shape that fits (sub 4, 2, 1 with the deepest ring the
+// shared memory holds) on the real operands and keeps the fastest; later launches of
+// the same key use it.  SAIGE_TC_AUTOTUNE=0 keeps the fixed choice of tc_rings.
+namespace {
+
+struct TuneKey {
+  int dev, pass_b, ng, nk;
+  unsigned grid;
+  bool operator<(const TuneKey& o) const {
+    if (dev != o.dev) return dev < o.dev;
+    if (pass_b != o.pass_b) return pass_b < o.pass_b;
+    if (ng != o.ng) return ng < o.ng;
+    if (nk != o.nk) return nk < o.nk;
+    return grid < o.grid;
+  }
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, Rings> g_tune;
+std::atomic<int64_t> g_tune_trials{0};
+
+bool autotune_on() {
+  const char* e = getenv("SAIGE_TC_AUTOTUNE");
+  return !(e && e[0] == '0');
+}
+
+std::vector<Rings> tc_candidates(int ng, bool pass_b) {
+  std::vector<Rings> out;
+  const size_t room = kSmemBudget - tc_fixed_bytes();
+  const Rings base = tc_rings(ng, pass_b);
+  for (int sub : {4, 2, 1}) {
+    const size_t ls = plan_l_stage(ng, pass_b, sub);
+    if (2 * ls > room) continue;
+    Rings g = base;
+    g.sub = sub;
+    g.sl = (int)std::min<size_t>(kMaxSL, room / ls);
+    out.push_back(g);
+  }
+  return out;
+}
+
+}  // namespace
+
+// Launches pass kPassB with the tuned ring shape of its key, tuning it first when the
+// key is new.  a carries everything but the ring shape.
+template <bool kPassB>
+static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st) {
+  const Rings fixed = tc_rings(a.ng, kPassB);
+  if (!autotune_on()) {
+    a.sub = fixed.sub;
+    a.sl = fixed.sl;
+    a.sa = fixed.sa;
+    SG_CUDA(launch_tc<kPassB>(grid, a, st));
+    return Status();
+  }
+  const TuneKey key{dev, kPassB ? 1 : 0, a.ng, a.nk, grid};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      a.sub = it->second.sub;
+      a.sl = it->second.sl;
+      a.sa = it->second.sa;
+      SG_CUDA(launch_tc<kPassB>(grid, a, st));
+      return Status();
+    }
+  }
+  const std::vector<Rings> cand = tc_candidates(a.ng, kPassB);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  SG_CUDA(cudaEventCreate(&e0));
+  SG_CUDA(cudaEventCreate(&e1));
+  Rings best = fixed;
+  float best_ms = 0.f;
+  bool have = false;
+  Status st_out;
+  for (const Rings& g : cand) {
+    a.sub = g.sub;
+    a.sl = g.sl;
+    a.sa = g.sa;
+    cudaEventRecord(e0, st);
+    const cudaError_t le = launch_tc<kPassB>(grid, a, st);
+    if (le != cudaSuccess) {
+      (void)cudaGetLastError();
+      continue;
+    }
+    cudaEventRecord(e1, st);
+    if (cudaEventSynchronize(e1) != cudaSuccess) {
+      st_out = fail(SAIGE_ECUDA, "tensor-core launch failed while tuning: %s",
+                    cudaGetErrorString(cudaGetLastError()));
+      break;
+    }
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    g_tune_trials += 1;
+    if (!have || ms < best_ms) {
+      best = g;
+      best_ms = ms;
+      have = true;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!st_out.ok()) return st_out;
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    g_tune[key] = best;
+  }
+  // the output of the last trial is already complete; launch again only when the
+  // chosen shape was not the last one tried, so that the result comes from it too
+  if (!have || !(cand.back().sub == best.sub && cand.back().sl == best.sl)) {
+    a.sub = best.sub;
+    a.sl = best.sl;
+    a.sa = best.sa;
+    SG_CUDA(launch_tc<kPassB>(grid, a, st));
+  }
+  return Status();
+}
+
+int64_t tc_autotune_trials() { return g_tune_trials.load(); }
 
 Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
                   cudaStream_t st) {
@@ -942,10 +1071,6 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.ng = ng;
       a.r = r;
       a.nk = (int)n_stages_a;
-      const Rings g = tc_rings(ng, false);
-      a.sub = g.sub;
-      a.sl = g.sl;
-      a.sa = g.sa;
       a.tiles = p->tiles_m.as<uint8_t>();
       a.img_g = p->img_a.as<uint8_t>();
       a.scale_g = sc.scale_v;
@@ -959,7 +1084,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       const unsigned grid = (unsigned)(h->m_pad / kRows);
       cudaEvent_t t0 = nullptr, t1 = nullptr;
       SG_TRY(mark(&t0));
-      SG_CUDA(launch_tc<false>(grid, a, st));
+      SG_TRY(launch_tc_tuned<false>(h->device, grid, a, st));
       // leave-one-chromosome-out: the left-out markers' rows of u do not enter pass B
       if (h->masked) SG_CUDA(mask_rows_f64(p->u.as<double>(), h->m_pad, r, h->excl.as<uint8_t>(),
                                            h->m, st));
@@ -989,10 +1114,6 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.ng = ng;
       a.r = r;
       a.nk = (int)n_stages_b;
-      const Rings g = tc_rings(ng, true);
-      a.sub = g.sub;
-      a.sl = g.sl;
-      a.sa = g.sa;
       a.tiles = p->tiles_s.as<uint8_t>();
       a.img_g = p->img_w.as<uint8_t>();
       a.img_m = p->img_c.as<uint8_t>();
@@ -1008,7 +1129,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       const unsigned grid = (unsigned)(h->n_pad / kRows);
       cudaEvent_t t0 = nullptr, t1 = nullptr;
       SG_TRY(mark(&t0));
-      SG_CUDA(launch_tc<true>(grid, a, st));
+      SG_TRY(launch_tc_tuned<true>(h->device, grid, a, st));
       SG_TRY(mark(&t1));
       if (h->profiling) ev_b.emplace_back(t0, t1);
       h->stats.tc_pass_b_launches += 1;

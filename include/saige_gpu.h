@@ -432,6 +432,12 @@ int32_t saige_grm_reset_stats(saige_grm* h);
 /* Kernels this library has launched in the process so far. */
 int64_t saige_kernel_launches(void);
 
+/* Trial launches of the tensor-core ring-shape autotuner in this process: the first
+ * MIXED product of each (pass, column group, grid, stage count) times every ring shape
+ * that fits and keeps the fastest (results are identical for all shapes).
+ * SAIGE_TC_AUTOTUNE=0 in the environment keeps the fixed shape. */
+int64_t saige_tc_autotune_trials(void);
+
 /* ---------------------------------------------------------------------
  * Explicit GRM: replaces compute_dense_grm (saige-core/src/grm/dense.rs:22-112),
  * compute_grm_from_dosages (dense.rs:115-186), compute_sparse_grm

@@ -120,3 +120,22 @@ def test_large_blocks_reused_from_cache_give_same_products():
         outs.append(grm.mat_vec(v))
         grm.close()
     assert np.array_equal(outs[0], outs[1]) and np.array_equal(outs[0], outs[2])
+
+
+def test_autotuned_ring_shapes_give_identical_products(monkeypatch):
+    # the ring shape changes only the speed of the exact-integer product
+    n, m = 3000, 2600
+    spec = cs.CohortSpec(n=n, m=m, seed=41, missing_rate=0.01)
+    bed = cs.gen_bed(spec)
+    af, mac, nv = cs.bed_marker_stats(bed, n, m)
+    g, _ = cs.select_grm_markers(af, mac, nv, n)
+    v = np.random.default_rng(3).standard_normal((37, n))
+    monkeypatch.setenv("SAIGE_TC_AUTOTUNE", "0")
+    fixed = cs.OnTheFlyGrm.from_bed(bed, n, m, g, af[g], precision=cs.PREC_MIXED).mat_vec(v)
+    monkeypatch.setenv("SAIGE_TC_AUTOTUNE", "1")
+    before = int(cs.api.LIB.saige_tc_autotune_trials())
+    grm = cs.OnTheFlyGrm.from_bed(bed, n, m, g, af[g], precision=cs.PREC_MIXED)
+    tuned = grm.mat_vec(v)      # tunes both passes of this key
+    again = grm.mat_vec(v)      # uses the tuned shapes
+    assert int(cs.api.LIB.saige_tc_autotune_trials()) > before
+    assert np.array_equal(fixed, tuned) and np.array_equal(tuned, again)

@@ -146,3 +146,22 @@ def test_fit_null_outputs_written_and_read_back(tmp_path):
     assert np.array_equal(mdl.tau, fr.ai_reml.tau)
     assert mdl.variance_ratio.variance_ratio == fr.variance_ratio.variance_ratio
     assert open(vr_path).read().endswith(" null 1\n")
+
+
+def test_pinned_upload_path_gives_the_same_fit():
+    # from pinned host memory the .bed is uploaded in chunks with the counts overlapped
+    import torch
+    n, m = 1500, 2500
+    spec = cs.CohortSpec(n=n, m=m, seed=31, missing_rate=0.02, prevalence=0.2, h2=0.3, n_covar=2)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    pinned = torch.empty(bed.size, dtype=torch.uint8, pin_memory=True)
+    pinned.numpy()[:] = bed
+    cfg = cs.AiRemlConfig(max_iter=4, precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
+                          warm_start=cs.WARM_RECYCLED)
+    a = cs.fit_null_from_bed(bed, n, m, y, x, cs.TraitType.Binary, cfg, variance_ratio=True)
+    b = cs.fit_null_from_bed(pinned.numpy(), n, m, y, x, cs.TraitType.Binary, cfg,
+                             variance_ratio=True)
+    assert (a.m_grm, a.m_vr) == (b.m_grm, b.m_vr)
+    assert np.array_equal(a.ai_reml.tau, b.ai_reml.tau)
+    assert a.variance_ratio.variance_ratio == b.variance_ratio.variance_ratio
