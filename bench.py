@@ -80,6 +80,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--warm", choices=["previous", "recycled", "learned"], default="recycled",
                     help="PCG start of the fast configuration")
+    ap.add_argument("--no-cohorts", action="store_true",
+                    help="skip the 16 sub-cohort fits")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-versus-recycled start comparison")
     ap.add_argument("--no-explicit-grm", action="store_true",
@@ -465,6 +467,28 @@ def run_ours(args, world, rank, local):
             # the reference solves each used marker alone: its PCG iterations plus the
             # A*0 product of each solve (decomposition.rs:226)
             "reference_kv_estimate": int(v.pcg_iters + v.n_solved)}
+    # 16 sub-cohorts of the same .bed, N log-uniform in [5k, 60k] (the workload's
+    # sub-cohort part): their fits one after the other and concurrently (own threads and
+    # streams), from the same host buffer
+    if not args.no_cohorts and world == 1 and host_bed is not None:
+        rng = np.random.default_rng(WORKLOAD["seed"])
+        sizes = np.exp(rng.uniform(np.log(5000), np.log(min(60000, n)), 16)).astype(int)
+        cohorts = []
+        for sz in sizes:
+            idx = np.sort(rng.choice(n, int(sz), replace=False))
+            cohorts.append((idx, y[idx], x[idx]))
+        hb = host_bed.numpy()
+        cs.fit_null_cohorts(hb, n, m, cohorts[:2], cs.TraitType.Binary, fast, concurrent=True)
+        seq, seq_wall = cs.fit_null_cohorts(hb, n, m, cohorts, cs.TraitType.Binary, fast,
+                                            concurrent=False)
+        con, con_wall = cs.fit_null_cohorts(hb, n, m, cohorts, cs.TraitType.Binary, fast,
+                                            concurrent=True)
+        line["sub_cohorts"] = {
+            "n_cohorts": len(cohorts), "sizes": [int(v) for v in sizes],
+            "sequential_s": seq_wall, "concurrent_s": con_wall,
+            "speedup": seq_wall / con_wall, "fits_per_s": len(cohorts) / con_wall,
+            "same_tau": all(np.array_equal(a.tau, b.tau) for a, b in zip(seq, con)),
+            "config": "fit_null::run per cohort (counts, QC, GRM, AI-REML), .bed uploaded once"}
     # the learned start against the recycled one on the same cohort, to an AI-REML
     # tolerance tight enough for several iterations (the default 0.02 stops after the
     # first iteration with tau1 > 0, before the network has a transition to learn from)

@@ -228,6 +228,12 @@ SIGNATURES = {
     "saige_release_cached_memory": (C.c_int32, []),
     "saige_write_null_model": (C.c_int32, [C.c_char_p, P(NullModelC)]),
     "saige_xvx_inv_xv": (C.c_int32, [_d, _d, C.c_int64, C.c_int32, _d]),
+    "saige_fit_null_cohorts": (
+        C.c_int32,
+        [_u8, _sz, C.c_int64, C.c_int64, C.c_int32, P(_i64), _i64, P(_d), P(_d), C.c_int32,
+         C.c_int32, C.c_double, C.c_double, P(AiRemlConfigC), C.c_int32, P(AiRemlSummaryC), P(_d),
+         _i64, _d],
+    ),
     "saige_mlp_param_count": (C.c_int32, []),
     "saige_mlp_initial_params": (C.c_int32, [C.c_uint64, P(C.c_float)]),
     "saige_mlp_eval": (C.c_int32, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64,

@@ -827,6 +827,55 @@ def fit_null_from_bed(bed, n_fam: int, m_tot: int, y, x, trait_type: TraitType,
     return FitNullResult(res, mg.value, mv.value, vr)
 
 
+@dataclass
+class CohortFit:
+    tau: np.ndarray
+    iterations: int
+    converged: bool
+    alpha: np.ndarray
+    m_grm: int
+    n_kv_launches: int
+    pcg_iters: int
+    seconds: float
+
+
+def fit_null_cohorts(bed, n_fam: int, m_tot: int, cohorts, trait_type: TraitType,
+                     config: AiRemlConfig = AiRemlConfig(), min_maf: float = 0.01,
+                     max_missing: float = 0.15, concurrent: bool = True):
+    """fit_null::run (genotype part, no variance ratio) for each sub-cohort of one .bed.
+    cohorts: sequence of (sample_idx, y, x).  Returns ([CohortFit], wall seconds); with
+    concurrent the cohorts run on their own threads and streams."""
+    b = _bed_array(bed)
+    k = len(cohorts)
+    sidx = [np.ascontiguousarray(c[0], dtype=np.int64) for c in cohorts]
+    ys = [_f64(c[1]) for c in cohorts]
+    xs, ps = zip(*[_design(c[2], ys[i].size) for i, c in enumerate(cohorts)])
+    if len(set(ps)) != 1:
+        raise SaigeError(_lib.EINVAL, "every cohort needs the same covariate count")
+    p = ps[0]
+    alphas = [np.zeros(p) for _ in range(k)]
+    P = C.POINTER
+    s_arr = (P(C.c_int64) * k)(*[_i64ptr(a) for a in sidx])
+    n_arr = np.array([a.size for a in sidx], dtype=np.int64)
+    y_arr = (P(C.c_double) * k)(*[_dptr(a) for a in ys])
+    x_arr = (P(C.c_double) * k)(*[_dptr(a) for a in xs])
+    a_arr = (P(C.c_double) * k)(*[_dptr(a) for a in alphas])
+    outs = (_lib.AiRemlSummaryC * k)()
+    mg = np.zeros(k, dtype=np.int64)
+    wall = C.c_double(0.0)
+    cfg = _lib.AiRemlConfigC(config.max_iter, config.tol, config.pcg_tol, config.pcg_max_iter,
+                             config.n_random_vectors, config.seed, config.precision, config.solve,
+                             config.warm_start, config.precond)
+    check(LIB.saige_fit_null_cohorts(
+        b.ctypes.data_as(C.POINTER(C.c_uint8)), b.size, n_fam, m_tot, k, s_arr, _i64ptr(n_arr),
+        y_arr, x_arr, p, int(trait_type), min_maf, max_missing, C.byref(cfg), 1 if concurrent else 0,
+        outs, a_arr, _i64ptr(mg), C.byref(wall)))
+    res = [CohortFit(np.array([o.tau[0], o.tau[1]]), o.iterations, bool(o.converged), alphas[i],
+                     int(mg[i]), o.n_kv_launches, o.pcg_iters, o.seconds)
+           for i, o in enumerate(outs)]
+    return res, wall.value
+
+
 def _with_extension(prefix, ext: str) -> str:
     """std::path::Path::with_extension: replace (or add) the last component's extension."""
     import os

@@ -34,6 +34,7 @@ SOURCES = [
     "grm_explicit.cu",
     "warm.cu",
     "mlp.cu",
+    "cohorts.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

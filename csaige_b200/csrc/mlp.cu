@@ -13,6 +13,8 @@
 #include <string.h>
 
 #include <cmath>
+#include <mutex>
+#include <set>
 #include <vector>
 
 #include "mlp.cuh"
@@ -398,15 +400,21 @@ __global__ void mlp_val_kernel(const float* __restrict__ y, const float* __restr
 constexpr size_t kFwdSmem = (size_t)(kSmemWFloats + IN * kFwdThreads + 2 * H * kFwdThreads) * 4;
 constexpr size_t kTrainSmem = (size_t)(kSmemWFloats + IN * kTrainThreads + 3 * H * kTrainThreads) * 4;
 
+// The dynamic shared-memory limits are a per-device attribute: set once per device.
 cudaError_t set_smem_attrs() {
-  static bool done = false;
-  if (done) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)kFwdSmem);
+  static std::mutex mu;
+  static std::set<int> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lk(mu);
+  if (done.count(dev)) return cudaSuccess;
+  e = cudaFuncSetAttribute(mlp_forward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)kFwdSmem);
   if (e != cudaSuccess) return e;
   e = cudaFuncSetAttribute(mlp_grad_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)kTrainSmem);
-  if (e == cudaSuccess) done = true;
+  if (e == cudaSuccess) done.insert(dev);
   return e;
 }
 

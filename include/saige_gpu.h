@@ -526,6 +526,21 @@ int32_t saige_sparse_grm_from_triplets(int64_t n, int64_t nnz, const int32_t* ro
 int32_t saige_write_sparse_grm(const saige_sparse_grm* g, const char* const* sample_ids,
                                int64_t n_ids, const char* mtx_path, const char* ids_path);
 
+/* Fit-null of n_cohorts sub-cohorts of one .bed (sample_idx[c][0..n[c]), y[c],
+ * x[c] n[c] x p column-major): per cohort the steps of saige_fit_null_from_bed
+ * without the variance ratio (counts, QC and VR/GRM split over the cohort's samples,
+ * GRM, AI-REML) — fit_null::run per cohort (fit_null.rs:199-287).  The .bed is
+ * uploaded once; with concurrent != 0 each cohort runs on its own host thread and
+ * stream, so that small cohorts' launches overlap.  out[c], alpha[c] (p, may be
+ * NULL), m_grm[c] (may be NULL); wall_seconds (may be NULL) = the whole call. */
+int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                               int32_t n_cohorts, const int64_t* const* sample_idx,
+                               const int64_t* n, const double* const* y, const double* const* x,
+                               int32_t p, int32_t trait, double min_maf, double max_missing,
+                               const saige_ai_reml_config* cfg, int32_t concurrent,
+                               saige_ai_reml_summary* out, double* const* alpha, int64_t* m_grm,
+                               double* wall_seconds);
+
 /* ---------------------------------------------------------------------
  * The MLP of the learned PCG start (SAIGE_WARM_LEARNED; no reference
  * counterpart).  8 inputs, three tanh layers of 64, a linear output; BF16

@@ -165,3 +165,27 @@ def test_pinned_upload_path_gives_the_same_fit():
     assert (a.m_grm, a.m_vr) == (b.m_grm, b.m_vr)
     assert np.array_equal(a.ai_reml.tau, b.ai_reml.tau)
     assert a.variance_ratio.variance_ratio == b.variance_ratio.variance_ratio
+
+
+@pytest.mark.parametrize("concurrent", [True, False])
+def test_sub_cohort_fits_equal_their_own_fits(concurrent):
+    # fit_null::run per sub-cohort of one .bed, concurrently on threads and streams
+    n, m = 3000, 2000
+    spec = cs.CohortSpec(n=n, m=m, seed=37, missing_rate=0.01, prevalence=0.3, h2=0.3, n_covar=2)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    rng = np.random.default_rng(5)
+    cohorts = []
+    for size in (700, 1300, 2200):
+        idx = np.sort(rng.choice(n, size, replace=False))
+        cohorts.append((idx, y[idx], x[idx]))
+    cfg = cs.AiRemlConfig(max_iter=6, precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
+                          warm_start=cs.WARM_RECYCLED)
+    res, wall = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg,
+                                    concurrent=concurrent)
+    assert wall > 0 and len(res) == 3
+    for (idx, yc, xc), r in zip(cohorts, res):
+        one = cs.fit_null_from_bed(bed, n, m, yc, xc, cs.TraitType.Binary, cfg, sample_idx=idx)
+        assert r.m_grm == one.m_grm
+        assert np.array_equal(r.tau, one.ai_reml.tau)
+        assert np.array_equal(r.alpha, one.ai_reml.alpha)
