@@ -80,6 +80,7 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--warm", choices=["previous", "recycled", "learned"], default="recycled",
                     help="PCG start of the fast configuration")
+    ap.add_argument("--no-loco", action="store_true", help="skip the LOCO fits")
     ap.add_argument("--no-cohorts", action="store_true",
                     help="skip the 16 sub-cohort fits")
     ap.add_argument("--no-learned", action="store_true",
@@ -467,6 +468,29 @@ def run_ours(args, world, rank, local):
             # the reference solves each used marker alone: its PCG iterations plus the
             # A*0 product of each solve (decomposition.rs:226)
             "reference_kv_estimate": int(v.pcg_iters + v.n_solved)}
+    # LOCO (loco.rs:54-117): one fit per chromosome with it left out of the GRM; the
+    # GRM markers are split into 22 blocks in proportion to the GRCh38 autosome lengths
+    loco_sizes = None
+    if not args.no_loco and world == 1:
+        lengths = [248, 242, 198, 190, 181, 171, 159, 145, 138, 134, 135, 133, 114, 107, 102,
+                   90, 83, 80, 59, 64, 47, 51]
+        mg = len(gidx)
+        cuts = (np.cumsum([0] + lengths) / sum(lengths) * mg).astype(int)
+        chrom = [""] * mg
+        for c in range(22):
+            for j in range(cuts[c], cuts[c + 1]):
+                chrom[j] = str(c + 1)
+        loco_sizes = [int(cuts[c + 1] - cuts[c]) for c in range(22)]
+        t0 = time.perf_counter()
+        lres = cs.run_loco(y, x, grm, chrom, cs.TraitType.Binary, fast)
+        lwall = time.perf_counter() - t0
+        line["loco"] = {
+            "chromosomes": 22, "wall_s": lwall,
+            "device_s": float(sum(r.seconds for r in lres.values())),
+            "n_kv": int(sum(r.n_kv for r in lres.values())),
+            "ai_reml_iterations": int(sum(r.iterations for r in lres.values())),
+            "config": "22 chromosome blocks of the GRM markers, fast configuration, one handle "
+                      "(markers left out by masking between the product passes)"}
     # 16 sub-cohorts of the same .bed, N log-uniform in [5k, 60k] (the workload's
     # sub-cohort part): their fits one after the other and concurrently (own threads and
     # streams), from the same host buffer
@@ -534,6 +558,18 @@ def run_ours(args, world, rank, local):
         line["cpu_baseline"] = {
             "value": per_kv * kv_fit, "unit": "s", "cores": smp.threads, "kind": "port",
             "sample": smp.describe(m, kv_fit), "sec_per_kv": per_kv}
+        # the same per-product CPU time, times each extra path's reference product count
+        if "variance_ratio" in line:
+            vr = line["variance_ratio"]
+            vr["cpu_extrapolated_s"] = per_kv * vr["reference_kv_estimate"]
+            vr["cpu_note"] = ("reference products (one PCG per used marker) x the CPU port's "
+                              "seconds per product")
+        if "loco" in line and loco_sizes is not None:
+            mg = float(sum(loco_sizes))
+            line["loco"]["cpu_extrapolated_s"] = sum(per_kv * kv_fit * (mg - mc) / mg
+                                                     for mc in loco_sizes)
+            line["loco"]["cpu_note"] = ("22 fits x the reference strategy's product count x the "
+                                        "CPU port's seconds per product, scaled by M - M_chrom")
     if rank == 0 and world == 1 and not args.no_explicit_grm:
         line["explicit_grm"] = explicit_grm_block(cs, local, args.grm_n, args.grm_m,
                                                   args.grm_reps)

@@ -888,31 +888,46 @@ static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
 // ---- ring-shape autotuner ----------------------------------------------------
 // The ring shape (sub-stages per load stage, load-ring depth, TMEM operand slots)
 // does not change a product's result — the sums are exact integers and the epilogue
-// is per element — only its speed.  The first launch of each (pass, ng, grid, nk)
-// in the process times every shape that fits (sub 4, 2, 1 with the deepest ring the
-// shared memory holds) on the real operands and keeps the fastest; later launches of
-// the same key use it.  SAIGE_TC_AUTOTUNE=0 keeps the fixed choice of tc_rings.
+// is per element — only its speed.  The first launch of each key — pass, ng and the
+// launch's size class (log2 of its 4 KB stages) — in the process times every shape that
+// fits (sub 4, 2, 1 with the deepest ring the shared memory holds) on the real operands
+// and keeps the fastest; later launches of the key use it.  Launches of fewer than
+// kTuneMinStages stages keep the fixed choice of tc_rings (their trials would cost more
+// than they can save), as does SAIGE_TC_AUTOTUNE=0 (=2 tunes every size).  SAIGE_TIMING=1
+// logs each trial.
 namespace {
 
 struct TuneKey {
-  int dev, pass_b, ng, nk;
-  unsigned grid;
+  int dev, pass_b, ng, size_class;
   bool operator<(const TuneKey& o) const {
     if (dev != o.dev) return dev < o.dev;
     if (pass_b != o.pass_b) return pass_b < o.pass_b;
     if (ng != o.ng) return ng < o.ng;
-    if (nk != o.nk) return nk < o.nk;
-    return grid < o.grid;
+    return size_class < o.size_class;
   }
 };
+
+constexpr double kTuneMinStages = 1 << 20;  // ~4 GB of code tiles per launch
+
+int size_class(double stages) {
+  int c = 0;
+  while (stages >= 2.0) {
+    stages *= 0.5;
+    ++c;
+  }
+  return c;
+}
 
 std::mutex g_tune_mu;
 std::map<TuneKey, Rings> g_tune;
 std::atomic<int64_t> g_tune_trials{0};
 
-bool autotune_on() {
+// SAIGE_TC_AUTOTUNE: 0 off, 2 every launch size, otherwise (default) launches of at
+// least kTuneMinStages stages.
+int autotune_level() {
   const char* e = getenv("SAIGE_TC_AUTOTUNE");
-  return !(e && e[0] == '0');
+  if (!e || !e[0]) return 1;
+  return e[0] == '0' ? 0 : (e[0] == '2' ? 2 : 1);
 }
 
 std::vector<Rings> tc_candidates(int ng, bool pass_b) {
@@ -937,14 +952,16 @@ std::vector<Rings> tc_candidates(int ng, bool pass_b) {
 template <bool kPassB>
 static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st) {
   const Rings fixed = tc_rings(a.ng, kPassB);
-  if (!autotune_on()) {
+  const double stages = (double)grid * (double)a.nk;
+  const int level = autotune_level();
+  if (level == 0 || (level == 1 && stages < kTuneMinStages)) {
     a.sub = fixed.sub;
     a.sl = fixed.sl;
     a.sa = fixed.sa;
     SG_CUDA(launch_tc<kPassB>(grid, a, st));
     return Status();
   }
-  const TuneKey key{dev, kPassB ? 1 : 0, a.ng, a.nk, grid};
+  const TuneKey key{dev, kPassB ? 1 : 0, a.ng, size_class(stages)};
   {
     std::lock_guard<std::mutex> lk(g_tune_mu);
     auto it = g_tune.find(key);
@@ -964,6 +981,8 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
   float best_ms = 0.f;
   bool have = false;
   Status st_out;
+  const char* tlog = getenv("SAIGE_TIMING");
+  const bool log = tlog && tlog[0] == '1';
   for (const Rings& g : cand) {
     a.sub = g.sub;
     a.sl = g.sl;
@@ -983,6 +1002,9 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     float ms = 0.f;
     cudaEventElapsedTime(&ms, e0, e1);
     g_tune_trials += 1;
+    if (log)
+      fprintf(stderr, "[saige tune] pass %c ng %d grid %u nk %d: sub %d sl %d -> %.3f ms\n",
+              kPassB ? 'B' : 'A', a.ng, grid, a.nk, g.sub, g.sl, ms);
     if (!have || ms < best_ms) {
       best = g;
       best_ms = ms;

@@ -132,7 +132,7 @@ def test_autotuned_ring_shapes_give_identical_products(monkeypatch):
     v = np.random.default_rng(3).standard_normal((37, n))
     monkeypatch.setenv("SAIGE_TC_AUTOTUNE", "0")
     fixed = cs.OnTheFlyGrm.from_bed(bed, n, m, g, af[g], precision=cs.PREC_MIXED).mat_vec(v)
-    monkeypatch.setenv("SAIGE_TC_AUTOTUNE", "1")
+    monkeypatch.setenv("SAIGE_TC_AUTOTUNE", "2")  # tune this small size too
     before = int(cs.api.LIB.saige_tc_autotune_trials())
     grm = cs.OnTheFlyGrm.from_bed(bed, n, m, g, af[g], precision=cs.PREC_MIXED)
     tuned = grm.mat_vec(v)      # tunes both passes of this key
