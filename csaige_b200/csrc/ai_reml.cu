@@ -91,13 +91,25 @@ Status coldots(Fit& f, const double* a, const double* b, int q, std::vector<doub
 }
 
 // PCG of Sigma = tau0 W^-1 + tau1 K on q columns of b into x (x0 optional).
+struct Extra {
+  const double* in = nullptr;
+  double* out = nullptr;
+  int n = 0;
+};
+
 Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const double tau[2],
-             const double* ax0 = nullptr, double* r_out = nullptr) {
+             const double* ax0 = nullptr, double* r_out = nullptr, double* kx = nullptr,
+             const double* kx0 = nullptr, bool* kx_valid = nullptr, Extra extra = Extra()) {
   PcgRun run;
   run.b = b;
   run.x0 = x0;
   run.ax0 = x0 ? ax0 : nullptr;
   run.r_out = r_out;
+  run.kx = kx;
+  run.kx0 = x0 ? kx0 : nullptr;
+  run.extra_in = extra.in;
+  run.extra_out = extra.out;
+  run.n_extra = extra.n;
   run.wv = f.wmax;
   run.d = f.d;
   run.tau0 = tau[0];
@@ -110,6 +122,7 @@ Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const 
   run.force_step = x0 != nullptr;
   SG_TRY(pcg_run(f.h, run, f.st));
   f.pcg_iters += run.total_iters;
+  if (kx_valid) *kx_valid = run.kx_valid;
   return Status();
 }
 
@@ -147,12 +160,14 @@ struct Recycle {
   int mb_max = 0, nk = 0;
   DevBuf mem;                           // one block (large blocks are cached)
   double *v, *av, *x0, *ax0, *br;       // basis, images (+ b), start, its image, block r
-  double *kin, *kout;                   // [Py | X*_t | pk' | pw'] and its K-image
+  double *kv, *kx0;                     // K-images of the basis columns and of the start
+  double *kblock, *kpk, *kpw;           // K X* of the latest block solve, K of the AI solutions
+  double *kin, *kout;                   // [Py | X*_t | pk' | pw' (| learned)] and its K-image
   double *gam, *gpart, *gout;
-  bool have_ksol = false;               // kout holds K X*_t of the previous iteration
-  bool have_kpk = false, have_kpw = false;  // K of the previous AI solutions is in kout
-  int at_pk = 0, at_pw = 0;                  // their columns in kout
-  int64_t fallbacks = 0;
+  bool have_kblock = false, have_kpk = false, have_kpw = false;
+  bool kv_ok = true;                    // every basis column of the current start has kv
+  bool with_pw = false;                 // the fit has the W^-1 AI solve (quantitative)
+  int64_t fallbacks = 0, kpy_launches_saved = 0;
   // learned correction (SAIGE_WARM_LEARNED): an MLP trained on the change of the
   // block solutions between iterations predicts the next change; the prediction joins
   // the next block basis, its K-image from the K Py launch
@@ -193,7 +208,7 @@ Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint
     SG_TRY(mlp_init(rc.mlp, seed, f.st));
   }
   const size_t mb = (size_t)rc.mb_max, nk = (size_t)rc.nk;
-  const size_t ncol = mb + (mb + q) + 3 * q + 2 * nk;
+  const size_t ncol = mb + (mb + q) + 3 * q + 2 * nk + mb + q + q + 2;
   const size_t nsmall = mb * q + gram_partial_doubles(f.n, (int)mb, (int)(mb + q)) + mb * (mb + q);
   SG_TRY(rc.mem.reserve((ncol * ld + nsmall) * 8));
   double* b = rc.mem.as<double>();
@@ -205,6 +220,11 @@ Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint
   rc.br = b;                b += q * ld;
   rc.kin = b;               b += nk * ld;
   rc.kout = b;              b += nk * ld;
+  rc.kv = b;                b += mb * ld;
+  rc.kx0 = b;               b += q * ld;
+  rc.kblock = b;            b += q * ld;
+  rc.kpk = b;               b += ld;
+  rc.kpw = b;               b += ld;
   rc.gam = b;               b += mb * q;
   rc.gout = b;              b += mb * (mb + q);
   rc.gpart = b;
@@ -267,6 +287,7 @@ Status galerkin_start(Fit& f, Recycle& rc, int mb, int q, bool& ok) {
   SG_CUDA(cudaMemcpyAsync(rc.gam, gam.data(), gam.size() * 8, cudaMemcpyHostToDevice, f.st));
   SG_CUDA(combo(rc.v, mb, rc.gam, q, rc.x0, false, f.n, ld, f.st));
   SG_CUDA(combo(rc.av, mb, rc.gam, q, rc.ax0, false, f.n, ld, f.st));
+  if (rc.kv_ok) SG_CUDA(combo(rc.kv, mb, rc.gam, q, rc.kx0, false, f.n, ld, f.st));
   return Status();
 }
 
@@ -276,20 +297,24 @@ Status basis_cols(Fit& f, Recycle& rc, int at, const double* x, const double* kx
                   const double tau[2]) {
   const int64_t ld = f.ld;
   SG_TRY(copy_cols(f, x, rc.v + (size_t)at * ld, k));
+  SG_TRY(copy_cols(f, kx, rc.kv + (size_t)at * ld, k));
   SG_CUDA(sigma_image(x, kx, f.wmax, tau[0], tau[1], rc.av + (size_t)at * ld, f.n, ld, k, f.st));
   return Status();
 }
 
 // The block solve of one iteration from the recycled start: basis [X | U] and the
-// previous iteration's block solutions (f.sol on entry).  Leaves the final residual
-// in rc.br.
-Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const double tau[2]) {
+// previous iteration's block solutions (f.sol on entry, K-image rc.kblock).  Leaves the
+// final residual in rc.br and K X*_t in rc.kblock; kx_ok tells whether that K-image was
+// formed (false when the iteration has tau1 = 0, whose solve forms no product).
+Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const double tau[2],
+                            bool& kx_ok) {
   const int64_t ld = f.ld;
   int mb = 0;
+  rc.kv_ok = true;
   SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
   mb += f.p + f.nrv;
-  if (rc.have_ksol) {
-    SG_TRY(basis_cols(f, rc, mb, f.sol, rc.kout + ld, f.q, tau));
+  if (rc.have_kblock) {
+    SG_TRY(basis_cols(f, rc, mb, f.sol, rc.kblock, f.q, tau));
     mb += f.q;
   }
   if (rc.have_delta) {
@@ -301,8 +326,23 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
   SG_TRY(copy_cols(f, f.rhs, rc.av + (size_t)mb * ld, f.q));
   bool ok = false;
   SG_TRY(galerkin_start(f, rc, mb, f.q, ok));
-  if (ok) return solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br);
-  return solve(f, f.rhs, f.sol, x0_prev, f.q, tau, nullptr, rc.br);
+  kx_ok = false;
+  // the previous AI solutions whose K-image is missing (their solve had tau1 = 0) ride
+  // in the first product of this solve, for this iteration's AI starts
+  Extra ex;
+  if (!rc.learned && tau[1] != 0.0) {
+    const bool need_pk = f.have_prev_pk && !rc.have_kpk;
+    const bool need_pw = rc.with_pw && f.have_prev_pw && !rc.have_kpw;
+    if (need_pk && need_pw) ex = Extra{f.pk_raw, rc.kpk, 2};  // adjacent columns
+    else if (need_pk) ex = Extra{f.pk_raw, rc.kpk, 1};
+    else if (need_pw) ex = Extra{f.pw_raw, rc.kpw, 1};
+    if (need_pk) rc.have_kpk = true;
+    if (need_pw) rc.have_kpw = true;
+  }
+  if (ok)
+    return solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br, rc.kblock, rc.kx0, &kx_ok, ex);
+  return solve(f, f.rhs, f.sol, x0_prev, f.q, tau, nullptr, rc.br, rc.kblock, nullptr, &kx_ok,
+               ex);
 }
 
 // K Py, and in the same launch K X*_t (this iteration's block solutions, for the next
@@ -323,11 +363,22 @@ Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw, int trait,
   if (rc.learned) SG_TRY(learn_step(f, rc, trait, tau, k));
   SG_TRY(grm_product(f.h, rc.kin, rc.kout, k, nullptr, f.cfg->precision, f.st));
   SG_TRY(copy_cols(f, rc.kout, f.kpy, 1));
-  rc.have_ksol = true;
+  SG_TRY(copy_cols(f, rc.kout + ld, rc.kblock, f.q));
+  rc.have_kblock = true;
+  if (with_pk) SG_TRY(copy_cols(f, rc.kout + (size_t)at_pk * ld, rc.kpk, 1));
+  if (with_pw) SG_TRY(copy_cols(f, rc.kout + (size_t)at_pw * ld, rc.kpw, 1));
   rc.have_kpk = with_pk;
   rc.have_kpw = with_pw;
-  rc.at_pk = at_pk;
-  rc.at_pw = at_pw;
+  return Status();
+}
+
+// K Py without a product: the block solve kept K X*_t beside X*_t, so
+// K Py = K (Sinv y - Sinv X alpha) = kblock[:, 0] - kblock[:, 1..p] alpha (alpha on the
+// device in f.dsmall, as for Py).
+Status kpy_from_block(Fit& f, Recycle& rc) {
+  SG_TRY(copy_cols(f, rc.kblock, f.kpy, 1));
+  SG_CUDA(sub_combo(f.kpy, 1, rc.kblock + f.ld, f.p, f.dsmall, f.n, f.ld, f.st));
+  ++rc.kpy_launches_saved;
   return Status();
 }
 
@@ -395,27 +446,37 @@ Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k) {
 }
 
 // One AI solve Sigma x = b (one column) from a recycled start over this iteration's
-// block solutions (image b_block - r_block), [X | U] and the previous solution of the
-// same system (x on entry, K-image at kprev when have).
-Status ai_solve_recycled(Fit& f, Recycle& rc, const double* b, double* x, const double* kprev,
-                         bool have, const double tau[2]) {
+// block solutions (image b_block - r_block, K-image rc.kblock), [X | U] and the previous
+// solution of the same system (x on entry, K-image kx when have).  K of the new
+// solution is kept in kx; have tells on return whether it was formed.
+Status ai_solve_recycled(Fit& f, Recycle& rc, const double* b, double* x, double* kx, bool& have,
+                         const double tau[2]) {
   const int64_t ld = f.ld;
   int mb = 0;
+  rc.kv_ok = rc.have_kblock;
   SG_TRY(copy_cols(f, f.sol, rc.v, f.q));
+  SG_TRY(copy_cols(f, rc.kblock, rc.kv, f.q));
   SG_CUDA(sub_cols(f.rhs, rc.br, rc.av, f.n, ld, f.q, f.st));
   mb += f.q;
   SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
   mb += f.p + f.nrv;
   if (have) {
-    SG_TRY(basis_cols(f, rc, mb, x, kprev, 1, tau));
+    SG_TRY(basis_cols(f, rc, mb, x, kx, 1, tau));
     mb += 1;
   }
   SG_TRY(copy_cols(f, b, rc.av + (size_t)mb * ld, 1));
   bool ok = false;
   SG_TRY(galerkin_start(f, rc, mb, 1, ok));
-  if (ok) return solve(f, b, x, rc.x0, 1, tau, rc.ax0, nullptr);
-  if (have) SG_TRY(copy_cols(f, x, rc.x0, 1));
-  return solve(f, b, x, have ? rc.x0 : nullptr, 1, tau);
+  bool kx_ok = false;
+  if (ok) {
+    SG_TRY(solve(f, b, x, rc.x0, 1, tau, rc.ax0, nullptr, kx, rc.kv_ok ? rc.kx0 : nullptr,
+                 &kx_ok));
+  } else {
+    if (have) SG_TRY(copy_cols(f, x, rc.x0, 1));
+    SG_TRY(solve(f, b, x, have ? rc.x0 : nullptr, 1, tau, nullptr, nullptr, kx, nullptr, &kx_ok));
+  }
+  have = kx_ok;
+  return Status();
 }
 
 }  // namespace
@@ -584,6 +645,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   const double* pre_diag = cfg->precond == SAIGE_PRECOND_DIAG_K ? diagk.as<double>() : nullptr;
   Recycle rc;
   if (recyc) SG_TRY(recycle_init(f, rc, learned, diagk.as<double>(), cfg->seed));
+  rc.with_pw = !(trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL);
 
   const bool fix_tau_e = trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL;
   double tau[2] = {1.0, 0.0};
@@ -603,8 +665,9 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     if (warm && f.have_prev)
       SG_CUDA(cudaMemcpyAsync(prev.ptr, f.sol, (size_t)ld * f.q * 8, cudaMemcpyDeviceToDevice, f.st));
     const double* x0 = (warm && f.have_prev) ? prev.as<double>() : nullptr;
+    bool block_kx = false;
     if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
-      SG_TRY(block_solve_recycled(f, rc, x0, tau));
+      SG_TRY(block_solve_recycled(f, rc, x0, tau, block_kx));
     } else if (cfg->solve == SAIGE_SOLVE_BLOCK) {
       SG_TRY(solve(f, f.rhs, f.sol, x0, f.q, tau));
     } else {
@@ -635,9 +698,11 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     // P y = Sinv y - SinvX alpha; YPAPY = Py' K Py (ai_reml.rs:221-232)
     SG_TRY(copy_cols(f, SinvY, f.py, 1));
     SG_CUDA(sub_combo(f.py, 1, SinvX, p, f.dsmall, n, ld, f.st));
-    if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK)
+    if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK && block_kx && !rc.learned) {
+      SG_TRY(kpy_from_block(f, rc));  // K X*_t and K Py without a launch
+    } else if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
       SG_TRY(kpy_recycled(f, rc, f.have_prev_pk, !fix_tau_e && f.have_prev_pw, trait, tau));
-    else
+    } else
       SG_TRY(grm_product(h, f.py, f.kpy, 1, nullptr, cfg->precision, f.st));
     tm.mark("  kpy");
     std::vector<double> r1;
@@ -657,8 +722,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     // AI = (K P y)' P (K P y) (ai_reml.rs:263-273)
     // warm start from the previous iteration's unprojected solution
     if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
-      SG_TRY(ai_solve_recycled(f, rc, f.kpy, f.pk_raw, rc.kout + (size_t)rc.at_pk * ld,
-                               rc.have_kpk, tau));
+      SG_TRY(ai_solve_recycled(f, rc, f.kpy, f.pk_raw, rc.kpk, rc.have_kpk, tau));
     } else {
       if (warm && f.have_prev_pk) SG_TRY(copy_cols(f, f.pk_raw, f.pw, 1));
       SG_TRY(solve(f, f.kpy, f.pk_raw, (warm && f.have_prev_pk) ? f.pw : nullptr, 1, tau));
@@ -683,8 +747,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
       SG_TRY(coldots(f, f.py, f.invw_py, 1, r1));
       score_e = r1[0] - trace_w;
       if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
-        SG_TRY(ai_solve_recycled(f, rc, f.invw_py, f.pw_raw, rc.kout + (size_t)rc.at_pw * ld,
-                                 rc.have_kpw, tau));
+        SG_TRY(ai_solve_recycled(f, rc, f.invw_py, f.pw_raw, rc.kpw, rc.have_kpw, tau));
       } else {
         if (warm && f.have_prev_pw) SG_TRY(copy_cols(f, f.pw_raw, f.tmpq, 1));
         SG_TRY(solve(f, f.invw_py, f.pw_raw, (warm && f.have_prev_pw) ? f.tmpq : nullptr, 1, tau));

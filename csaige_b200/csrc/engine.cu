@@ -399,8 +399,10 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
   const int q = run.q;
   const int64_t n = h->n, ld = h->n_pad;
   PcgScratch s;
-  SG_TRY(pcg_scratch(h, q, s));
+  const int ne = run.extra_in && run.extra_out ? run.n_extra : 0;
+  SG_TRY(pcg_scratch(h, q + ne, s));  // room for the extra columns in p and kp
   std::vector<int32_t> state((size_t)q, kColActive);
+  bool extra_done = ne == 0;
   // With tau1 = 0 the operator is tau0 W^-1 (or tau0 W): tau1 K v contributes only
   // zeros, so no GRM product is formed and K v reads as 0.
   const bool no_k = run.tau1 == 0.0;
@@ -410,6 +412,9 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
     // r = b - A x0 (decomposition.rs:225-227)
     SG_CUDA(cudaMemsetAsync(s.cols.state, 0, (size_t)q * sizeof(int32_t), st));
     if (!no_k) SG_TRY(grm_product(h, run.x0, s.kp, q, nullptr, run.precision, st));
+    if (run.kx && !no_k)
+      SG_CUDA(cudaMemcpyAsync(run.kx, s.kp, (size_t)ld * q * sizeof(double),
+                              cudaMemcpyDeviceToDevice, st));
     if (run.w_inverse)
       SG_CUDA(pcg_apply(run.x0, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
                         s.partial, st));
@@ -418,6 +423,14 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
                           s.partial, st));
     ax0 = s.ap;
   }
+  if (run.kx && !(run.x0 && !run.ax0)) {
+    if (run.x0 && run.kx0)
+      SG_CUDA(cudaMemcpyAsync(run.kx, run.kx0, (size_t)ld * q * sizeof(double),
+                              cudaMemcpyDeviceToDevice, st));
+    else
+      SG_CUDA(cudaMemsetAsync(run.kx, 0, (size_t)ld * q * sizeof(double), st));
+  }
+  run.kx_valid = run.kx && !no_k && (!run.x0 || !run.ax0 || run.kx0);
   SG_CUDA(pcg_start(run.b, run.x0, ax0, run.d, run.x, s.r, s.z, s.p, n, ld, q, run.tol,
                     run.force_step && run.x0 != nullptr, s.cols, s.partial, s.small, st));
   if (run.max_iter <= 0) {
@@ -432,7 +445,19 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
       bool any = false;
       for (int c = 0; c < q; ++c) any |= state[(size_t)c] == kColActive;
       if (!any) break;
-      if (!no_k) SG_TRY(grm_product(h, s.p, s.kp, q, state.data(), run.precision, st));
+      if (!no_k && !extra_done) {
+        // the extra columns ride in this launch
+        SG_CUDA(cudaMemcpyAsync(s.p + (size_t)q * ld, run.extra_in, (size_t)ld * ne * sizeof(double),
+                                cudaMemcpyDeviceToDevice, st));
+        std::vector<int32_t> st2 = state;
+        st2.resize((size_t)(q + ne), kColActive);
+        SG_TRY(grm_product(h, s.p, s.kp, q + ne, st2.data(), run.precision, st));
+        SG_CUDA(cudaMemcpyAsync(run.extra_out, s.kp + (size_t)q * ld, (size_t)ld * ne * sizeof(double),
+                                cudaMemcpyDeviceToDevice, st));
+        extra_done = true;
+      } else if (!no_k) {
+        SG_TRY(grm_product(h, s.p, s.kp, q, state.data(), run.precision, st));
+      }
       if (run.w_inverse)
         SG_CUDA(pcg_apply(s.p, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
                           s.partial, st));
@@ -440,9 +465,11 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
         SG_CUDA(pcg_apply_w(s.p, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
                             s.partial, st));
       SG_CUDA(pcg_step(run.x, s.r, s.z, s.p, s.ap, run.d, n, ld, q, run.max_iter, s.cols,
-                       s.partial, s.small, st));
+                       s.partial, s.small, st, run.kx_valid ? run.kx : nullptr, s.kp));
     }
   }
+  if (!extra_done)
+    SG_TRY(grm_product(h, run.extra_in, run.extra_out, ne, nullptr, run.precision, st));
   if (run.r_out)
     SG_CUDA(cudaMemcpyAsync(run.r_out, s.r, (size_t)ld * q * sizeof(double),
                             cudaMemcpyDeviceToDevice, st));

@@ -103,6 +103,16 @@ struct PcgRun {
   // outputs
   double* x = nullptr;         // device n_pad x q
   double* r_out = nullptr;     // optional: the final residual b - Sigma x (device n_pad x q)
+  // optional: K x kept beside x from the products K p (device n_pad x q); kx0 = K x0
+  // when x0 and ax0 are given.  kx_valid is false when no product was formed (tau1 = 0).
+  double* kx = nullptr;
+  const double* kx0 = nullptr;
+  bool kx_valid = false;
+  // optional: n_extra more columns (device, ld apart) multiplied by K in the solve's
+  // first product launch, the product into extra_out; a separate launch when none runs
+  const double* extra_in = nullptr;
+  double* extra_out = nullptr;
+  int n_extra = 0;
   std::vector<int32_t> iters, state;
   std::vector<double> resid;
   int64_t total_iters = 0;

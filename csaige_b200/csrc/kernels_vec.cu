@@ -176,7 +176,8 @@ __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r
                                   double* __restrict__ z, const double* __restrict__ p,
                                   const double* __restrict__ ap, const double* __restrict__ d,
                                   int64_t n, int64_t ld, PcgCols cols,
-                                  double* __restrict__ partial) {
+                                  double* __restrict__ partial, double* __restrict__ kx,
+                                  const double* __restrict__ kp) {
   __shared__ double sh[kT / 32];
   const int c = blockIdx.y;
   if (cols.state[c] != kColActive) return;
@@ -188,6 +189,7 @@ __global__ void pcg_update_kernel(double* __restrict__ x, double* __restrict__ r
   double s_rz = 0.0, s_rr = 0.0;
   for (int64_t i = lo + threadIdx.x; i < hi; i += kT) {
     x[off + i] += alpha * p[off + i];
+    if (kx) kx[off + i] += alpha * kp[off + i];  // K x follows x: K x += alpha K p
     const double ri = r[off + i] - alpha * ap[off + i];
     r[off + i] = ri;
     const double zi = ri / d[i];
@@ -447,9 +449,9 @@ cudaError_t pcg_apply_w(const double* p, const double* kp, const double* w, doub
 
 cudaError_t pcg_step(double* x, double* r, double* z, double* p, const double* ap,
                      const double* d, int64_t n, int64_t ld, int q, int max_iter, PcgCols cols,
-                     double* partial, double* scratch2q, cudaStream_t st) {
+                     double* partial, double* scratch2q, cudaStream_t st, double* kx, const double* kp) {
   const int nb = red_blocks(n);
-  pcg_update_kernel<<<dim3(nb, q), kT, 0, st>>>(x, r, z, p, ap, d, n, ld, cols, partial);
+  pcg_update_kernel<<<dim3(nb, q), kT, 0, st>>>(x, r, z, p, ap, d, n, ld, cols, partial, kx, kp);
   pcg_update_finish<<<(unsigned)ceil_div(q, 8), 256, 0, st>>>(partial, nb, q, max_iter, cols,
                                                               scratch2q);
   unsigned gx = (unsigned)ceil_div(n, kT);

@@ -47,10 +47,12 @@ cudaError_t pcg_apply(const double* p, const double* kp, const double* wmax, dou
 cudaError_t pcg_apply_w(const double* p, const double* kp, const double* w, double tau0,
                         double tau1, double* ap, int64_t n, int64_t ld, int q, PcgCols cols,
                         double* partial, cudaStream_t st);
-// x += alpha p, r -= alpha ap, z = r / d, then beta, ||r|| test, p = z + beta p.
+// x += alpha p, r -= alpha ap, z = r / d, then beta, ||r|| test, p = z + beta p;
+// with kx, also kx += alpha kp (K x kept beside x from the products K p).
 cudaError_t pcg_step(double* x, double* r, double* z, double* p, const double* ap,
                      const double* d, int64_t n, int64_t ld, int q, int max_iter, PcgCols cols,
-                     double* partial, double* scratch2q, cudaStream_t st);
+                     double* partial, double* scratch2q, cudaStream_t st, double* kx = nullptr,
+                     const double* kp = nullptr);
 
 // Elementwise helpers for the AI-REML loop.
 // Jacobi diagonal of fit-null: wmax = max(w,1e-30), d = tau0/wmax + tau1 (1 when |d| <= 1e-30);
