@@ -160,6 +160,8 @@ class GrmStatsC(C.Structure):
         ("tc_pass_b_ms", C.c_double),
         ("fp32_launches", C.c_int64),
         ("fp32_ms", C.c_double),
+        ("sc_launches", C.c_int64),
+        ("sc_ms", C.c_double),
     ]
 
 

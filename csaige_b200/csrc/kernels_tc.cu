@@ -736,6 +736,249 @@ __global__ void __launch_bounds__(128)
   }
 }
 
+// ---------------------------------------------------------------------------
+// Single-column products on the CUDA cores.  With one column the tensor-core
+// passes are bound by their fixed per-stage cost (eight MMAs and the unpack of a
+// 4 KB code tile for three limb columns), so one column costs nearly what 42 do.
+// These kernels form the same exact integer sums with dp4a — the limbs of q as
+// int8 planes, genotypes and missing flags expanded four at a time by byte
+// permutes — and apply the same FP64 epilogue, so their results are bit-identical
+// to the tensor-core path's.
+// ---------------------------------------------------------------------------
+// byte_perm tables indexed by the 2-bit code: genotype (00 -> 2, 01 -> 0 (missing),
+// 10 -> 1, 11 -> 0) and missing flag (01 -> 1)
+constexpr uint32_t kLutGeno = 0x00010002u;
+constexpr uint32_t kLutMiss = 0x00000100u;
+constexpr int kSrWarpMarkers = 8;                        // pass A: markers per warp
+constexpr int kSrBlockMarkers = 8 * kSrWarpMarkers;      // pass A: markers per block
+constexpr int kSrWords = 256;                            // pass A: sample words staged per round
+constexpr int kSrChunk = 2048;  // markers of limb planes staged per pass-B round
+
+// The four 4-entry groups of a packed word (device layout: entry 4j+i at bit
+// 16(j>>1) + 2(j&1) + 4i) as byte-permute selectors; group g = entries 4g..4g+3.
+__device__ __forceinline__ void sr_selectors(uint32_t w, uint32_t sel[4]) {
+  sel[0] = w & 0x3333u;
+  sel[1] = (w >> 2) & 0x3333u;
+  sel[2] = (w >> 16) & 0x3333u;
+  sel[3] = (w >> 18) & 0x3333u;
+}
+
+// q = rint(x / scale) as in quant_v_kernel, into three int8 planes (l2, l1, l0) of
+// length n_pad (zero past len), and sum q.
+__global__ void __launch_bounds__(256)
+    sr_quant_v_kernel(const double* __restrict__ v, int64_t len, int64_t n_pad,
+                      const unsigned long long* __restrict__ amax, double* __restrict__ scale_out,
+                      int8_t* __restrict__ planes, unsigned long long* __restrict__ sum_q) {
+  __shared__ long long sh[8];
+  const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  const double sc = scale_of(amax[0]);
+  long long q = 0;
+  if (i < n_pad) {
+    const double x = i < len ? v[i] : 0.0;
+    q = __double2ll_rn(x / sc);
+    int l2, l1, l0;
+    limbs(q, l2, l1, l0);
+    planes[i] = (int8_t)l2;
+    planes[n_pad + i] = (int8_t)l1;
+    planes[2 * n_pad + i] = (int8_t)l0;
+  }
+  long long t = q;
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int k = 0; k < 8; ++k) s += sh[k];
+    atomicAdd(sum_q, (unsigned long long)s);
+    if (blockIdx.x == 0) scale_out[0] = sc;
+  }
+}
+
+// w = u inv_s, c = w 2p quantised as in quant_wc_kernel into planes (w: l2 l1 l0,
+// c: l2 l1 l0; length m_pad each), and sum qc.
+__global__ void __launch_bounds__(256)
+    sr_quant_wc_kernel(const double* __restrict__ u, int64_t m_pad,
+                       const double* __restrict__ inv_s, const double* __restrict__ two_p,
+                       const unsigned long long* __restrict__ amax_w,
+                       const unsigned long long* __restrict__ amax_c, double* __restrict__ scale_w,
+                       double* __restrict__ scale_c, int8_t* __restrict__ planes,
+                       unsigned long long* __restrict__ sum_c) {
+  __shared__ long long sh[8];
+  const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
+  const double sw = scale_of(amax_w[0]), scc = scale_of(amax_c[0]);
+  long long qc = 0;
+  if (m < m_pad) {
+    const double w = u[m] * inv_s[m];
+    const double c = w * two_p[m];
+    const long long qw = __double2ll_rn(w / sw);
+    qc = __double2ll_rn(c / scc);
+    int l2, l1, l0;
+    limbs(qw, l2, l1, l0);
+    planes[m] = (int8_t)l2;
+    planes[m_pad + m] = (int8_t)l1;
+    planes[2 * m_pad + m] = (int8_t)l0;
+    limbs(qc, l2, l1, l0);
+    planes[3 * m_pad + m] = (int8_t)l2;
+    planes[4 * m_pad + m] = (int8_t)l1;
+    planes[5 * m_pad + m] = (int8_t)l0;
+  }
+  long long t = qc;
+  for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = t;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    long long s = 0;
+    for (int k = 0; k < 8; ++k) s += sh[k];
+    atomicAdd(sum_c, (unsigned long long)s);
+    if (blockIdx.x == 0) {
+      scale_w[0] = sw;
+      scale_c[0] = scc;
+    }
+  }
+}
+
+// Pass A of one column: block = 64 markers x all samples, warp = 8 markers.  The
+// limb planes of q are staged in shared memory kSrWords words (16 samples each) at a
+// time and shared by the block's warps; each lane keeps the six sums of its warp's 8
+// markers over its words, and the warp's sums are finished as in the tensor-core
+// epilogue.
+__global__ void __launch_bounds__(256, 2)
+    sr_pass_a_kernel(const uint32_t* __restrict__ geno, int64_t wpr,
+                     const int8_t* __restrict__ planes, int64_t n_pad,
+                     const unsigned long long* __restrict__ sum_q,
+                     const double* __restrict__ scale_v, const double* __restrict__ two_p,
+                     const double* __restrict__ inv_s, double* __restrict__ u) {
+  __shared__ uint4 sp[3][kSrWords];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t m0 = (int64_t)blockIdx.x * kSrBlockMarkers + warp * kSrWarpMarkers;
+  const uint32_t* rows = geno + m0 * wpr;
+  int acc[kSrWarpMarkers][6];
+#pragma unroll
+  for (int k = 0; k < kSrWarpMarkers; ++k)
+#pragma unroll
+    for (int j = 0; j < 6; ++j) acc[k][j] = 0;
+  const int64_t n_words = n_pad / 16;
+  for (int64_t c0 = 0; c0 < n_words; c0 += kSrWords) {
+    const int cn = n_words - c0 < kSrWords ? (int)(n_words - c0) : kSrWords;
+    __syncthreads();
+    for (int t = threadIdx.x; t < 3 * kSrWords; t += 256) {
+      const int pl = t / kSrWords, k = t % kSrWords;
+      sp[pl][k] = k < cn ? __ldg(reinterpret_cast<const uint4*>(planes + pl * n_pad) + c0 + k)
+                         : make_uint4(0u, 0u, 0u, 0u);
+    }
+    __syncthreads();
+    for (int t = lane; t < cn; t += 32) {
+      uint32_t w[kSrWarpMarkers];
+#pragma unroll
+      for (int k = 0; k < kSrWarpMarkers; ++k) w[k] = __ldg(rows + k * wpr + c0 + t);
+      const uint4 a2 = sp[0][t], a1 = sp[1][t], a0 = sp[2][t];
+      const int l2[4] = {(int)a2.x, (int)a2.y, (int)a2.z, (int)a2.w};
+      const int l1[4] = {(int)a1.x, (int)a1.y, (int)a1.z, (int)a1.w};
+      const int l0[4] = {(int)a0.x, (int)a0.y, (int)a0.z, (int)a0.w};
+#pragma unroll
+      for (int k = 0; k < kSrWarpMarkers; ++k) {
+        uint32_t sel[4];
+        sr_selectors(w[k], sel);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int gb = (int)__byte_perm(kLutGeno, 0u, sel[g]);
+          const int mb = (int)__byte_perm(kLutMiss, 0u, sel[g]);
+          acc[k][0] = __dp4a(gb, l2[g], acc[k][0]);
+          acc[k][1] = __dp4a(gb, l1[g], acc[k][1]);
+          acc[k][2] = __dp4a(gb, l0[g], acc[k][2]);
+          acc[k][3] = __dp4a(mb, l2[g], acc[k][3]);
+          acc[k][4] = __dp4a(mb, l1[g], acc[k][4]);
+          acc[k][5] = __dp4a(mb, l0[g], acc[k][5]);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kSrWarpMarkers; ++k)
+#pragma unroll
+    for (int j = 0; j < 6; ++j)
+      for (int o = 16; o > 0; o >>= 1) acc[k][j] += __shfl_xor_sync(0xffffffffu, acc[k][j], o);
+  const double S = (double)(long long)sum_q[0];
+#pragma unroll
+  for (int k = 0; k < kSrWarpMarkers; ++k) {
+    if (lane != k) continue;
+    const int64_t m = m0 + k;
+    const double G = 65536.0 * (double)acc[k][0] + 256.0 * (double)acc[k][1] + (double)acc[k][2];
+    const double Mi = 65536.0 * (double)acc[k][3] + 256.0 * (double)acc[k][4] + (double)acc[k][5];
+    const double tt = __dsub_rn(G, __dmul_rn(two_p[m], S - Mi));
+    u[m] = __dmul_rn(inv_s[m], __dmul_rn(scale_v[0], tt));
+  }
+}
+
+// Pass B of one column: block = one 128-sample tile of tiles_s, thread = sample.  The
+// marker limb planes are staged in shared memory kSrChunk markers at a time.
+__global__ void __launch_bounds__(128)
+    sr_pass_b_kernel(const uint8_t* __restrict__ tiles_s, int64_t n_mt,
+                     const int8_t* __restrict__ planes, int64_t m_pad,
+                     const unsigned long long* __restrict__ sum_c,
+                     const double* __restrict__ scale_w, const double* __restrict__ scale_c,
+                     double out_scale, double* __restrict__ out) {
+  __shared__ __align__(16) int8_t sp[6][kSrChunk];
+  const int64_t st = blockIdx.x;
+  const int r = threadIdx.x;
+  int acc[6] = {0, 0, 0, 0, 0, 0};
+  for (int64_t mt0 = 0; mt0 < n_mt; mt0 += kSrChunk / 128) {
+    const int64_t base = mt0 * 128;
+    const int64_t len = m_pad - base < kSrChunk ? m_pad - base : (int64_t)kSrChunk;
+    __syncthreads();
+    for (int t = threadIdx.x; t < 6 * (kSrChunk / 16); t += 128) {
+      const int pl = t / (kSrChunk / 16), k = t % (kSrChunk / 16);
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (16 * k < len)
+        v = __ldg(reinterpret_cast<const uint4*>(planes + (int64_t)pl * m_pad + base) + k);
+      reinterpret_cast<uint4*>(sp[pl])[k] = v;
+    }
+    __syncthreads();
+    const int64_t mt_end = mt0 + kSrChunk / 128 < n_mt ? mt0 + kSrChunk / 128 : n_mt;
+    for (int64_t mt = mt0; mt < mt_end; ++mt) {
+      const uint4* row = reinterpret_cast<const uint4*>(tiles_s + (st * n_mt + mt) * kTileBytes +
+                                                        (int64_t)r * 32);
+      const uint4 h0 = __ldg(row), h1 = __ldg(row + 1);
+      const uint32_t words[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+      const int off = (int)(mt - mt0) * 128;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        uint32_t sel[4];
+        sr_selectors(words[j], sel);
+        const int mk = off + 16 * j;
+        const uint4 w2 = *reinterpret_cast<const uint4*>(sp[0] + mk);
+        const uint4 w1 = *reinterpret_cast<const uint4*>(sp[1] + mk);
+        const uint4 w0 = *reinterpret_cast<const uint4*>(sp[2] + mk);
+        const uint4 c2 = *reinterpret_cast<const uint4*>(sp[3] + mk);
+        const uint4 c1 = *reinterpret_cast<const uint4*>(sp[4] + mk);
+        const uint4 c0 = *reinterpret_cast<const uint4*>(sp[5] + mk);
+        const int W2[4] = {(int)w2.x, (int)w2.y, (int)w2.z, (int)w2.w};
+        const int W1[4] = {(int)w1.x, (int)w1.y, (int)w1.z, (int)w1.w};
+        const int W0[4] = {(int)w0.x, (int)w0.y, (int)w0.z, (int)w0.w};
+        const int C2[4] = {(int)c2.x, (int)c2.y, (int)c2.z, (int)c2.w};
+        const int C1[4] = {(int)c1.x, (int)c1.y, (int)c1.z, (int)c1.w};
+        const int C0[4] = {(int)c0.x, (int)c0.y, (int)c0.z, (int)c0.w};
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int gb = (int)__byte_perm(kLutGeno, 0u, sel[g]);
+          const int mb = (int)__byte_perm(kLutMiss, 0u, sel[g]);
+          acc[0] = __dp4a(gb, W2[g], acc[0]);
+          acc[1] = __dp4a(gb, W1[g], acc[1]);
+          acc[2] = __dp4a(gb, W0[g], acc[2]);
+          acc[3] = __dp4a(mb, C2[g], acc[3]);
+          acc[4] = __dp4a(mb, C1[g], acc[4]);
+          acc[5] = __dp4a(mb, C0[g], acc[5]);
+        }
+      }
+    }
+  }
+  const double G = 65536.0 * (double)acc[0] + 256.0 * (double)acc[1] + (double)acc[2];
+  const double Mi = 65536.0 * (double)acc[3] + 256.0 * (double)acc[4] + (double)acc[5];
+  const double S = (double)(long long)sum_c[0];
+  out[st * 128 + r] =
+      __dmul_rn(out_scale, __dsub_rn(__dmul_rn(scale_w[0], G), __dmul_rn(scale_c[0], S - Mi)));
+}
+
 size_t tc_fixed_bytes() { return 1024 + 8 * (2 * kMaxSL + kMaxSA + 1) + 16; }
 
 struct Rings {
@@ -1070,8 +1313,42 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     SG_CUDA(cudaEventRecord(*e, st));
     return Status();
   };
-  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_a, ev_b;
-  for (size_t c0 = 0; c0 < cols.size(); c0 += kMaxR) {
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_a, ev_b, ev_s;
+  const char* sc_env = getenv("SAIGE_SC");
+  const bool single = cols.size() == 1 && !(sc_env && sc_env[0] == '0');
+  if (single) {
+    // one column: both passes on the CUDA cores (same integer sums, same epilogue)
+    int8_t* planes_a = p->img_a.as<int8_t>();  // 3 x n_pad limb planes of q
+    int8_t* planes_b = p->img_w.as<int8_t>();  // 6 x m_pad limb planes of qw, qc
+    double* u = p->u.as<double>();
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    SG_TRY(mark(&t0));
+    SG_CUDA(cudaMemsetAsync(p->scal.ptr, 0, 5 * kMaxR * 8, st));
+    const dim3 g1a((unsigned)std::min<int64_t>(ceil_div(h->n, 256), 296), 1u);
+    amax_v_kernel<<<g1a, 256, 0, st>>>(v, h->n_pad, h->n, p->cmap.as<int>(), sc.amax_v);
+    sr_quant_v_kernel<<<(unsigned)ceil_div(h->n_pad, 256), 256, 0, st>>>(
+        v + (int64_t)cols[0] * h->n_pad, h->n, h->n_pad, sc.amax_v, sc.scale_v, planes_a, sc.sum_v);
+    sr_pass_a_kernel<<<(unsigned)(h->m_pad / kSrBlockMarkers), 256, 0, st>>>(
+        h->geno, h->wpr, planes_a, h->n_pad, sc.sum_v, sc.scale_v, h->two_p, h->inv_s, u);
+    SG_CHECK_LAUNCH();
+    if (h->masked) SG_CUDA(mask_rows_f64(u, h->m_pad, 1, h->excl.as<uint8_t>(), h->m, st));
+    const dim3 g1b((unsigned)std::min<int64_t>(ceil_div(h->m_pad, 256), 296), 1u);
+    amax_wc_kernel<<<g1b, 256, 0, st>>>(u, h->m_pad, h->m_pad, h->inv_s, h->two_p, sc.amax_w,
+                                        sc.amax_c);
+    sr_quant_wc_kernel<<<(unsigned)ceil_div(h->m_pad, 256), 256, 0, st>>>(
+        u, h->m_pad, h->inv_s, h->two_p, sc.amax_w, sc.amax_c, sc.scale_w, sc.scale_c, planes_b,
+        sc.sum_c);
+    sr_pass_b_kernel<<<(unsigned)(h->n_pad / kRows), kRows, 0, st>>>(
+        p->tiles_s.as<uint8_t>(), h->m_pad / kRows, planes_b, h->m_pad, sc.sum_c, sc.scale_w,
+        sc.scale_c, 1.0 / (double)(h->masked ? h->m_active : h->m), kp + (int64_t)cols[0] * h->n_pad);
+    SG_CHECK_LAUNCH();
+    count_launches(6);
+    SG_TRY(mark(&t1));
+    if (h->profiling) ev_s.emplace_back(t0, t1);
+    h->stats.sc_launches += 1;
+    h->n_kv += 1;
+  }
+  for (size_t c0 = 0; c0 < (single ? 0 : cols.size()); c0 += kMaxR) {
     const int r = (int)std::min<size_t>(kMaxR, cols.size() - c0);
     const int ng = (int)round_up(3 * r, 16);
     const int* cmap = p->cmap.as<int>() + c0;
@@ -1172,6 +1449,11 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     float ms = 0.f;
     SG_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
     h->stats.tc_pass_b_ms += ms;
+  }
+  for (auto& pr : ev_s) {
+    float ms = 0.f;
+    SG_CUDA(cudaEventElapsedTime(&ms, pr.first, pr.second));
+    h->stats.sc_ms += ms;
   }
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
   if (err) return fail(SAIGE_TIMEOUT, "tensor-core GRM product: a pipeline wait timed out");

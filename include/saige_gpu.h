@@ -422,6 +422,8 @@ typedef struct {
   double tc_pass_b_ms;
   int64_t fp32_launches;      /* FP32 product columns                        */
   double fp32_ms;
+  int64_t sc_launches;        /* MIXED single-column products on the CUDA    */
+  double sc_ms;               /* cores (both passes; dp4a, same sums)        */
 } saige_grm_stats;
 
 /* Turn per-kernel CUDA-event timing on (1) or off (0) for a handle. */
