@@ -501,30 +501,6 @@ SG_API void saige_ai_reml_config_default(saige_ai_reml_config* c) {
   c->precond = SAIGE_PRECOND_UNIT;
 }
 
-// With SAIGE_TIMING=1 in the environment, saige_fit_null_from_bed and the AI-REML
-// fit print the wall time of each phase (device synchronised at each mark) to stderr.
-struct PhaseTimer {
-  bool on = false;
-  const int64_t* launches = nullptr;  // GRM product launches, reported per phase when set
-  int64_t l0 = 0;
-  std::chrono::steady_clock::time_point t0;
-  PhaseTimer() {
-    const char* e = getenv("SAIGE_TIMING");
-    on = e && e[0] == '1';
-    t0 = std::chrono::steady_clock::now();
-  }
-  void mark(const char* what) {
-    if (!on) return;
-    cudaDeviceSynchronize();
-    const auto t1 = std::chrono::steady_clock::now();
-    const int64_t l = launches ? *launches : 0;
-    fprintf(stderr, "[saige timing] %-10s %8.2f ms  %lld GRM launches\n", what,
-            std::chrono::duration<double, std::milli>(t1 - t0).count(), (long long)(l - l0));
-    l0 = l;
-    t0 = t1;
-  }
-};
-
 static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n, int32_t p,
                        int32_t trait, const saige_ai_reml_config* cfg, saige_ai_reml_summary* out,
                        double* alpha_out, double* mu_out, double* eta_out, double* w_out,
@@ -903,6 +879,8 @@ SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t
     if (n_chrom <= 0) return fail(SAIGE_EINVAL, "n_chrom must be positive").code;
     if (p <= 0 || p > 64) return fail(SAIGE_EINVAL, "p must be in 1..64").code;
     if (trait < 0 || trait > 2) return fail(SAIGE_EINVAL, "unknown trait type").code;
+    if (h->m_eff != h->m)
+      return fail(SAIGE_EINVAL, "handle keeps rows outside its GRM (a streamed fit-null build)").code;
     for (int64_t j = 0; j < h->m; ++j)
       if (marker_chrom[j] < 0 || marker_chrom[j] >= n_chrom)
         return fail(SAIGE_EINVAL, "marker %lld: chromosome code %d outside 0..%d", (long long)j,
@@ -952,16 +930,20 @@ SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t
 // as it has landed, so that the counts hide under the PCIe transfer; af, mac and
 // n_valid then follow traits.rs:42-54 from the exact counts (counted = true).  From
 // pageable memory it is one copy and counted = false.
+static bool is_pinned(const void* p) {
+  cudaPointerAttributes attr{};
+  const bool pinned =
+      cudaPointerGetAttributes(&attr, p) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+  (void)cudaGetLastError();
+  return pinned;
+}
+
 static Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
                                const int64_t* sample_idx, int64_t n, DevBuf& d_bed,
                                std::vector<double>& af, std::vector<double>& mac,
                                std::vector<int64_t>& nv, bool& counted) {
   counted = false;
-  cudaPointerAttributes attr{};
-  const bool pinned =
-      cudaPointerGetAttributes(&attr, bed) == cudaSuccess && attr.type == cudaMemoryTypeHost;
-  (void)cudaGetLastError();
-  if (!pinned) {
+  if (!is_pinned(bed)) {
     SG_CUDA(cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice));
     return Status();
   }
@@ -1050,32 +1032,51 @@ SG_API int32_t saige_fit_null_from_bed(const uint8_t* bed, size_t bed_len, int64
     tm.mark("alloc bed");
     std::vector<double> af((size_t)m_tot), mac((size_t)m_tot);
     std::vector<int64_t> nv((size_t)m_tot);
-    int32_t rc = SAIGE_OK;
-    bool counted = false;
-    s = upload_and_count(bed, bed_len, n_fam, m_tot, sample_idx, n, d_bed, af, mac, nv, counted);
-    if (!s.ok()) return s.code;
-    tm.mark(counted ? "upload+counts" : "upload");
-    if (!counted) {
-      rc = saige_bed_marker_stats_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx, n,
-                                      af.data(), mac.data(), nv.data());
-      if (rc != SAIGE_OK) return rc;
-      tm.mark("counts");
-    }
-    std::vector<int64_t> gidx((size_t)m_tot), vidx((size_t)m_tot);
+    std::vector<int64_t> gidx, vidx;
     int64_t m_grm = 0, m_vr = 0;
-    rc = saige_select_grm_markers(af.data(), mac.data(), nv.data(), m_tot, n, min_maf, max_missing,
-                                  c.seed, gidx.data(), &m_grm, vidx.data(), &m_vr);
-    if (rc != SAIGE_OK) return rc;
+    int32_t rc = SAIGE_OK;
+    saige_grm* h = nullptr;
+    // MIXED fits from pinned memory build the GRM while the .bed streams in
+    const bool mixed_only = c.precision == SAIGE_PREC_MIXED &&
+                            (!vr_out || !vr_cfg || vr_cfg->precision == SAIGE_PREC_MIXED);
+    if (mixed_only && is_pinned(bed)) {
+      s = stream_fit_null_grm(bed, bed_len, n_fam, m_tot, sample_idx, n, min_maf, max_missing,
+                              c.seed, d_bed, af, mac, nv, vidx, m_grm, &h);
+      if (!s.ok() && s.code != SAIGE_ENOMEM) return s.code;
+      if (s.ok()) {
+        m_vr = (int64_t)vidx.size();
+        tm.mark("stream grm");
+      } else {
+        h = nullptr;  // short of memory for the streamed build: the steps below
+        set_error("");
+      }
+    }
+    if (!h) {
+      bool counted = false;
+      s = upload_and_count(bed, bed_len, n_fam, m_tot, sample_idx, n, d_bed, af, mac, nv, counted);
+      if (!s.ok()) return s.code;
+      tm.mark(counted ? "upload+counts" : "upload");
+      if (!counted) {
+        rc = saige_bed_marker_stats_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx, n,
+                                        af.data(), mac.data(), nv.data());
+        if (rc != SAIGE_OK) return rc;
+        tm.mark("counts");
+      }
+      gidx.resize((size_t)m_tot);
+      vidx.resize((size_t)m_tot);
+      rc = saige_select_grm_markers(af.data(), mac.data(), nv.data(), m_tot, n, min_maf,
+                                    max_missing, c.seed, gidx.data(), &m_grm, vidx.data(), &m_vr);
+      if (rc != SAIGE_OK) return rc;
+      tm.mark("select");
+      std::vector<double> gaf((size_t)m_grm);
+      for (int64_t j = 0; j < m_grm; ++j) gaf[(size_t)j] = af[(size_t)gidx[(size_t)j]];
+      rc = saige_grm_create_from_bed_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx,
+                                         n, gidx.data(), m_grm, gaf.data(), -1, &h);
+      if (rc != SAIGE_OK) return rc;
+      tm.mark("grm");
+    }
     if (m_grm_out) *m_grm_out = m_grm;
     if (m_vr_out) *m_vr_out = m_vr;
-    tm.mark("select");
-    std::vector<double> gaf((size_t)m_grm);
-    for (int64_t j = 0; j < m_grm; ++j) gaf[(size_t)j] = af[(size_t)gidx[(size_t)j]];
-    saige_grm* h = nullptr;
-    rc = saige_grm_create_from_bed_dev(d_bed.as<uint8_t>(), bed_len, n_fam, m_tot, sample_idx, n,
-                                       gidx.data(), m_grm, gaf.data(), -1, &h);
-    if (rc != SAIGE_OK) return rc;
-    tm.mark("grm");
     // the variance-ratio candidates' packed rows outlive the full .bed
     VrRows vr_rows;
     std::vector<double> vr_mac;

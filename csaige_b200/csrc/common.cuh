@@ -5,7 +5,9 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <chrono>
 #include <cstdio>
+#include <cstdlib>
 #include <string>
 
 #include "../../include/saige_gpu.h"
@@ -64,5 +66,30 @@ __device__ __forceinline__ float warp_sum(float v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
+
+// With SAIGE_TIMING=1 in the environment, saige_fit_null_from_bed, the GRM handle
+// build and the AI-REML fit print the wall time of each phase (device synchronised
+// at each mark) to stderr.
+struct PhaseTimer {
+  bool on = false;
+  const int64_t* launches = nullptr;  // GRM product launches, reported per phase when set
+  int64_t l0 = 0;
+  std::chrono::steady_clock::time_point t0;
+  PhaseTimer() {
+    const char* e = getenv("SAIGE_TIMING");
+    on = e && e[0] == '1';
+    t0 = std::chrono::steady_clock::now();
+  }
+  void mark(const char* what) {
+    if (!on) return;
+    cudaDeviceSynchronize();
+    const auto t1 = std::chrono::steady_clock::now();
+    const int64_t l = launches ? *launches : 0;
+    fprintf(stderr, "[saige timing] %-10s %8.2f ms  %lld GRM launches\n", what,
+            std::chrono::duration<double, std::milli>(t1 - t0).count(), (long long)(l - l0));
+    l0 = l;
+    t0 = t1;
+  }
+};
 
 }  // namespace saige

@@ -149,11 +149,13 @@ Status pick_device(int32_t want, int* dev) {
   int d = want;
   if (d < 0) SG_CUDA(cudaGetDevice(&d));
   if (d >= count) return fail(SAIGE_EINVAL, "device %d out of range (%d devices)", d, count);
-  cudaDeviceProp prop;
-  SG_CUDA(cudaGetDeviceProperties(&prop, d));
-  if (prop.major != 10 || prop.minor != 0)
+  // two attribute queries (a full cudaGetDeviceProperties costs milliseconds per call)
+  int major = 0, minor = 0;
+  SG_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, d));
+  SG_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, d));
+  if (major != 10 || minor != 0)
     return fail(SAIGE_ECUDA, "device %d is sm_%d%d; this library is built for sm_100a only", d,
-                prop.major, prop.minor);
+                major, minor);
   SG_CUDA(cudaSetDevice(d));
   if (dev) *dev = d;
   return Status();
@@ -196,6 +198,7 @@ static Status grm_alloc(saige_grm* h, int64_t n, int64_t m) {
   h->n_pad = round_up(std::max<int64_t>(n, 1), kSamplePad);
   h->wpr = h->n_pad / 16;
   h->m = m;
+  h->m_eff = m;
   h->m_pad = round_up(std::max<int64_t>(m, 1), kMarkerPad);
   SG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   SG_TRY(h->geno_buf.reserve((size_t)h->m_pad * h->wpr * 4));
@@ -317,7 +320,7 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
   SG_TRY(h->v32.reserve((size_t)h->n_pad * sizeof(float)));
   SG_TRY(h->u32.reserve((size_t)h->m_pad * sizeof(float)));
   SG_TRY(h->ypart.reserve((size_t)h->n_splits * h->n_pad * sizeof(float)));
-  const float scale = 1.0f / (float)(h->masked ? h->m_active : h->m);
+  const float scale = 1.0f / (float)(h->masked ? h->m_active : h->m_eff);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (h->profiling) {
     SG_CUDA(cudaEventCreate(&e0));
@@ -355,7 +358,7 @@ static Status grm_product_fp32(saige_grm* h, const double* v, double* kp, int q,
 
 Status grm_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
                    int precision, cudaStream_t st) {
-  if (h->m == 0 || (h->masked && h->m_active == 0)) {
+  if (h->m_eff == 0 || (h->masked && h->m_active == 0)) {
     // pcg.rs:132-134: no markers -> zero vector
     for (int c = 0; c < q; ++c)
       if (!active || active[c] == kColActive)
@@ -664,6 +667,29 @@ SG_API int32_t saige_rademacher_probes(uint64_t seed, int32_t n_vec, int64_t n, 
   SG_GUARD_END
 }
 
+// fit_null.rs:209-222: the QC a marker passes to enter the GRM or the variance-ratio
+// candidates.
+static bool qc_pass(double af, int64_t n_valid, int64_t n, double min_maf, double max_missing) {
+  const double missing_rate = 1.0 - ((double)n_valid / (double)n);
+  return af >= min_maf && af <= 1.0 - min_maf && missing_rate <= max_missing;
+}
+
+// fit_null.rs:234-243: 1000 draws of gen_range(0..pass.len()) from ChaCha8(seed),
+// sorted and deduplicated; a drawn marker with mac >= 20 is a variance-ratio
+// candidate (flags[i] = 1 for position i of pass), every other passing marker is a
+// GRM marker.
+static void vr_candidate_flags(const std::vector<int64_t>& pass, const double* mac, uint64_t seed,
+                               std::vector<uint8_t>& flags) {
+  ChaCha8 rng(seed);
+  std::vector<uint64_t> cand(1000);
+  for (auto& c : cand) c = rng.gen_range(0, (uint64_t)pass.size());
+  std::sort(cand.begin(), cand.end());
+  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
+  flags.assign(pass.size(), 0);
+  for (uint64_t c : cand)
+    if (mac[pass[(size_t)c]] >= 20.0) flags[(size_t)c] = 1;
+}
+
 SG_API int32_t saige_select_grm_markers(const double* af, const double* mac,
                                         const int64_t* n_valid, int64_t m_tot, int64_t n,
                                         double min_maf, double max_missing, uint64_t seed,
@@ -676,24 +702,14 @@ SG_API int32_t saige_select_grm_markers(const double* af, const double* mac,
   // fit_null.rs:209-222
   std::vector<int64_t> pass;
   pass.reserve((size_t)m_tot);
-  for (int64_t j = 0; j < m_tot; ++j) {
-    const double missing_rate = 1.0 - ((double)n_valid[j] / (double)n);
-    if (af[j] >= min_maf && af[j] <= 1.0 - min_maf && missing_rate <= max_missing)
-      pass.push_back(j);
-  }
+  for (int64_t j = 0; j < m_tot; ++j)
+    if (qc_pass(af[j], n_valid[j], n, min_maf, max_missing)) pass.push_back(j);
   *m_grm = 0;
   *m_vr = 0;
   if (pass.empty())
     return fail(SAIGE_EINVAL, "no marker passes QC (gen_range(0..0) in the reference)").code;
-  // fit_null.rs:234-243
-  ChaCha8 rng(seed);
-  std::vector<uint64_t> cand(1000);
-  for (auto& c : cand) c = rng.gen_range(0, (uint64_t)pass.size());
-  std::sort(cand.begin(), cand.end());
-  cand.erase(std::unique(cand.begin(), cand.end()), cand.end());
-  std::vector<uint8_t> vr(pass.size(), 0);
-  for (uint64_t c : cand)
-    if (mac[pass[(size_t)c]] >= 20.0) vr[(size_t)c] = 1;
+  std::vector<uint8_t> vr;
+  vr_candidate_flags(pass, mac, seed, vr);
   int64_t g = 0, v = 0;
   for (size_t i = 0; i < pass.size(); ++i) {
     if (vr[i]) vr_idx[v++] = pass[i];
@@ -736,9 +752,12 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
   }
   saige_grm* h = new saige_grm();
   h->device = dev;
+  PhaseTimer tm;
   auto body = [&]() -> Status {
     SG_TRY(grm_alloc(h, n, m));
+    tm.mark(" grm alloc");
     SG_TRY(grm_upload_meta(h, allele_freqs));
+    tm.mark(" grm meta");
     if (m > 0) {
       const int64_t bpm = (n_fam + 3) / 4;
       const size_t used = (size_t)(3 + bpm * m_tot);
@@ -751,7 +770,9 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
       }
       SG_TRY(bed_gather_dev(src, n_fam, rows, sidx, identity, n, h->geno, h->wpr, nullptr,
                             h->stream));
+      tm.mark(" grm gather");
       SG_TRY(grm_blank_degenerate_rows(h, allele_freqs));
+      tm.mark(" grm blank");
     }
     SG_CUDA(cudaStreamSynchronize(h->stream));
     return Status();
@@ -764,6 +785,201 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
   *out = h;
   return SAIGE_OK;
 }
+
+// The fit-null GRM built while the .bed streams in from pinned host memory.  The
+// upload runs in marker chunks on a copy stream; as each chunk lands, the handle's
+// stream counts its alleles and missing calls (K1), the host applies the marker QC
+// to the chunk, and the chunk's passing markers are gathered into the next rows of
+// the handle and tiled as soon as a 128-row group is complete — all under the
+// transfer of the chunks that follow.  The rows are every QC-passing marker in .bed
+// order; the variance-ratio candidates, drawn only once the number of passing
+// markers is known, stay in place with 2p = 1/s = 0 (so that every product gets an
+// exact zero from them) and m_eff = m - candidates is the GRM's M.  The integer
+// products of the MIXED path are then bit-identical to those of a handle holding
+// only the GRM markers; FP32 products would sum in another grouping, so this build
+// serves MIXED fits only.
+namespace saige {
+
+Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                           const int64_t* sample_idx, int64_t n, double min_maf,
+                           double max_missing, uint64_t seed, DevBuf& d_bed,
+                           std::vector<double>& af, std::vector<double>& mac,
+                           std::vector<int64_t>& nv, std::vector<int64_t>& vidx, int64_t& m_grm,
+                           saige_grm** out) {
+  *out = nullptr;
+  SG_TRY(check_bed_header(bed, bed_len, n_fam, m_tot));
+  std::vector<int32_t> sidx;
+  bool identity = true;
+  SG_TRY(check_subset(sample_idx, n, n_fam, sidx, identity));
+  if (d_bed.bytes < bed_len) return fail(SAIGE_EINVAL, "device .bed buffer too small");
+  int dev = 0;
+  SG_TRY(pick_device(-1, &dev));
+  const int64_t bpm = (n_fam + 3) / 4;
+  const int64_t cap = round_up(m_tot, kMarkerPad);
+  saige_grm* h = new saige_grm();
+  h->device = dev;
+  struct Streams {
+    cudaStream_t c = nullptr;
+    std::vector<cudaEvent_t> ev;
+    cudaStream_t k = nullptr;
+    ~Streams() {
+      if (c) cudaStreamSynchronize(c);
+      if (k) cudaStreamSynchronize(k);
+      for (cudaEvent_t e : ev) cudaEventDestroy(e);
+      if (c) cudaStreamDestroy(c);
+    }
+  };
+  // Host-mapped memory for what crosses PCIe beside the .bed (row lists, counts): no
+  // copy of it queues behind the chunks on the copy engines.
+  struct Mapped {
+    void* p = nullptr;
+    ~Mapped() {
+      if (p) cudaFreeHost(p);
+    }
+  };
+  PhaseTimer tm;
+  auto body = [&]() -> Status {
+    Mapped mp;  // outlives the streams' last use of it (destroyed after ss)
+    Streams ss;
+    SG_CUDA(cudaStreamCreateWithFlags(&ss.c, cudaStreamNonBlocking));
+    // the sample subset ahead of the .bed on the copy stream (the counts need it)
+    DevBuf d_sidx;
+    const int32_t* sp = nullptr;
+    if (!identity) {
+      SG_TRY(d_sidx.reserve(sidx.size() * 4));
+      SG_CUDA(cudaMemcpyAsync(d_sidx.ptr, sidx.data(), sidx.size() * 4, cudaMemcpyHostToDevice,
+                              ss.c));
+      sp = d_sidx.as<int32_t>();
+    }
+    // every chunk's copy is queued first, so that all the set-up below overlaps the
+    // transfer; the kernels follow chunk by chunk
+    constexpr int kChunks = 32;
+    const int64_t per = ceil_div(m_tot, (int64_t)kChunks);
+    uint8_t* dst = d_bed.as<uint8_t>();
+    for (int64_t j0 = 0; j0 < m_tot; j0 += per) {
+      const int64_t j1 = std::min(m_tot, j0 + per);
+      const size_t lo = j0 == 0 ? 0 : (size_t)(3 + j0 * bpm);
+      const size_t hi = j1 == m_tot ? bed_len : (size_t)(3 + j1 * bpm);
+      SG_CUDA(cudaMemcpyAsync(dst + lo, bed + lo, hi - lo, cudaMemcpyHostToDevice, ss.c));
+      cudaEvent_t e = nullptr;
+      SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ss.ev.push_back(e);
+      SG_CUDA(cudaEventRecord(e, ss.c));
+    }
+    h->n = n;
+    h->n_pad = round_up(std::max<int64_t>(n, 1), kSamplePad);
+    h->wpr = h->n_pad / 16;
+    SG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    ss.k = h->stream;
+    SG_TRY(h->geno_buf.reserve((size_t)cap * h->wpr * 4));
+    h->geno = h->geno_buf.as<uint32_t>();
+    SG_CUDA(cudaMalloc(&h->zlut, (size_t)cap * sizeof(float4)));
+    SG_CUDA(cudaMalloc(&h->two_p, (size_t)cap * sizeof(double)));
+    SG_CUDA(cudaMalloc(&h->inv_s, (size_t)cap * sizeof(double)));
+    SG_TRY(tc_stream_begin(h, cap));
+    // all[j] = j (the rows the counts read), prow (the passing rows, in .bed order),
+    // cnt (alt and missing counts per marker)
+    SG_CUDA(cudaHostAlloc(&mp.p, (size_t)m_tot * 32, cudaHostAllocMapped));
+    int64_t* all_h = static_cast<int64_t*>(mp.p);
+    int64_t* prow_h = all_h + m_tot;
+    int64_t* cnt_h = prow_h + m_tot;
+    void* mapped_dev = nullptr;
+    SG_CUDA(cudaHostGetDevicePointer(&mapped_dev, mp.p, 0));
+    const int64_t* all_d = static_cast<const int64_t*>(mapped_dev);
+    const int64_t* prow_d = all_d + m_tot;
+    int64_t* cnt_d = const_cast<int64_t*>(prow_d) + m_tot;
+    for (int64_t j = 0; j < m_tot; ++j) all_h[j] = j;
+    cudaEvent_t counted = nullptr;
+    SG_CUDA(cudaEventCreateWithFlags(&counted, cudaEventDisableTiming));
+    ss.ev.push_back(counted);
+    std::vector<int64_t> pass;
+    pass.reserve((size_t)m_tot);
+    int64_t mt_done = 0;
+    size_t chunk = 0;
+    for (int64_t j0 = 0; j0 < m_tot; j0 += per, ++chunk) {
+      const int64_t j1 = std::min(m_tot, j0 + per);
+      SG_CUDA(cudaStreamWaitEvent(h->stream, ss.ev[chunk], 0));
+      SG_CUDA(launch_bed_gather(dst, bpm, all_d + j0, j1 - j0, sp, n, nullptr, 0, cnt_d + 2 * j0,
+                                h->stream));
+      SG_CUDA(cudaEventRecord(counted, h->stream));
+      SG_CUDA(cudaEventSynchronize(counted));
+      const size_t p0 = pass.size();
+      std::vector<int64_t> degenerate;
+      for (int64_t j = j0; j < j1; ++j) {
+        const int64_t alt = cnt_h[2 * j], miss = cnt_h[2 * j + 1];
+        const int64_t valid = n - miss;
+        // traits.rs:42-54, the same f64 operations on the same exact integers
+        const double sum = (double)alt;
+        af[(size_t)j] = valid > 0 ? sum / (2.0 * (double)valid) : 0.0;
+        const double other = 2.0 * (double)valid - sum;
+        mac[(size_t)j] = sum < other ? sum : other;
+        nv[(size_t)j] = valid;
+        if (!qc_pass(af[(size_t)j], valid, n, min_maf, max_missing)) continue;
+        const double p = af[(size_t)j];
+        if (!(sqrt(2.0 * p * (1.0 - p)) > 1e-10)) degenerate.push_back((int64_t)pass.size());
+        prow_h[pass.size()] = j;
+        pass.push_back(j);
+      }
+      const size_t p1 = pass.size();
+      if (p1 > p0) {
+        SG_CUDA(launch_bed_gather(dst, bpm, prow_d + p0, (int64_t)(p1 - p0), sp, n,
+                                  h->geno + p0 * (size_t)h->wpr, h->wpr, nullptr, h->stream));
+        // a zero standardised column: codes 11, as grm_blank_degenerate_rows does
+        for (int64_t r : degenerate)
+          SG_CUDA(cudaMemsetAsync(h->geno + (size_t)r * h->wpr, 0xFF, (size_t)h->wpr * 4,
+                                  h->stream));
+      }
+      const int64_t mt_full = (int64_t)p1 / kMarkerPad;
+      SG_TRY(tc_stream_tiles(h, mt_done, mt_full, h->stream));
+      mt_done = mt_full;
+    }
+    tm.mark(" stream chunks");
+    if (pass.empty())
+      return fail(SAIGE_EINVAL, "no marker passes QC (gen_range(0..0) in the reference)");
+    std::vector<uint8_t> flags;
+    vr_candidate_flags(pass, mac.data(), seed, flags);
+    const int64_t rows = (int64_t)pass.size();
+    h->m = rows;
+    h->m_pad = round_up(rows, kMarkerPad);
+    // padding rows: all codes 11, 2p = 1/s = 0
+    SG_CUDA(cudaMemsetAsync(h->geno + (size_t)rows * h->wpr, 0xFF,
+                            (size_t)(h->m_pad - rows) * h->wpr * 4, h->stream));
+    SG_TRY(tc_stream_tiles(h, mt_done, h->m_pad / kMarkerPad, h->stream));
+    std::vector<double> row_af((size_t)rows);
+    for (int64_t r = 0; r < rows; ++r) row_af[(size_t)r] = af[(size_t)pass[(size_t)r]];
+    std::vector<float4> zl;
+    std::vector<double> tp, is;
+    marker_meta(row_af.data(), rows, h->m_pad, zl, tp, is);
+    vidx.clear();
+    for (int64_t r = 0; r < rows; ++r) {
+      if (!flags[(size_t)r]) continue;
+      vidx.push_back(pass[(size_t)r]);
+      zl[(size_t)r] = make_float4(0.f, 0.f, 0.f, 0.f);
+      tp[(size_t)r] = 0.0;
+      is[(size_t)r] = 0.0;
+    }
+    SG_CUDA(cudaMemcpyAsync(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                            h->stream));
+    SG_CUDA(cudaMemcpyAsync(h->two_p, tp.data(), tp.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    SG_CUDA(cudaMemcpyAsync(h->inv_s, is.data(), is.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    h->m_eff = rows - (int64_t)vidx.size();
+    m_grm = h->m_eff;
+    h->n_splits = fp32_z_splits(h->n_pad, h->m_pad);
+    SG_CUDA(cudaStreamSynchronize(h->stream));
+    SG_CUDA(cudaStreamSynchronize(ss.c));
+    tm.mark(" stream tail");
+    return Status();
+  };
+  Status s = body();
+  if (!s.ok()) {
+    grm_free(h);
+    return s;
+  }
+  *out = h;
+  return Status();
+}
+
+}  // namespace saige
 
 SG_API int32_t saige_grm_create_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam,
                                          int64_t m_tot, const int64_t* sample_idx, int64_t n,

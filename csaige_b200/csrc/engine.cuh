@@ -47,6 +47,18 @@ Status bed_gather_dev(const uint8_t* bed_dev, int64_t n_fam, const std::vector<i
                       const std::vector<int32_t>& sidx, bool identity, int64_t n,
                       uint32_t* geno_out, int64_t wpr, int64_t* counts_dev, cudaStream_t st);
 
+// The fit-null GRM handle built while the .bed (pinned host memory, bed_len bytes)
+// streams into d_bed: marker counts into af/mac/nv (length m_tot), the QC of
+// fit_null.rs:209-222, the variance-ratio candidates into vidx, m_grm = the GRM's M.
+// The handle's rows are all QC-passing markers; the candidates' rows carry
+// 2p = 1/s = 0 and m_eff = m_grm.  For MIXED products only.
+Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                           const int64_t* sample_idx, int64_t n, double min_maf,
+                           double max_missing, uint64_t seed, DevBuf& d_bed,
+                           std::vector<double>& af, std::vector<double>& mac,
+                           std::vector<int64_t>& nv, std::vector<int64_t>& vidx, int64_t& m_grm,
+                           saige_grm** out);
+
 }  // namespace saige
 
 struct saige_grm {
@@ -54,7 +66,10 @@ struct saige_grm {
   cudaStream_t stream = nullptr;
   std::recursive_mutex mu;
   int64_t n = 0, n_pad = 0, wpr = 0;  // samples, padded samples, 32-bit words per row
-  int64_t m = 0, m_pad = 0;           // markers, padded markers
+  int64_t m = 0, m_pad = 0;           // marker rows, padded marker rows
+  // markers that enter K (the 1/M of every product): m, less the rows a streamed
+  // build kept in place with 2p = 1/s = 0 (variance-ratio candidates)
+  int64_t m_eff = 0;
   uint32_t* geno = nullptr;           // m_pad x wpr packed 2-bit codes (in geno_buf)
   saige::DevBuf geno_buf;
   float4* zlut = nullptr;             // per marker: f32 z for codes 00,01,10,11

@@ -77,7 +77,8 @@ struct TcArgs {
   int sub;                  // 128-entry sub-stages per load stage (1, 2 or 4)
   int sl;                   // load-ring depth in load stages (>= 2)
   int sa;                   // TMEM operand slots, one per sub-stage (even)
-  const uint8_t* tiles;     // this pass's code tiles, tile t at (t*nk + k)*4 KB
+  const uint8_t* tiles;     // this pass's code tiles, tile t at (t*tile_ld + k)*4 KB
+  int64_t tile_ld;          // tiles from one output tile's row of tiles to the next (>= nk)
   const uint8_t* img_g;     // nk x ng x 128 bytes
   const uint8_t* img_m;     // pass B: c image (same shape)
   const double* scale_g;    // [r]
@@ -382,7 +383,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
     // ---------------- producer: code tiles and limb tiles by bulk copy ----------------
     if (lane == 0) {
       const int n_load = (a.nk + a.sub - 1) / a.sub;
-      const uint8_t* codes = a.tiles + (size_t)tile * a.nk * kTileBytes;
+      const uint8_t* codes = a.tiles + (size_t)tile * a.tile_ld * kTileBytes;
       int S = 0;
       uint32_t ph = 0;  // (J / sl) & 1
       for (int J = 0; J < n_load; ++J) {
@@ -567,24 +568,26 @@ __device__ __forceinline__ int entry_bit(int e) {
   return 16 * (j >> 1) + 2 * (j & 1) + 4 * i;
 }
 
-// tiles_m[(mt * n_kt + kt)] row r = row-major row mt*128 + r, words kt*8 .. kt*8+7.
+// tiles_m[(mt * n_kt + kt)] row r = row-major row mt*128 + r, words kt*8 .. kt*8+7,
+// for the marker tiles mt0 + blockIdx.y.
 __global__ void __launch_bounds__(256)
-    pack_tiles_kernel(const uint32_t* __restrict__ geno, int64_t wpr, int64_t n_kt,
+    pack_tiles_kernel(const uint32_t* __restrict__ geno, int64_t wpr, int64_t n_kt, int64_t mt0,
                       uint8_t* __restrict__ tiles) {
-  const int64_t kt = blockIdx.x, mt = blockIdx.y;
+  const int64_t kt = blockIdx.x, mt = mt0 + blockIdx.y;
   const int r = threadIdx.x >> 1, half = threadIdx.x & 1;
   const uint4 v = *reinterpret_cast<const uint4*>(geno + (mt * kRows + r) * wpr + kt * 8 + half * 4);
   *reinterpret_cast<uint4*>(tiles + (mt * n_kt + kt) * kTileBytes + r * 32 + half * 16) = v;
 }
 
-// tiles_s[(st * n_mt + mt)] row r = sample st*128 + r, word j = markers
-// mt*128 + 16j .. +15, read from tiles_m[(mt * n_st + st)].
+// tiles_s[(st * s_ld + mt)] row r = sample st*128 + r, word j = markers
+// mt*128 + 16j .. +15, read from tiles_m[(mt * n_st + st)], for the marker tiles
+// mt0 + blockIdx.x.
 __global__ void __launch_bounds__(256)
-    transpose_tiles_kernel(const uint8_t* __restrict__ tiles_m, int64_t n_st, int64_t n_mt,
-                           uint8_t* __restrict__ tiles_s) {
+    transpose_tiles_kernel(const uint8_t* __restrict__ tiles_m, int64_t n_st, int64_t s_ld,
+                           int64_t mt0, uint8_t* __restrict__ tiles_s) {
   __shared__ __align__(16) uint32_t src[kTileBytes / 4];
   __shared__ __align__(16) uint32_t dst[kTileBytes / 4];
-  const int64_t mt = blockIdx.x, st = blockIdx.y;
+  const int64_t mt = mt0 + blockIdx.x, st = blockIdx.y;
   const uint4* s4 = reinterpret_cast<const uint4*>(tiles_m + (mt * n_st + st) * kTileBytes);
   reinterpret_cast<uint4*>(src)[threadIdx.x] = s4[threadIdx.x];
   __syncthreads();
@@ -601,7 +604,7 @@ __global__ void __launch_bounds__(256)
     dst[r * 8 + j] = w;
   }
   __syncthreads();
-  reinterpret_cast<uint4*>(tiles_s + (st * n_mt + mt) * kTileBytes)[threadIdx.x] =
+  reinterpret_cast<uint4*>(tiles_s + (st * s_ld + mt) * kTileBytes)[threadIdx.x] =
       reinterpret_cast<const uint4*>(dst)[threadIdx.x];
 }
 
@@ -913,7 +916,7 @@ __global__ void __launch_bounds__(256, 2)
 // Pass B of one column: block = one 128-sample tile of tiles_s, thread = sample.  The
 // marker limb planes are staged in shared memory kSrChunk markers at a time.
 __global__ void __launch_bounds__(128)
-    sr_pass_b_kernel(const uint8_t* __restrict__ tiles_s, int64_t n_mt,
+    sr_pass_b_kernel(const uint8_t* __restrict__ tiles_s, int64_t n_mt, int64_t s_ld,
                      const int8_t* __restrict__ planes, int64_t m_pad,
                      const unsigned long long* __restrict__ sum_c,
                      const double* __restrict__ scale_w, const double* __restrict__ scale_c,
@@ -936,7 +939,7 @@ __global__ void __launch_bounds__(128)
     __syncthreads();
     const int64_t mt_end = mt0 + kSrChunk / 128 < n_mt ? mt0 + kSrChunk / 128 : n_mt;
     for (int64_t mt = mt0; mt < mt_end; ++mt) {
-      const uint4* row = reinterpret_cast<const uint4*>(tiles_s + (st * n_mt + mt) * kTileBytes +
+      const uint4* row = reinterpret_cast<const uint4*>(tiles_s + (st * s_ld + mt) * kTileBytes +
                                                         (int64_t)r * 32);
       const uint4 h0 = __ldg(row), h1 = __ldg(row + 1);
       const uint32_t words[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
@@ -1009,6 +1012,7 @@ size_t tc_smem_bytes(int ng, bool pass_b) {
 
 struct TcPlan {
   DevBuf tiles_m, tiles_s, img_a, img_w, img_c, u, scal, cmap, trace;
+  int64_t s_ld = 0;  // tiles_s: marker tiles per sample tile (>= m_pad / 128)
   bool tracing = false;
 };
 
@@ -1040,23 +1044,31 @@ static Status trace_dump(TcPlan* p, const char* what, cudaStream_t st) {
 
 // Builds the two tile copies of the packed genotypes (marker-major for pass A,
 // sample-major for pass B) from the row-major copy, on the handle's stream.
-static Status build_tiles(saige_grm* h, TcPlan* p) {
-  const int64_t n_mt = h->m_pad / kRows, n_st = h->n_pad / kKt;
-  const size_t bytes = (size_t)n_mt * n_st * kTileBytes;
-  SG_TRY(p->tiles_m.reserve(bytes));
-  SG_TRY(p->tiles_s.reserve(bytes));
-  pack_tiles_kernel<<<dim3((unsigned)n_st, (unsigned)n_mt), 256, 0, h->stream>>>(
-      h->geno, h->wpr, n_st, p->tiles_m.as<uint8_t>());
+// Tiles of the marker tiles [mt0, mt1) from the row-major rows, on stream st.
+static Status tiles_range(saige_grm* h, TcPlan* p, int64_t mt0, int64_t mt1, cudaStream_t st) {
+  if (mt1 <= mt0) return Status();
+  const int64_t n_st = h->n_pad / kKt;
+  pack_tiles_kernel<<<dim3((unsigned)n_st, (unsigned)(mt1 - mt0)), 256, 0, st>>>(
+      h->geno, h->wpr, n_st, mt0, p->tiles_m.as<uint8_t>());
   SG_CHECK_LAUNCH();
-  transpose_tiles_kernel<<<dim3((unsigned)n_mt, (unsigned)n_st), 256, 0, h->stream>>>(
-      p->tiles_m.as<uint8_t>(), n_st, n_mt, p->tiles_s.as<uint8_t>());
+  transpose_tiles_kernel<<<dim3((unsigned)(mt1 - mt0), (unsigned)n_st), 256, 0, st>>>(
+      p->tiles_m.as<uint8_t>(), n_st, p->s_ld, mt0, p->tiles_s.as<uint8_t>());
   SG_CHECK_LAUNCH();
   count_launches(2);
   return Status();
 }
 
-static Status tc_init(saige_grm* h) {
-  if (h->tc) return Status();
+static Status reserve_tiles(saige_grm* h, TcPlan* p, int64_t n_mt) {
+  const size_t bytes = (size_t)n_mt * (size_t)(h->n_pad / kKt) * kTileBytes;
+  SG_TRY(p->tiles_m.reserve(bytes));
+  SG_TRY(p->tiles_s.reserve(bytes));
+  p->s_ld = n_mt;
+  return Status();
+}
+
+// A new plan with the kernels' attributes set and, when asked for, the trace buffer;
+// the tiles are the caller's.
+static Status tc_plan_new(TcPlan** out) {
   TcPlan* p = new TcPlan();
   auto bail = [&](Status s) {
     delete p;
@@ -1068,8 +1080,6 @@ static Status tc_init(saige_grm* h) {
     if (e != cudaSuccess)
       return bail(fail(SAIGE_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e)));
   }
-  Status bs = build_tiles(h, p);
-  if (!bs.ok()) return bail(bs);
   const char* tr = getenv("SAIGE_TC_TRACE");
   p->tracing = tr && tr[0] == '1';
   if (p->tracing) {
@@ -1078,8 +1088,42 @@ static Status tc_init(saige_grm* h) {
     cudaError_t e = cudaMemset(p->trace.ptr, 0, (size_t)kTraceStages * kTraceSlots * 8);
     if (e != cudaSuccess) return bail(fail(SAIGE_ECUDA, "cudaMemset: %s", cudaGetErrorString(e)));
   }
+  *out = p;
+  return Status();
+}
+
+static Status tc_init(saige_grm* h) {
+  if (h->tc) return Status();
+  TcPlan* p = nullptr;
+  SG_TRY(tc_plan_new(&p));
+  PhaseTimer tm;
+  Status bs = reserve_tiles(h, p, h->m_pad / kRows);
+  if (bs.ok()) bs = tiles_range(h, p, 0, h->m_pad / kRows, h->stream);
+  if (!bs.ok()) {
+    delete p;
+    return bs;
+  }
+  tm.mark(" tc tiles");
   h->tc = p;
   return Status();
+}
+
+Status tc_stream_begin(saige_grm* h, int64_t rows_cap) {
+  if (h->tc) return fail(SAIGE_EINVAL, "tensor-core tiles already built");
+  TcPlan* p = nullptr;
+  SG_TRY(tc_plan_new(&p));
+  Status s = reserve_tiles(h, p, ceil_div(rows_cap, (int64_t)kRows));
+  if (!s.ok()) {
+    delete p;
+    return s;
+  }
+  h->tc = p;
+  return Status();
+}
+
+Status tc_stream_tiles(saige_grm* h, int64_t mt0, int64_t mt1, cudaStream_t st) {
+  if (!h->tc || mt1 > h->tc->s_ld) return fail(SAIGE_EINVAL, "tile range beyond the reserved tiles");
+  return tiles_range(h, h->tc, mt0, mt1, st);
 }
 
 void tc_destroy(saige_grm* h) {
@@ -1339,8 +1383,8 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
         u, h->m_pad, h->inv_s, h->two_p, sc.amax_w, sc.amax_c, sc.scale_w, sc.scale_c, planes_b,
         sc.sum_c);
     sr_pass_b_kernel<<<(unsigned)(h->n_pad / kRows), kRows, 0, st>>>(
-        p->tiles_s.as<uint8_t>(), h->m_pad / kRows, planes_b, h->m_pad, sc.sum_c, sc.scale_w,
-        sc.scale_c, 1.0 / (double)(h->masked ? h->m_active : h->m), kp + (int64_t)cols[0] * h->n_pad);
+        p->tiles_s.as<uint8_t>(), h->m_pad / kRows, p->s_ld, planes_b, h->m_pad, sc.sum_c, sc.scale_w,
+        sc.scale_c, 1.0 / (double)(h->masked ? h->m_active : h->m_eff), kp + (int64_t)cols[0] * h->n_pad);
     SG_CHECK_LAUNCH();
     count_launches(6);
     SG_TRY(mark(&t1));
@@ -1371,6 +1415,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.r = r;
       a.nk = (int)n_stages_a;
       a.tiles = p->tiles_m.as<uint8_t>();
+      a.tile_ld = n_stages_a;
       a.img_g = p->img_a.as<uint8_t>();
       a.scale_g = sc.scale_v;
       a.sum_q = reinterpret_cast<const long long*>(sc.sum_v);
@@ -1414,6 +1459,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.r = r;
       a.nk = (int)n_stages_b;
       a.tiles = p->tiles_s.as<uint8_t>();
+      a.tile_ld = p->s_ld;
       a.img_g = p->img_w.as<uint8_t>();
       a.img_m = p->img_c.as<uint8_t>();
       a.scale_g = sc.scale_w;
@@ -1422,7 +1468,7 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
       a.out = kp;
       a.out_ld = h->n_pad;
       a.col_map = cmap;
-      a.out_scale = 1.0 / (double)(h->masked ? h->m_active : h->m);
+      a.out_scale = 1.0 / (double)(h->masked ? h->m_active : h->m_eff);
       a.err = sc.err;
       a.trace = p->tracing ? p->trace.as<unsigned long long>() : nullptr;
       const unsigned grid = (unsigned)(h->n_pad / kRows);

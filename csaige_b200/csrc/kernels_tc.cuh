@@ -8,6 +8,11 @@ namespace saige {
 Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
                   cudaStream_t st);
 void tc_destroy(saige_grm* h);
+// Streamed build: reserves the code tiles for up to rows_cap marker rows (the
+// sample-major tiles keep that many marker tiles per sample tile), then builds the
+// tiles of marker tiles [mt0, mt1) from h->geno as those rows are complete.
+Status tc_stream_begin(saige_grm* h, int64_t rows_cap);
+Status tc_stream_tiles(saige_grm* h, int64_t mt0, int64_t mt1, cudaStream_t st);
 // Trial launches the ring-shape autotuner has timed in this process.
 int64_t tc_autotune_trials();
 

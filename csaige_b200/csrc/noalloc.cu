@@ -70,7 +70,7 @@ struct CurrentDevice {
 
 Status matvec_noalloc(saige_grm* h, const double* v, double* out, int64_t n, int nrhs,
                       cudaStream_t st) {
-  if (h->m == 0) {  // pcg.rs:132-134: no markers -> zero vector
+  if (h->m_eff == 0) {  // pcg.rs:132-134: no markers -> zero vector
     SG_CUDA(cudaMemsetAsync(out, 0, (size_t)n * nrhs * sizeof(double), st));
     return Status();
   }
@@ -88,7 +88,7 @@ Status matvec_noalloc(saige_grm* h, const double* v, double* out, int64_t n, int
   float* v32 = reinterpret_cast<float*>(base);
   float* u32 = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + v_bytes);
   float* ypart = reinterpret_cast<float*>(static_cast<unsigned char*>(base) + v_bytes + u_bytes);
-  const float scale = 1.0f / (float)h->m;
+  const float scale = 1.0f / (float)h->m_eff;
   for (int c = 0; c < nrhs; ++c) {
     const double* vc = v + (int64_t)c * n;
     double* oc = out + (int64_t)c * n;

@@ -249,7 +249,7 @@ cudaError_t learn_to_cols(const float* y, int64_t n, int64_t ld, int q, double* 
 }
 
 Status grm_diag(saige_grm* h, double* out, cudaStream_t st) {
-  const int64_t m_used = h->masked ? h->m_active : h->m;
+  const int64_t m_used = h->masked ? h->m_active : h->m_eff;
   const double scale = m_used > 0 ? 1.0 / (double)m_used : 0.0;
   grm_diag_kernel<<<(unsigned)ceil_div(h->n, 256), 256, 0, st>>>(
       h->geno, h->wpr, h->two_p, h->inv_s, h->masked ? h->excl.as<uint8_t>() : nullptr, h->m, h->n,

@@ -148,22 +148,36 @@ def test_fit_null_outputs_written_and_read_back(tmp_path):
     assert open(vr_path).read().endswith(" null 1\n")
 
 
-def test_pinned_upload_path_gives_the_same_fit():
-    # from pinned host memory the .bed is uploaded in chunks with the counts overlapped
+@pytest.mark.parametrize("subset,trait", [(False, cs.TraitType.Binary),
+                                           (True, cs.TraitType.Binary),
+                                           (True, cs.TraitType.Quantitative)])
+def test_pinned_upload_path_gives_the_same_fit(subset, trait):
+    # from pinned host memory a MIXED fit builds its GRM while the .bed streams in: the
+    # rows are all QC-passing markers, the variance-ratio candidates kept with zero 2p
+    # and 1/s; the products are exact integers, so the fit and the ratio must equal
+    # those of the steps on pageable memory (GRM markers only) bit for bit
     import torch
     n, m = 1500, 2500
-    spec = cs.CohortSpec(n=n, m=m, seed=31, missing_rate=0.02, prevalence=0.2, h2=0.3, n_covar=2)
+    spec = cs.CohortSpec(n=n, m=m, seed=31, missing_rate=0.02, prevalence=0.2, h2=0.3, n_covar=2,
+                         trait=trait)
     bed = cs.gen_bed(spec)
     y, x = cs.gen_pheno(spec)
+    sidx = None
+    if subset:
+        sidx = np.sort(np.random.default_rng(3).choice(n, 1201, replace=False))
+        y, x = y[sidx], x[sidx]
     pinned = torch.empty(bed.size, dtype=torch.uint8, pin_memory=True)
     pinned.numpy()[:] = bed
     cfg = cs.AiRemlConfig(max_iter=4, precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
                           warm_start=cs.WARM_RECYCLED)
-    a = cs.fit_null_from_bed(bed, n, m, y, x, cs.TraitType.Binary, cfg, variance_ratio=True)
-    b = cs.fit_null_from_bed(pinned.numpy(), n, m, y, x, cs.TraitType.Binary, cfg,
-                             variance_ratio=True)
+    # a MAF filter that drops markers in every chunk
+    kw = dict(sample_idx=sidx, min_maf=0.05, variance_ratio=True)
+    a = cs.fit_null_from_bed(bed, n, m, y, x, trait, cfg, **kw)
+    b = cs.fit_null_from_bed(pinned.numpy(), n, m, y, x, trait, cfg, **kw)
+    assert 0 < a.m_grm < m - a.m_vr
     assert (a.m_grm, a.m_vr) == (b.m_grm, b.m_vr)
     assert np.array_equal(a.ai_reml.tau, b.ai_reml.tau)
+    assert np.array_equal(a.ai_reml.alpha, b.ai_reml.alpha)
     assert a.variance_ratio.variance_ratio == b.variance_ratio.variance_ratio
 
 
