@@ -193,6 +193,15 @@ static void marker_meta(const double* af, int64_t m, int64_t m_pad, std::vector<
   }
 }
 
+// zlut, two_p and inv_s for `rows` marker rows in one block (from the buffer cache)
+static Status grm_alloc_meta(saige_grm* h, int64_t rows) {
+  SG_TRY(h->meta_buf.reserve((size_t)rows * (sizeof(float4) + 2 * sizeof(double))));
+  h->zlut = h->meta_buf.as<float4>();
+  h->two_p = reinterpret_cast<double*>(h->zlut + rows);
+  h->inv_s = h->two_p + rows;
+  return Status();
+}
+
 static Status grm_alloc(saige_grm* h, int64_t n, int64_t m) {
   h->n = n;
   h->n_pad = round_up(std::max<int64_t>(n, 1), kSamplePad);
@@ -203,9 +212,7 @@ static Status grm_alloc(saige_grm* h, int64_t n, int64_t m) {
   SG_CUDA(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   SG_TRY(h->geno_buf.reserve((size_t)h->m_pad * h->wpr * 4));
   h->geno = h->geno_buf.as<uint32_t>();
-  SG_CUDA(cudaMalloc(&h->zlut, (size_t)h->m_pad * sizeof(float4)));
-  SG_CUDA(cudaMalloc(&h->two_p, (size_t)h->m_pad * sizeof(double)));
-  SG_CUDA(cudaMalloc(&h->inv_s, (size_t)h->m_pad * sizeof(double)));
+  SG_TRY(grm_alloc_meta(h, h->m_pad));
   // padding rows: all codes 11 (genotype 0, not missing); their 1/s and 2p are 0
   SG_CUDA(cudaMemsetAsync(h->geno + (size_t)m * h->wpr, 0xFF,
                           (size_t)(h->m_pad - m) * h->wpr * 4, h->stream));
@@ -249,9 +256,9 @@ static void grm_free(saige_grm* h) {
   h->ws_io.release();
   h->geno_buf.release();
   h->geno = nullptr;
-  if (h->zlut) cudaFree(h->zlut);
-  if (h->two_p) cudaFree(h->two_p);
-  if (h->inv_s) cudaFree(h->inv_s);
+  h->meta_buf.release();
+  h->zlut = nullptr;
+  h->two_p = h->inv_s = nullptr;
   if (h->stream) cudaStreamDestroy(h->stream);
   delete h;
 }
@@ -873,9 +880,7 @@ Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, in
     ss.k = h->stream;
     SG_TRY(h->geno_buf.reserve((size_t)cap * h->wpr * 4));
     h->geno = h->geno_buf.as<uint32_t>();
-    SG_CUDA(cudaMalloc(&h->zlut, (size_t)cap * sizeof(float4)));
-    SG_CUDA(cudaMalloc(&h->two_p, (size_t)cap * sizeof(double)));
-    SG_CUDA(cudaMalloc(&h->inv_s, (size_t)cap * sizeof(double)));
+    SG_TRY(grm_alloc_meta(h, cap));
     SG_TRY(tc_stream_begin(h, cap));
     // all[j] = j (the rows the counts read), prow (the passing rows, in .bed order),
     // cnt (alt and missing counts per marker)

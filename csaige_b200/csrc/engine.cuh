@@ -18,7 +18,7 @@ namespace saige {
 // reserve() reuses a cached block of the same device of 1 to 1.25 times the size,
 // so that repeated fits of one cohort shape do not map and unmap tens of GB each
 // time.  release_cached_blocks() hands the cache back to the driver.
-constexpr size_t kCacheMinBytes = (size_t)16 << 20;
+constexpr size_t kCacheMinBytes = (size_t)1 << 20;
 
 struct DevBuf {
   void* ptr = nullptr;
@@ -72,6 +72,7 @@ struct saige_grm {
   int64_t m_eff = 0;
   uint32_t* geno = nullptr;           // m_pad x wpr packed 2-bit codes (in geno_buf)
   saige::DevBuf geno_buf;
+  saige::DevBuf meta_buf;             // holds zlut, two_p and inv_s
   float4* zlut = nullptr;             // per marker: f32 z for codes 00,01,10,11
   double* two_p = nullptr;            // per marker 2p (0 for padding)
   double* inv_s = nullptr;            // per marker 1/sqrt(2p(1-p)) (0 when degenerate / padding)

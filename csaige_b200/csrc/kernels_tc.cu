@@ -76,7 +76,8 @@ struct TcArgs {
   int nk;                   // pipeline stages over K
   int sub;                  // 128-entry sub-stages per load stage (1, 2 or 4)
   int sl;                   // load-ring depth in load stages (>= 2)
-  int sa;                   // TMEM operand slots, one per sub-stage (even)
+  int sa;                   // TMEM operand slots, one per sub-stage (a multiple of 2 hb)
+  int hb;                   // sub-stages per handoff to the MMA warp (1 or 2)
   const uint8_t* tiles;     // this pass's code tiles, tile t at (t*tile_ld + k)*4 KB
   int64_t tile_ld;          // tiles from one output tile's row of tiles to the next (>= nk)
   const uint8_t* img_g;     // nk x ng x 128 bytes
@@ -338,7 +339,9 @@ __device__ __forceinline__ void expand_word(uint32_t w, uint32_t* g, uint32_t* m
   m[3] = __byte_perm(kLutM, 0u, hi2);
 }
 
-template <bool kPassB>
+// kHb: sub-stages per handoff (a.hb), a template parameter so that the batch loops
+// unroll to straight-line code.
+template <bool kPassB, int kHb>
 __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -413,37 +416,47 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
     // Ring positions advance incrementally: no division in the loop.
     const uint32_t idesc = i8_idesc(a.ng);
     int t = 0, s = 0, ab = 0;  // sub-stage within the load stage, load slot, operand slot
-    for (int k = 0; k < a.nk; ++k) {
-      // trace stores come from lane 1: a memory access by the issuing lane would drain its MMAs
+    // One named-barrier handoff per batch of hb sub-stages (slots ab .. ab + hb - 1,
+    // barrier 1 + ab / hb): the warp waits once, then lane 0 issues the whole batch.
+    for (int k = 0; k < a.nk;) {
       if (lane == 1) {
         trace_mark(a, k, 6);  // MMA warp reaches the stage
         if (a.trace && blockIdx.x == 0 && k < kTraceStages)
           a.trace[k * kTraceSlots + 7] = (unsigned long long)clock64();  // SM clock at the same point
       }
-      named_bar_sync(1 + ab, kHandoffThreads);
+      named_bar_sync(1 + (ab >> (kHb - 1)), kHandoffThreads);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (lane == 1) trace_mark(a, k, 4);  // MMA may issue
-      if (lane == 0) {
-        const uint64_t bg = sw128_desc(P.B_g(s, t));
-        const uint64_t bm = kPassB ? sw128_desc(P.B_m(s, t)) : bg;
-        const uint32_t ag = tmem_a + (uint32_t)ab * kSlotCols, am = ag + 32u;
+      const int k_batch = k;
 #pragma unroll
-        for (int kk = 0; kk < kKt / 32; ++kk) {
-          // K advance of 32 int8: 8 TMEM columns of A, 32 bytes (2 x 16 B) along a B row
-          const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
-          mma_i8_ts(tmem_g, ag + 8u * kk, bg + 2u * kk, idesc, acc);
-          mma_i8_ts(tmem_m, am + 8u * kk, bm + 2u * kk, idesc, acc);
+      for (int j = 0; j < kHb; ++j, ++k) {
+        if (kHb > 1 && k >= a.nk) break;
+        if (lane == 0) {
+          // genotype and missing-flag MMAs alternate (two independent accumulators
+          // pipeline; grouping each accumulator's MMAs measured 15-40 % slower), and
+          // each sub-stage is committed as soon as its MMAs are issued, so that its
+          // operand and load slots free up one sub-stage earlier than a batch commit
+          const uint64_t bg = sw128_desc(P.B_g(s, t));
+          const uint64_t bm = kPassB ? sw128_desc(P.B_m(s, t)) : bg;
+          const uint32_t ag = tmem_a + (uint32_t)ab * kSlotCols, am = ag + 32u;
+#pragma unroll
+          for (int kk = 0; kk < kKt / 32; ++kk) {
+            // K advance of 32 int8: 8 TMEM columns of A, 32 bytes (2 x 16 B) along a B row
+            const uint32_t acc = (k > 0 || kk > 0) ? 1u : 0u;
+            mma_i8_ts(tmem_g, ag + 8u * kk, bg + 2u * kk, idesc, acc);
+            mma_i8_ts(tmem_m, am + 8u * kk, bm + 2u * kk, idesc, acc);
+          }
+          mma_commit(P.ADONE(ab));
+          if (t == a.sub - 1 || k == a.nk - 1) mma_commit(P.LDONE(s));
         }
-        mma_commit(P.ADONE(ab));
-        if (t == a.sub - 1 || k == a.nk - 1) mma_commit(P.LDONE(s));
+        if (++t == a.sub) {
+          t = 0;
+          if (++s == a.sl) s = 0;
+        }
+        if (++ab == a.sa) ab = 0;
       }
       __syncwarp();
-      if (lane == 1) trace_mark(a, k, 5);  // MMAs issued
-      if (++t == a.sub) {
-        t = 0;
-        if (++s == a.sl) s = 0;
-      }
-      if (++ab == a.sa) ab = 0;
+      if (lane == 1) trace_mark(a, k_batch, 5);  // MMAs issued
     }
     if (lane == 0) mma_commit(P.ACCF());
   } else {
@@ -456,47 +469,62 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
     const int row = lg * 32 + lane;
     const uint32_t lane_off = (uint32_t)(lg * 32) << 16;
     bool live = true;  // false once a wait gave up: the remaining stages only hand over
-    // ring positions of sub-stage k, advanced incrementally by 2 (no division in the loop)
-    int t = grp % a.sub, s = (grp / a.sub) % a.sl, ab = grp;
-    uint32_t ph_l = (uint32_t)((grp / a.sub) / a.sl) & 1u;  // phase parity of FULL(s) for k
-    uint32_t ph_a = 0;                                        // (k / sa) & 1
-    for (int k = grp; k < a.nk; k += 2) {
-      if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err);
-      if (live && row == 0) trace_mark(a, k, 1);  // codes landed
-      // operand slot ab is free once the MMAs of its previous use (sub-stage k - sa) completed
-      if (live && k >= a.sa) live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err);
-      live = __all_sync(0xffffffffu, live);  // warp-uniform: the barrier calls below must agree
-      if (live) {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (row == 0) trace_mark(a, k, 2);  // operand slot free
-        const uint32_t crow = P.CODES(s, t) + (uint32_t)row * 32u;
-        const uint4 c0 = lds128(crow), c1 = lds128(crow + 16u);
-        const uint32_t words[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
-        uint32_t g[32], m[32];
-#pragma unroll
-        for (int c = 0; c < 8; ++c) expand_word(words[c], g + 4 * c, m + 4 * c);
-        const uint32_t slot = tmem_a + lane_off + (uint32_t)ab * kSlotCols;
-        tmem_st32(slot, g);
-        tmem_st32(slot + 32u, m);
-        tmem_wait_st();
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        if (row == 0) trace_mark(a, k, 3);  // unpack done
-      }
-      // Every sub-stage is handed over, also after an abort, so that the MMA warp
-      // never waits for an arrival that does not come.  While live, the wait on
-      // ADONE of sub-stage k - sa keeps this group at most one use ahead of the
-      // MMA warp on each named barrier; after an abort bar.sync does that instead.
-      if (live)
-        named_bar_arrive(1 + ab, kHandoffThreads);
-      else
-        named_bar_sync(1 + ab, kHandoffThreads);
-      t += 2;
-      while (t >= a.sub) {
-        t -= a.sub;
+    // Group g takes the batches b = g, g + 2, ... of hb sub-stages (sub-stages b hb ..
+    // b hb + hb - 1).  Ring positions of the current sub-stage advance one sub-stage at
+    // a time (no division in the loop).
+    constexpr int hb = kHb;
+    int t = 0, s = 0, ab = 0;
+    uint32_t ph_l = 0;  // phase parity of FULL(s) for the current sub-stage
+    uint32_t ph_a = 0;  // (k / sa) & 1
+    auto step = [&]() {
+      if (++t == a.sub) {
+        t = 0;
         if (++s == a.sl) { s = 0; ph_l ^= 1u; }
       }
-      ab += 2;
-      if (ab >= a.sa) { ab -= a.sa; ph_a ^= 1u; }
+      if (++ab == a.sa) { ab = 0; ph_a ^= 1u; }
+    };
+    for (int j = 0; j < grp * hb; ++j) step();
+    for (int kb = grp * hb; kb < a.nk; kb += 2 * hb) {
+      const int bar = 1 + (ab >> (hb - 1));  // the batch's named barrier
+#pragma unroll
+      for (int j = 0; j < hb; ++j) {
+        const int k = kb + j;
+        if (hb == 1 || k < a.nk) {
+          if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err);
+          if (live && row == 0) trace_mark(a, k, 1);  // codes landed
+          // operand slot ab is free once the MMAs of its previous use (sub-stage k - sa)
+          // completed
+          if (live && k >= a.sa) live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err);
+          live = __all_sync(0xffffffffu, live);  // warp-uniform: the barrier calls below must agree
+          if (live) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (row == 0) trace_mark(a, k, 2);  // operand slot free
+            const uint32_t crow = P.CODES(s, t) + (uint32_t)row * 32u;
+            const uint4 c0 = lds128(crow), c1 = lds128(crow + 16u);
+            const uint32_t words[8] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w};
+            uint32_t g[32], m[32];
+#pragma unroll
+            for (int c = 0; c < 8; ++c) expand_word(words[c], g + 4 * c, m + 4 * c);
+            const uint32_t slot = tmem_a + lane_off + (uint32_t)ab * kSlotCols;
+            tmem_st32(slot, g);
+            tmem_st32(slot + 32u, m);
+            tmem_wait_st();
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            if (row == 0) trace_mark(a, k, 3);  // unpack done
+          }
+        }
+        step();
+      }
+      // Every batch is handed over, also after an abort, so that the MMA warp never
+      // waits for an arrival that does not come.  While live, the wait on ADONE of the
+      // slots' previous use keeps this group at most one use ahead of the MMA warp on
+      // its named barrier; after an abort bar.sync does that instead.
+      if (live)
+        named_bar_arrive(bar, kHandoffThreads);
+      else
+        named_bar_sync(bar, kHandoffThreads);
+#pragma unroll
+      for (int j = 0; j < hb; ++j) step();  // the other group's batch
     }
     // ---------------- epilogue: two warps per TMEM lane group ----------------
     __syncwarp();
@@ -748,22 +776,37 @@ __global__ void __launch_bounds__(128)
 // permutes — and apply the same FP64 epilogue, so their results are bit-identical
 // to the tensor-core path's.
 // ---------------------------------------------------------------------------
-// byte_perm tables indexed by the 2-bit code: genotype (00 -> 2, 01 -> 0 (missing),
-// 10 -> 1, 11 -> 0) and missing flag (01 -> 1)
-constexpr uint32_t kLutGeno = 0x00010002u;
-constexpr uint32_t kLutMiss = 0x00000100u;
+// prmt tables of the NEGATED genotype (codes 00, 01, 10, 11 -> -2, 0, -1, 0) and of
+// the missing flag (01 -> 1).  A selector nibble holds the code either in its bits
+// 0-1 (value c: byte c of x) or in its bits 2-3 (value 4c: byte 0 or byte 4 (y),
+// sign-replicated when the code's high bit is set — 10 gives sign(x.byte0), 11
+// sign(y.byte0)); both tables give the right byte in both positions, so the
+// selectors need masks but no shifts.
+constexpr uint32_t kNegGenoX = 0x00FF00FEu, kNegGenoY = 0u;
+constexpr uint32_t kMissX = 0x00000100u, kMissY = 0x00000001u;
 constexpr int kSrWarpMarkers = 8;                        // pass A: markers per warp
 constexpr int kSrBlockMarkers = 8 * kSrWarpMarkers;      // pass A: markers per block
 constexpr int kSrWords = 256;                            // pass A: sample words staged per round
 constexpr int kSrChunk = 2048;  // markers of limb planes staged per pass-B round
+static_assert(kSamplePad % 256 == 0, "pass B of one column takes sample tiles in pairs");
+
+__device__ __forceinline__ uint32_t prmt(uint32_t x, uint32_t y, uint32_t sel) {
+  uint32_t d;
+  asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(x), "r"(y), "r"(sel));
+  return d;
+}
 
 // The four 4-entry groups of a packed word (device layout: entry 4j+i at bit
-// 16(j>>1) + 2(j&1) + 4i) as byte-permute selectors; group g = entries 4g..4g+3.
-__device__ __forceinline__ void sr_selectors(uint32_t w, uint32_t sel[4]) {
-  sel[0] = w & 0x3333u;
-  sel[1] = (w >> 2) & 0x3333u;
-  sel[2] = (w >> 16) & 0x3333u;
-  sel[3] = (w >> 18) & 0x3333u;
+// 16(j>>1) + 2(j&1) + 4i; group g = entries 4g..4g+3) as four bytes each of -g and
+// of the missing flag.
+__device__ __forceinline__ void sr_expand(uint32_t w, int neg_g[4], int miss[4]) {
+  const uint32_t hi = w >> 16;
+  const uint32_t sel[4] = {w & 0x3333u, w & 0xCCCCu, hi & 0x3333u, hi & 0xCCCCu};
+#pragma unroll
+  for (int g = 0; g < 4; ++g) {
+    neg_g[g] = (int)prmt(kNegGenoX, kNegGenoY, sel[g]);
+    miss[g] = (int)prmt(kMissX, kMissY, sel[g]);
+  }
 }
 
 // q = rint(x / scale) as in quant_v_kernel, into three int8 planes (l2, l1, l0) of
@@ -880,12 +923,11 @@ __global__ void __launch_bounds__(256, 2)
       const int l0[4] = {(int)a0.x, (int)a0.y, (int)a0.z, (int)a0.w};
 #pragma unroll
       for (int k = 0; k < kSrWarpMarkers; ++k) {
-        uint32_t sel[4];
-        sr_selectors(w[k], sel);
+        int gbs[4], mbs[4];
+        sr_expand(w[k], gbs, mbs);
 #pragma unroll
         for (int g = 0; g < 4; ++g) {
-          const int gb = (int)__byte_perm(kLutGeno, 0u, sel[g]);
-          const int mb = (int)__byte_perm(kLutMiss, 0u, sel[g]);
+          const int gb = gbs[g], mb = mbs[g];
           acc[k][0] = __dp4a(gb, l2[g], acc[k][0]);
           acc[k][1] = __dp4a(gb, l1[g], acc[k][1]);
           acc[k][2] = __dp4a(gb, l0[g], acc[k][2]);
@@ -906,15 +948,17 @@ __global__ void __launch_bounds__(256, 2)
   for (int k = 0; k < kSrWarpMarkers; ++k) {
     if (lane != k) continue;
     const int64_t m = m0 + k;
-    const double G = 65536.0 * (double)acc[k][0] + 256.0 * (double)acc[k][1] + (double)acc[k][2];
+    // the genotype sums were formed with -g
+    const double G = -(65536.0 * (double)acc[k][0] + 256.0 * (double)acc[k][1] + (double)acc[k][2]);
     const double Mi = 65536.0 * (double)acc[k][3] + 256.0 * (double)acc[k][4] + (double)acc[k][5];
     const double tt = __dsub_rn(G, __dmul_rn(two_p[m], S - Mi));
     u[m] = __dmul_rn(inv_s[m], __dmul_rn(scale_v[0], tt));
   }
 }
 
-// Pass B of one column: block = one 128-sample tile of tiles_s, thread = sample.  The
-// marker limb planes are staged in shared memory kSrChunk markers at a time.
+// Pass B of one column: block = two 128-sample tiles of tiles_s, thread = one sample of
+// each (the limb words it loads serve both).  The marker limb planes are staged in
+// shared memory kSrChunk markers at a time.
 __global__ void __launch_bounds__(128)
     sr_pass_b_kernel(const uint8_t* __restrict__ tiles_s, int64_t n_mt, int64_t s_ld,
                      const int8_t* __restrict__ planes, int64_t m_pad,
@@ -922,9 +966,13 @@ __global__ void __launch_bounds__(128)
                      const double* __restrict__ scale_w, const double* __restrict__ scale_c,
                      double out_scale, double* __restrict__ out) {
   __shared__ __align__(16) int8_t sp[6][kSrChunk];
-  const int64_t st = blockIdx.x;
+  const int64_t st0 = 2 * (int64_t)blockIdx.x;
   const int r = threadIdx.x;
-  int acc[6] = {0, 0, 0, 0, 0, 0};
+  int acc[2][6];
+#pragma unroll
+  for (int h = 0; h < 2; ++h)
+#pragma unroll
+    for (int e = 0; e < 6; ++e) acc[h][e] = 0;
   for (int64_t mt0 = 0; mt0 < n_mt; mt0 += kSrChunk / 128) {
     const int64_t base = mt0 * 128;
     const int64_t len = m_pad - base < kSrChunk ? m_pad - base : (int64_t)kSrChunk;
@@ -939,15 +987,18 @@ __global__ void __launch_bounds__(128)
     __syncthreads();
     const int64_t mt_end = mt0 + kSrChunk / 128 < n_mt ? mt0 + kSrChunk / 128 : n_mt;
     for (int64_t mt = mt0; mt < mt_end; ++mt) {
-      const uint4* row = reinterpret_cast<const uint4*>(tiles_s + (st * s_ld + mt) * kTileBytes +
-                                                        (int64_t)r * 32);
-      const uint4 h0 = __ldg(row), h1 = __ldg(row + 1);
-      const uint32_t words[8] = {h0.x, h0.y, h0.z, h0.w, h1.x, h1.y, h1.z, h1.w};
+      uint32_t words[2][8];
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const uint4* row = reinterpret_cast<const uint4*>(
+            tiles_s + ((st0 + h) * s_ld + mt) * kTileBytes + (int64_t)r * 32);
+        const uint4 h0 = __ldg(row), h1 = __ldg(row + 1);
+        words[h][0] = h0.x; words[h][1] = h0.y; words[h][2] = h0.z; words[h][3] = h0.w;
+        words[h][4] = h1.x; words[h][5] = h1.y; words[h][6] = h1.z; words[h][7] = h1.w;
+      }
       const int off = (int)(mt - mt0) * 128;
 #pragma unroll
       for (int j = 0; j < 8; ++j) {
-        uint32_t sel[4];
-        sr_selectors(words[j], sel);
         const int mk = off + 16 * j;
         const uint4 w2 = *reinterpret_cast<const uint4*>(sp[0] + mk);
         const uint4 w1 = *reinterpret_cast<const uint4*>(sp[1] + mk);
@@ -962,30 +1013,38 @@ __global__ void __launch_bounds__(128)
         const int C1[4] = {(int)c1.x, (int)c1.y, (int)c1.z, (int)c1.w};
         const int C0[4] = {(int)c0.x, (int)c0.y, (int)c0.z, (int)c0.w};
 #pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          const int gb = (int)__byte_perm(kLutGeno, 0u, sel[g]);
-          const int mb = (int)__byte_perm(kLutMiss, 0u, sel[g]);
-          acc[0] = __dp4a(gb, W2[g], acc[0]);
-          acc[1] = __dp4a(gb, W1[g], acc[1]);
-          acc[2] = __dp4a(gb, W0[g], acc[2]);
-          acc[3] = __dp4a(mb, C2[g], acc[3]);
-          acc[4] = __dp4a(mb, C1[g], acc[4]);
-          acc[5] = __dp4a(mb, C0[g], acc[5]);
+        for (int h = 0; h < 2; ++h) {
+          int gbs[4], mbs[4];
+          sr_expand(words[h][j], gbs, mbs);
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            acc[h][0] = __dp4a(gbs[g], W2[g], acc[h][0]);
+            acc[h][1] = __dp4a(gbs[g], W1[g], acc[h][1]);
+            acc[h][2] = __dp4a(gbs[g], W0[g], acc[h][2]);
+            acc[h][3] = __dp4a(mbs[g], C2[g], acc[h][3]);
+            acc[h][4] = __dp4a(mbs[g], C1[g], acc[h][4]);
+            acc[h][5] = __dp4a(mbs[g], C0[g], acc[h][5]);
+          }
         }
       }
     }
   }
-  const double G = 65536.0 * (double)acc[0] + 256.0 * (double)acc[1] + (double)acc[2];
-  const double Mi = 65536.0 * (double)acc[3] + 256.0 * (double)acc[4] + (double)acc[5];
   const double S = (double)(long long)sum_c[0];
-  out[st * 128 + r] =
-      __dmul_rn(out_scale, __dsub_rn(__dmul_rn(scale_w[0], G), __dmul_rn(scale_c[0], S - Mi)));
+#pragma unroll
+  for (int h = 0; h < 2; ++h) {
+    // the genotype sums were formed with -g
+    const double G =
+        -(65536.0 * (double)acc[h][0] + 256.0 * (double)acc[h][1] + (double)acc[h][2]);
+    const double Mi = 65536.0 * (double)acc[h][3] + 256.0 * (double)acc[h][4] + (double)acc[h][5];
+    out[(st0 + h) * 128 + r] = __dmul_rn(
+        out_scale, __dsub_rn(__dmul_rn(scale_w[0], G), __dmul_rn(scale_c[0], S - Mi)));
+  }
 }
 
 size_t tc_fixed_bytes() { return 1024 + 8 * (2 * kMaxSL + kMaxSA + 1) + 16; }
 
 struct Rings {
-  int sub, sl, sa;
+  int sub, sl, sa, hb;
 };
 
 // Ring shapes for a launch: load stages of up to four sub-stages (16 KB of
@@ -1000,6 +1059,8 @@ Rings tc_rings(int ng, bool pass_b) {
   while (g.sub > 1 && 2 * (size_t)plan_l_stage(ng, pass_b, g.sub) > room) g.sub >>= 1;
   g.sl = (int)std::min<size_t>(kMaxSL, room / plan_l_stage(ng, pass_b, g.sub));
   g.sa = std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols)) & ~1;
+  // one sub-stage per handoff (two, a tuner candidate, measured 1-5 % slower)
+  g.hb = 1;
   return g;
 }
 
@@ -1074,7 +1135,8 @@ static Status tc_plan_new(TcPlan** out) {
     delete p;
     return s;
   };
-  for (auto kern : {tc_grm_kernel<false>, tc_grm_kernel<true>}) {
+  for (auto kern : {tc_grm_kernel<false, 1>, tc_grm_kernel<true, 1>, tc_grm_kernel<false, 2>,
+                    tc_grm_kernel<true, 2>}) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSmemBudget);
     if (e != cudaSuccess)
@@ -1162,12 +1224,16 @@ static Scal carve(TcPlan* p) {
 
 template <bool kPassB>
 static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
-  if (a.sa < 2 || (a.sa & 1) || a.sa > kMaxSA || a.sl < 2 || a.sl > kMaxSL || a.sub < 1 ||
+  if (a.hb < 1 || a.hb > 2 || a.sa < 2 * a.hb || a.sa % (2 * a.hb) || a.sa > kMaxSA ||
+      a.sl < 2 || a.sl > kMaxSL || a.sub < 1 ||
       a.sub > 4)
     return cudaErrorInvalidValue;
   const size_t smem = tc_fixed_bytes() + (size_t)a.sl * plan_l_stage(a.ng, kPassB, a.sub);
   if (smem > kSmemBudget) return cudaErrorInvalidValue;
-  tc_grm_kernel<kPassB><<<grid, kThreads, smem, st>>>(a);
+  if (a.hb == 2)
+    tc_grm_kernel<kPassB, 2><<<grid, kThreads, smem, st>>>(a);
+  else
+    tc_grm_kernel<kPassB, 1><<<grid, kThreads, smem, st>>>(a);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1177,7 +1243,8 @@ static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
 // does not change a product's result — the sums are exact integers and the epilogue
 // is per element — only its speed.  The first launch of each key — pass, ng and the
 // launch's size class (log2 of its 4 KB stages) — in the process times every shape that
-// fits (sub 4, 2, 1 with the deepest ring the shared memory holds) on the real operands
+// fits (sub 4, 2, 1 with the deepest ring the shared memory holds; one or two
+// sub-stages per handoff where four operand slots fit) on the real operands
 // and keeps the fastest; later launches of the key use it.  Launches of fewer than
 // kTuneMinStages stages keep the fixed choice of tc_rings (their trials would cost more
 // than they can save), as does SAIGE_TC_AUTOTUNE=0 (=2 tunes every size).  SAIGE_TIMING=1
@@ -1228,6 +1295,11 @@ std::vector<Rings> tc_candidates(int ng, bool pass_b) {
     g.sub = sub;
     g.sl = (int)std::min<size_t>(kMaxSL, room / ls);
     out.push_back(g);
+    if (g.sa >= 4) {  // the same ring with two sub-stages per handoff (four slots)
+      g.hb = 2;
+      g.sa = 4;
+      out.push_back(g);
+    }
   }
   return out;
 }
@@ -1245,6 +1317,7 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     a.sub = fixed.sub;
     a.sl = fixed.sl;
     a.sa = fixed.sa;
+    a.hb = fixed.hb;
     SG_CUDA(launch_tc<kPassB>(grid, a, st));
     return Status();
   }
@@ -1256,6 +1329,7 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
       a.sub = it->second.sub;
       a.sl = it->second.sl;
       a.sa = it->second.sa;
+      a.hb = it->second.hb;
       SG_CUDA(launch_tc<kPassB>(grid, a, st));
       return Status();
     }
@@ -1274,6 +1348,7 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     a.sub = g.sub;
     a.sl = g.sl;
     a.sa = g.sa;
+    a.hb = g.hb;
     cudaEventRecord(e0, st);
     const cudaError_t le = launch_tc<kPassB>(grid, a, st);
     if (le != cudaSuccess) {
@@ -1290,8 +1365,8 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     cudaEventElapsedTime(&ms, e0, e1);
     g_tune_trials += 1;
     if (log)
-      fprintf(stderr, "[saige tune] pass %c ng %d grid %u nk %d: sub %d sl %d -> %.3f ms\n",
-              kPassB ? 'B' : 'A', a.ng, grid, a.nk, g.sub, g.sl, ms);
+      fprintf(stderr, "[saige tune] pass %c ng %d grid %u nk %d: sub %d sl %d hb %d -> %.3f ms\n",
+              kPassB ? 'B' : 'A', a.ng, grid, a.nk, g.sub, g.sl, g.hb, ms);
     if (!have || ms < best_ms) {
       best = g;
       best_ms = ms;
@@ -1311,6 +1386,7 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     a.sub = best.sub;
     a.sl = best.sl;
     a.sa = best.sa;
+    a.hb = best.hb;
     SG_CUDA(launch_tc<kPassB>(grid, a, st));
   }
   return Status();
@@ -1382,7 +1458,8 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     sr_quant_wc_kernel<<<(unsigned)ceil_div(h->m_pad, 256), 256, 0, st>>>(
         u, h->m_pad, h->inv_s, h->two_p, sc.amax_w, sc.amax_c, sc.scale_w, sc.scale_c, planes_b,
         sc.sum_c);
-    sr_pass_b_kernel<<<(unsigned)(h->n_pad / kRows), kRows, 0, st>>>(
+    // two sample tiles per block (n_pad is a multiple of 512: an even tile count)
+    sr_pass_b_kernel<<<(unsigned)(h->n_pad / (2 * kRows)), kRows, 0, st>>>(
         p->tiles_s.as<uint8_t>(), h->m_pad / kRows, p->s_ld, planes_b, h->m_pad, sc.sum_c, sc.scale_w,
         sc.scale_c, 1.0 / (double)(h->masked ? h->m_active : h->m_eff), kp + (int64_t)cols[0] * h->n_pad);
     SG_CHECK_LAUNCH();
