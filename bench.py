@@ -56,7 +56,7 @@ CPU_SAMPLE_MARKERS = 32768
 # plus the vector-limb tiles), from the ncu capture at N=200,000, m_pad=18,048:
 # pass A 922.8 MB, pass B 928.5 MB.  Reads scale with m_pad; the output writes
 # (pass A: m_pad*R*8 bytes, pass B: N*R*8 bytes) are added per launch.
-TC_READ_PER_MARKER_ROW = {"A": 922.8e6 / 18048, "B": 928.5e6 / 18048}
+TC_READ_PER_MARKER_ROW = {"A": 929.2e6 / 18048, "B": 935.0e6 / 18048}
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # Explicit GRM (create-sparse-grm) workload: an FP64 SYRK over all sample pairs, so
