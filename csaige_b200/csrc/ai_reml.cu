@@ -166,6 +166,10 @@ struct Recycle {
   double *gam, *gpart, *gout;
   bool have_kblock = false, have_kpk = false, have_kpw = false;
   bool kv_ok = true;                    // every basis column of the current start has kv
+  // K [X | U] was formed (f.kxu).  Without it (the recycled block fit) [X | U] joins a
+  // basis only while tau1 = 0, where its Sigma-image needs no K, and the Hutchinson
+  // trace takes K P u from the block solutions' K-images.
+  bool kxu_ok = true;
   bool with_pw = false;                 // the fit has the W^-1 AI solve (quantitative)
   int64_t fallbacks = 0, kpy_launches_saved = 0;
   // learned correction (SAIGE_WARM_LEARNED): an MLP trained on the change of the
@@ -311,8 +315,11 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
   const int64_t ld = f.ld;
   int mb = 0;
   rc.kv_ok = true;
-  SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
-  mb += f.p + f.nrv;
+  if (rc.kxu_ok || tau[1] == 0.0) {
+    SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
+    mb += f.p + f.nrv;
+    if (!rc.kxu_ok) rc.kv_ok = false;  // zero stand-ins for K [X | U]: no K x0
+  }
   if (rc.have_kblock) {
     SG_TRY(basis_cols(f, rc, mb, f.sol, rc.kblock, f.q, tau));
     mb += f.q;
@@ -340,7 +347,8 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
     if (need_pw) rc.have_kpw = true;
   }
   if (ok)
-    return solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br, rc.kblock, rc.kx0, &kx_ok, ex);
+    return solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br, rc.kblock,
+                 rc.kv_ok ? rc.kx0 : nullptr, &kx_ok, ex);
   return solve(f, f.rhs, f.sol, x0_prev, f.q, tau, nullptr, rc.br, rc.kblock, nullptr, &kx_ok,
                ex);
 }
@@ -458,8 +466,11 @@ Status ai_solve_recycled(Fit& f, Recycle& rc, const double* b, double* x, double
   SG_TRY(copy_cols(f, rc.kblock, rc.kv, f.q));
   SG_CUDA(sub_cols(f.rhs, rc.br, rc.av, f.n, ld, f.q, f.st));
   mb += f.q;
-  SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
-  mb += f.p + f.nrv;
+  if (rc.kxu_ok || tau[1] == 0.0) {
+    SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
+    mb += f.p + f.nrv;
+    if (!rc.kxu_ok) rc.kv_ok = false;
+  }
   if (have) {
     SG_TRY(basis_cols(f, rc, mb, x, kx, 1, tau));
     mb += 1;
@@ -601,17 +612,23 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   double* U = f.rhs + (size_t)(1 + p) * ld;
   SG_CUDA(cudaMemcpy2DAsync(f.rhs + ld, (size_t)ld * 8, f.x, (size_t)ld * 8, (size_t)ld * 8,
                             (size_t)p, cudaMemcpyDeviceToDevice, f.st));
-  // K u is the same every iteration (K and the probes are fixed): one block product.
-  // Recycled starts also use K X, from the same launch (X and U are adjacent in rhs).
+  // K u is the same every iteration (K and the probes are fixed): one block product,
+  // with K X in the same launch for the learned start (X and U are adjacent in rhs).
+  // The recycled block fit forms neither: its trace takes K P u from the K-images of the
+  // block solutions (K P u = K Sinv U - K Sinv X coef, both kept beside the solutions),
+  // which saves the launch.
   tm.mark("  irls");
   const bool recyc = cfg->warm_start == SAIGE_WARM_RECYCLED || cfg->warm_start == SAIGE_WARM_LEARNED;
-  if (recyc)
+  const bool learned = cfg->warm_start == SAIGE_WARM_LEARNED && cfg->solve == SAIGE_SOLVE_BLOCK;
+  const bool ku_free = recyc && !learned && cfg->solve == SAIGE_SOLVE_BLOCK;
+  if (ku_free)
+    SG_CUDA(cudaMemsetAsync(f.kxu, 0, (size_t)(p + f.nrv) * ld * 8, f.st));
+  else if (recyc)
     SG_TRY(grm_product(h, f.rhs + ld, f.kxu, p + f.nrv, nullptr, cfg->precision, f.st));
   else
     SG_TRY(grm_product(h, U, f.ku, f.nrv, nullptr, cfg->precision, f.st));
   tm.mark("  Ku");
   // exact diag K: the DIAG_K preconditioner and a feature of the learned start (K8)
-  const bool learned = cfg->warm_start == SAIGE_WARM_LEARNED && cfg->solve == SAIGE_SOLVE_BLOCK;
   DevBuf diagk;
   if (cfg->precond == SAIGE_PRECOND_DIAG_K || learned) {
     SG_TRY(diagk.reserve((size_t)ld * 8));
@@ -621,6 +638,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
   const double* pre_diag = cfg->precond == SAIGE_PRECOND_DIAG_K ? diagk.as<double>() : nullptr;
   Recycle rc;
   if (recyc) SG_TRY(recycle_init(f, rc, learned, diagk.as<double>(), cfg->seed));
+  rc.kxu_ok = !ku_free;
   rc.with_pw = !(trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL);
 
   const bool fix_tau_e = trait == SAIGE_TRAIT_BINARY || trait == SAIGE_TRAIT_SURVIVAL;
@@ -689,7 +707,15 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     SG_TRY(copy_cols(f, SinvU, f.pu, f.nrv));
     SG_TRY(p_project(f, f.pu, U, f.nrv, l));
     std::vector<double> tr;
-    SG_TRY(coldots(f, f.ku, f.pu, f.nrv, tr));
+    if (rc.kxu_ok) {
+      SG_TRY(coldots(f, f.ku, f.pu, f.nrv, tr));  // (K u)' P u
+    } else {
+      // u' K P u with K P u = K Sinv U - K Sinv X coef (coef of the projection above,
+      // still in f.dsmall; rc.kblock = K [Sinv y | Sinv X | Sinv U] of this iteration)
+      SG_TRY(copy_cols(f, rc.kblock + (size_t)(1 + p) * ld, f.tmpq, f.nrv));
+      SG_CUDA(sub_combo(f.tmpq, f.nrv, rc.kblock + ld, p, f.dsmall, n, ld, f.st));
+      SG_TRY(coldots(f, U, f.tmpq, f.nrv, tr));
+    }
     double trace_sum = 0.0;
     for (int k = 0; k < f.nrv; ++k) trace_sum += tr[(size_t)k];
     const double trace_grm = trace_sum / (double)f.nrv;
