@@ -45,6 +45,12 @@ struct CachedBlock {
 std::mutex g_cache_mu;
 std::vector<CachedBlock> g_cache;
 
+// the streamed fit-null build's host-mapped block (see stream_fit_null_grm)
+std::mutex g_mapped_mu;
+void* g_mapped = nullptr;
+size_t g_mapped_bytes = 0;
+bool g_mapped_busy = false;
+
 // Takes the smallest cached block of `dev` with want <= bytes <= 1.25 want.
 bool cache_take(int dev, size_t want, void** ptr, size_t* bytes) {
   std::lock_guard<std::mutex> lk(g_cache_mu);
@@ -837,11 +843,40 @@ Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, in
     }
   };
   // Host-mapped memory for what crosses PCIe beside the .bed (row lists, counts): no
-  // copy of it queues behind the chunks on the copy engines.
+  // copy of it queues behind the chunks on the copy engines.  One block is kept for
+  // the process and reused (pinning and unpinning host memory on every call cost
+  // milliseconds, once close to a second); a call that finds it in use by another
+  // thread takes a block of its own.
   struct Mapped {
     void* p = nullptr;
+    bool own = false;
     ~Mapped() {
-      if (p) cudaFreeHost(p);
+      if (own) {
+        cudaFreeHost(p);
+      } else if (p) {
+        std::lock_guard<std::mutex> lk(g_mapped_mu);
+        g_mapped_busy = false;
+      }
+    }
+    Status take(size_t bytes) {
+      {
+        std::lock_guard<std::mutex> lk(g_mapped_mu);
+        if (!g_mapped_busy) {
+          if (g_mapped_bytes < bytes) {
+            if (g_mapped) cudaFreeHost(g_mapped);
+            g_mapped = nullptr;
+            g_mapped_bytes = 0;
+            SG_CUDA(cudaHostAlloc(&g_mapped, bytes, cudaHostAllocMapped));
+            g_mapped_bytes = bytes;
+          }
+          g_mapped_busy = true;
+          p = g_mapped;
+          return Status();
+        }
+      }
+      own = true;
+      SG_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocMapped));
+      return Status();
     }
   };
   PhaseTimer tm;
@@ -884,7 +919,7 @@ Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, in
     SG_TRY(tc_stream_begin(h, cap));
     // all[j] = j (the rows the counts read), prow (the passing rows, in .bed order),
     // cnt (alt and missing counts per marker)
-    SG_CUDA(cudaHostAlloc(&mp.p, (size_t)m_tot * 32, cudaHostAllocMapped));
+    SG_TRY(mp.take((size_t)m_tot * 32));
     int64_t* all_h = static_cast<int64_t*>(mp.p);
     int64_t* prow_h = all_h + m_tot;
     int64_t* cnt_h = prow_h + m_tot;
@@ -976,6 +1011,7 @@ Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, in
     return Status();
   };
   Status s = body();
+  tm.mark(" stream exit");
   if (!s.ok()) {
     grm_free(h);
     return s;
