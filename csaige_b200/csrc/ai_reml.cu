@@ -7,6 +7,7 @@
 #include <cstdlib>
 #include <chrono>
 #include <cstdlib>
+#include <thread>
 #include <vector>
 
 #include "engine.cuh"
@@ -823,11 +824,24 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     for (int64_t i = 0; i < n; ++i) ss += (yh[(size_t)i] - mu[(size_t)i]) * (yh[(size_t)i] - mu[(size_t)i]);
     ll = -0.5 * (double)n * log(2.0 * M_PI * tau[0]) - 0.5 * ss / tau[0];
   } else {
-    for (int64_t i = 0; i < n; ++i) {
-      double mi = mu[(size_t)i];
-      mi = mi < 1e-15 ? 1e-15 : (mi > 1.0 - 1e-15 ? 1.0 - 1e-15 : mi);
-      ll += yh[(size_t)i] * log(mi) + (1.0 - yh[(size_t)i]) * log(1.0 - mi);
-    }
+    // the terms on host threads (the logs are most of the time), summed in sample order
+    // as the reference does, so the value is the same bit for bit
+    std::vector<double> term((size_t)n);
+    auto terms = [&](int64_t i0, int64_t i1) {
+      for (int64_t i = i0; i < i1; ++i) {
+        double mi = mu[(size_t)i];
+        mi = mi < 1e-15 ? 1e-15 : (mi > 1.0 - 1e-15 ? 1.0 - 1e-15 : mi);
+        term[(size_t)i] = yh[(size_t)i] * log(mi) + (1.0 - yh[(size_t)i]) * log(1.0 - mi);
+      }
+    };
+    const int nt = n >= 65536 ? (int)std::min<unsigned>(16u, std::max(1u, std::thread::hardware_concurrency())) : 1;
+    std::vector<std::thread> pool;
+    const int64_t per = ceil_div(n, (int64_t)nt);
+    for (int t = 1; t < nt; ++t)
+      pool.emplace_back(terms, std::min<int64_t>(n, t * per), std::min<int64_t>(n, (t + 1) * per));
+    terms(0, std::min<int64_t>(n, per));
+    for (auto& th : pool) th.join();
+    for (int64_t i = 0; i < n; ++i) ll += term[(size_t)i];
   }
   tm.mark("  loglik");
   float ms = 0.f;
