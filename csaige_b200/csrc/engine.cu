@@ -93,7 +93,16 @@ size_t cache_flush(int dev) {
 }
 }  // namespace
 
-void release_cached_blocks() { cache_flush(-1); }
+void release_cached_blocks() {
+  cache_flush(-1);
+  // the streamed build's host-mapped block, unless a build is using it
+  std::lock_guard<std::mutex> lk(g_mapped_mu);
+  if (g_mapped && !g_mapped_busy) {
+    cudaFreeHost(g_mapped);
+    g_mapped = nullptr;
+    g_mapped_bytes = 0;
+  }
+}
 
 Status DevBuf::reserve(size_t want) {
   if (want <= bytes) return Status();

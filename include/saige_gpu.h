@@ -205,12 +205,14 @@ int32_t saige_write_null_model(const char* path, const saige_null_model* model);
  * (x n x p column-major, out p*n doubles). Host only. */
 int32_t saige_xvx_inv_xv(const double* x, const double* w, int64_t n, int32_t p, double* out);
 
-/* No counterpart in the reference (memory management).  Device buffers of 256 MiB
- * and more (packed genotypes, tiles, the uploaded .bed) are kept in a per-device
- * cache when released and reused by later allocations of 1 to 1.25 times their size,
- * so that repeated fits of one cohort shape skip mapping and unmapping tens of GB.
- * This call frees the cached blocks of every device.  The cache also gives its
- * blocks back by itself when an allocation would otherwise fail. */
+/* No counterpart in the reference (memory management).  Device buffers of 1 MiB
+ * and more (packed genotypes, tiles, the uploaded .bed, per-marker metadata and
+ * workspaces) are kept in a per-device cache when released and reused by later
+ * allocations of 1 to 1.25 times their size, so that repeated fits of one cohort
+ * shape skip mapping and unmapping tens of GB.  This call frees the cached blocks of
+ * every device and the pinned host block of saige_fit_null_from_bed's streamed build.
+ * The cache also gives its blocks back by itself when an allocation would otherwise
+ * fail. */
 int32_t saige_release_cached_memory(void);
 
 /* The Rademacher probe vectors of fit_ai_reml (saige-core/src/glmm/ai_reml.rs:121-130):
