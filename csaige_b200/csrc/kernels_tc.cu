@@ -786,7 +786,7 @@ constexpr uint32_t kNegGenoX = 0x00FF00FEu, kNegGenoY = 0u;
 constexpr uint32_t kMissX = 0x00000100u, kMissY = 0x00000001u;
 constexpr int kSrWarpMarkers = 8;                        // pass A: markers per warp
 constexpr int kSrBlockMarkers = 8 * kSrWarpMarkers;      // pass A: markers per block
-constexpr int kSrWords = 256;                            // pass A: sample words staged per round
+constexpr int kSrWords = 1024;                           // pass A: sample words staged per round
 constexpr int kSrChunk = 2048;  // markers of limb planes staged per pass-B round
 static_assert(kSamplePad % 256 == 0, "pass B of one column takes sample tiles in pairs");
 

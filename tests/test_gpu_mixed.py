@@ -141,12 +141,12 @@ def test_autotuned_ring_shapes_give_identical_products(monkeypatch):
     assert np.array_equal(fixed, tuned) and np.array_equal(tuned, again)
 
 
-@pytest.mark.parametrize("n,m,sub", [(1001, 300, False), (5000, 2300, False), (4500, 700, True)])
+@pytest.mark.parametrize("n,m,sub", [(1001, 300, False), (17000, 2300, False), (4500, 700, True)])
 def test_single_column_cuda_core_path_equals_tensor_core_path(monkeypatch, n, m, sub):
     # one active column runs both passes with dp4a on the CUDA cores: the same exact
     # integer sums and the same FP64 epilogue, so every bit agrees with the tensor-core
     # passes (SAIGE_SC=0) and with the CPU model; the sizes cross the staging chunks
-    # (256 sample words in pass A, 2048 markers in pass B)
+    # (1024 sample words in pass A, 2048 markers in pass B)
     rng = np.random.default_rng(n + m)
     sidx = rng.permutation(n)[: n - 37] if sub else None
     grm, bed, keep, afs = _case(n, m, sidx=sidx, miss=0.02)
