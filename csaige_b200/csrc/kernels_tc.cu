@@ -913,6 +913,7 @@ __global__ void __launch_bounds__(256, 2)
                          : make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
+#pragma unroll 2
     for (int t = lane; t < cn; t += 32) {
       uint32_t w[kSrWarpMarkers];
 #pragma unroll
