@@ -913,7 +913,7 @@ __global__ void __launch_bounds__(256, 2)
                          : make_uint4(0u, 0u, 0u, 0u);
     }
     __syncthreads();
-#pragma unroll 2
+#pragma unroll 4
     for (int t = lane; t < cn; t += 32) {
       uint32_t w[kSrWarpMarkers];
 #pragma unroll
@@ -987,6 +987,7 @@ __global__ void __launch_bounds__(128)
     }
     __syncthreads();
     const int64_t mt_end = mt0 + kSrChunk / 128 < n_mt ? mt0 + kSrChunk / 128 : n_mt;
+#pragma unroll 2
     for (int64_t mt = mt0; mt < mt_end; ++mt) {
       uint32_t words[2][8];
 #pragma unroll
