@@ -352,7 +352,8 @@ def _design(x, n: int) -> tuple[np.ndarray, int]:
         a = a.reshape(n, -1, order="F")
     if a.shape[0] != n:
         raise SaigeError(_lib.EINVAL, f"x.nrows() = {a.shape[0]} != n = {n}")
-    return np.asfortranarray(a).ravel(order="F").copy(), a.shape[1]
+    # column-major n x p, copied only when the layout differs (the library reads it)
+    return np.asfortranarray(a).ravel(order="F"), a.shape[1]
 
 
 def fit_ai_reml(y, x, grm: OnTheFlyGrm, trait_type: TraitType,
@@ -480,12 +481,13 @@ def gen_bed_dev(spec: CohortSpec, dev_ptr: int) -> None:
 
 
 def gen_pheno(spec: CohortSpec) -> tuple[np.ndarray, np.ndarray]:
-    """(y, x) with x n x (1 + n_covar), intercept first."""
+    """(y, x) with x n x (1 + n_covar), intercept first, column-major (the layout of
+    saige-rs's nalgebra matrices and of this library's C ABI)."""
     y = np.empty(spec.n)
     x = np.empty(spec.n * (1 + spec.n_covar))
     s = spec.c()
     check(LIB.saige_gen_pheno(C.byref(s), _dptr(y), _dptr(x)))
-    return y, x.reshape(1 + spec.n_covar, spec.n).T.copy()
+    return y, x.reshape(1 + spec.n_covar, spec.n).T
 
 
 # ---------------------------------------------------------------------------
