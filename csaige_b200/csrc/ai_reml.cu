@@ -579,12 +579,20 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
                             cudaMemcpyHostToDevice, f.st));
 
   // ---- GLM IRLS initialisation (ai_reml.rs:431-482) --------------------
-  std::vector<double> alpha((size_t)p, 0.0), anew((size_t)p), l, xtwx, xtwz;
+  std::vector<double> alpha((size_t)p, 0.0), anew((size_t)p), l, xtwx((size_t)p * p),
+      xtwz((size_t)p), xw;
   SG_CUDA(init_mu(f.y, trait, f.mu, f.eta, n, f.st));
+  // rhs = [ytil | X] while the IRLS runs, so that X'W ytil and X'W X come from one
+  // reduction (each entry's sum is the same as from two)
+  SG_CUDA(cudaMemcpy2DAsync(f.rhs + ld, (size_t)ld * 8, f.x, (size_t)ld * 8, (size_t)ld * 8,
+                            (size_t)p, cudaMemcpyDeviceToDevice, f.st));
   for (int it = 0; it < 25; ++it) {
-    SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, f.ytil, n, f.st));
-    SG_TRY(dots(f, f.x, p, f.x, p, f.w, xtwx));
-    SG_TRY(dots(f, f.x, p, f.ytil, 1, f.w, xtwz));
+    SG_CUDA(work_vectors(f.y, f.eta, f.mu, trait, f.w, f.rhs, n, f.st));
+    SG_TRY(dots(f, f.x, p, f.rhs, 1 + p, f.w, xw));
+    for (int j = 0; j < p; ++j) {
+      xtwz[(size_t)j] = xw[(size_t)j * (1 + p)];
+      for (int k = 0; k < p; ++k) xtwx[(size_t)j * p + k] = xw[(size_t)j * (1 + p) + 1 + k];
+    }
     // symmetric fill as dense.rs:227-245 (j <= k computed, mirrored)
     for (int j = 0; j < p; ++j)
       for (int k = j + 1; k < p; ++k) xtwx[(size_t)k * p + j] = xtwx[(size_t)j * p + k];
@@ -675,9 +683,13 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     tm.mark("  block");
 
     // X' Sigma^-1 X and X' Sigma^-1 y (ai_reml.rs:189-205)
-    std::vector<double> dxs, dxy;
-    SG_TRY(dots(f, f.x, p, SinvX, p, nullptr, dxs));  // dxs[j*p+k] = X_j . SinvX_k
-    SG_TRY(dots(f, f.x, p, SinvY, 1, nullptr, dxy));
+    // X' [Sinv y | Sinv X] in one reduction: dxy[j] = X_j . SinvY, dxs[j*p+k] = X_j . SinvX_k
+    std::vector<double> dxs((size_t)p * p), dxy((size_t)p), dall;
+    SG_TRY(dots(f, f.x, p, SinvY, 1 + p, nullptr, dall));
+    for (int j = 0; j < p; ++j) {
+      dxy[(size_t)j] = dall[(size_t)j * (1 + p)];
+      for (int k = 0; k < p; ++k) dxs[(size_t)j * p + k] = dall[(size_t)j * (1 + p) + 1 + k];
+    }
     std::vector<double> cmat((size_t)p * p);
     for (int j = 0; j < p; ++j)
       for (int k = j; k < p; ++k) {
