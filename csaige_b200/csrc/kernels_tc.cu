@@ -1057,8 +1057,12 @@ struct Rings {
 Rings tc_rings(int ng, bool pass_b) {
   Rings g;
   const size_t room = kSmemBudget - tc_fixed_bytes();
+  // the most sub-stages per load stage that still leave a ring of four load stages:
+  // at the bench size the autotuner's trials put the shapes with a 2-3 stage ring
+  // 2-25 % behind (pass B at 43-64 columns most), and no deeper ring of fewer
+  // sub-stages lost more than 1 %
   g.sub = 4;
-  while (g.sub > 1 && 2 * (size_t)plan_l_stage(ng, pass_b, g.sub) > room) g.sub >>= 1;
+  while (g.sub > 1 && room / plan_l_stage(ng, pass_b, g.sub) < 4) g.sub >>= 1;
   g.sl = (int)std::min<size_t>(kMaxSL, room / plan_l_stage(ng, pass_b, g.sub));
   g.sa = std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols)) & ~1;
   // one sub-stage per handoff (two, a tuner candidate, measured 1-5 % slower)
@@ -1243,14 +1247,15 @@ static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
 // ---- ring-shape autotuner ----------------------------------------------------
 // The ring shape (sub-stages per load stage, load-ring depth, TMEM operand slots)
 // does not change a product's result — the sums are exact integers and the epilogue
-// is per element — only its speed.  The first launch of each key — pass, ng and the
-// launch's size class (log2 of its 4 KB stages) — in the process times every shape that
-// fits (sub 4, 2, 1 with the deepest ring the shared memory holds; one or two
-// sub-stages per handoff where four operand slots fit) on the real operands
-// and keeps the fastest; later launches of the key use it.  Launches of fewer than
-// kTuneMinStages stages keep the fixed choice of tc_rings (their trials would cost more
-// than they can save), as does SAIGE_TC_AUTOTUNE=0 (=2 tunes every size).  SAIGE_TIMING=1
-// logs each trial.
+// is per element — only its speed.  So the tuning needs no launches of its own: the
+// first launches of each key — pass, ng and the launch's size class (log2 of its 4 KB
+// stages) — in the process each run the real product with the next candidate shape
+// (sub 4, 2, 1 with the deepest ring the shared memory holds; one or two sub-stages per
+// handoff where four operand slots fit; tc_rings' choice first), timed with CUDA events
+// that are read at the key's next launch; once every candidate has run, the fastest is
+// kept for the later launches.  Launches of fewer than kTuneMinStages stages keep the
+// fixed choice of tc_rings, as does SAIGE_TC_AUTOTUNE=0 (=2 tunes every size).
+// SAIGE_TIMING=1 logs each timed candidate.
 namespace {
 
 struct TuneKey {
@@ -1274,8 +1279,18 @@ int size_class(double stages) {
   return c;
 }
 
+struct TuneState {
+  std::vector<Rings> cand;
+  std::vector<float> ms;               // per candidate; < 0: not timed (launch refused)
+  size_t next = 0;                     // next candidate to run
+  int pending = -1;                    // candidate whose events wait to be read
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  bool done = false;
+  Rings best{};
+};
+
 std::mutex g_tune_mu;
-std::map<TuneKey, Rings> g_tune;
+std::map<TuneKey, TuneState> g_tune;
 std::atomic<int64_t> g_tune_trials{0};
 
 // SAIGE_TC_AUTOTUNE: 0 off, 2 every launch size, otherwise (default) launches of at
@@ -1290,13 +1305,14 @@ std::vector<Rings> tc_candidates(int ng, bool pass_b) {
   std::vector<Rings> out;
   const size_t room = kSmemBudget - tc_fixed_bytes();
   const Rings base = tc_rings(ng, pass_b);
+  out.push_back(base);  // the fixed choice first
   for (int sub : {4, 2, 1}) {
     const size_t ls = plan_l_stage(ng, pass_b, sub);
     if (2 * ls > room) continue;
     Rings g = base;
     g.sub = sub;
     g.sl = (int)std::min<size_t>(kMaxSL, room / ls);
-    out.push_back(g);
+    if (!(g.sub == base.sub && g.sl == base.sl)) out.push_back(g);
     if (g.sa >= 4) {  // the same ring with two sub-stages per handoff (four slots)
       g.hb = 2;
       g.sa = 4;
@@ -1324,73 +1340,62 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     return Status();
   }
   const TuneKey key{dev, kPassB ? 1 : 0, a.ng, size_class(stages)};
-  {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    auto it = g_tune.find(key);
-    if (it != g_tune.end()) {
-      a.sub = it->second.sub;
-      a.sl = it->second.sl;
-      a.sa = it->second.sa;
-      a.hb = it->second.hb;
-      SG_CUDA(launch_tc<kPassB>(grid, a, st));
-      return Status();
-    }
-  }
-  const std::vector<Rings> cand = tc_candidates(a.ng, kPassB);
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  SG_CUDA(cudaEventCreate(&e0));
-  SG_CUDA(cudaEventCreate(&e1));
-  Rings best = fixed;
-  float best_ms = 0.f;
-  bool have = false;
-  Status st_out;
-  const char* tlog = getenv("SAIGE_TIMING");
-  const bool log = tlog && tlog[0] == '1';
-  for (const Rings& g : cand) {
+  auto use = [&](const Rings& g) {
     a.sub = g.sub;
     a.sl = g.sl;
     a.sa = g.sa;
     a.hb = g.hb;
-    cudaEventRecord(e0, st);
-    const cudaError_t le = launch_tc<kPassB>(grid, a, st);
-    if (le != cudaSuccess) {
-      (void)cudaGetLastError();
-      continue;
-    }
-    cudaEventRecord(e1, st);
-    if (cudaEventSynchronize(e1) != cudaSuccess) {
-      st_out = fail(SAIGE_ECUDA, "tensor-core launch failed while tuning: %s",
-                    cudaGetErrorString(cudaGetLastError()));
-      break;
-    }
+  };
+  // the state is held under the lock through the (asynchronous) launch, so that one
+  // key's candidates and events are used by one launch at a time
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  TuneState& ts = g_tune[key];
+  if (ts.done) {
+    use(ts.best);
+    SG_CUDA(launch_tc<kPassB>(grid, a, st));
+    return Status();
+  }
+  if (ts.cand.empty()) {
+    ts.cand = tc_candidates(a.ng, kPassB);
+    ts.ms.assign(ts.cand.size(), -1.f);
+    SG_CUDA(cudaEventCreate(&ts.e0));
+    SG_CUDA(cudaEventCreate(&ts.e1));
+  }
+  const char* tlog = getenv("SAIGE_TIMING");
+  const bool log = tlog && tlog[0] == '1';
+  if (ts.pending >= 0) {  // the previous candidate's launch of this key has long been queued
+    SG_CUDA(cudaEventSynchronize(ts.e1));
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, e0, e1);
-    g_tune_trials += 1;
+    SG_CUDA(cudaEventElapsedTime(&ms, ts.e0, ts.e1));
+    ts.ms[(size_t)ts.pending] = ms;
+    const Rings& g = ts.cand[(size_t)ts.pending];
     if (log)
       fprintf(stderr, "[saige tune] pass %c ng %d grid %u nk %d: sub %d sl %d hb %d -> %.3f ms\n",
               kPassB ? 'B' : 'A', a.ng, grid, a.nk, g.sub, g.sl, g.hb, ms);
-    if (!have || ms < best_ms) {
-      best = g;
-      best_ms = ms;
-      have = true;
+    ts.pending = -1;
+  }
+  while (ts.next < ts.cand.size()) {
+    const size_t c = ts.next++;
+    use(ts.cand[c]);
+    SG_CUDA(cudaEventRecord(ts.e0, st));
+    const cudaError_t le = launch_tc<kPassB>(grid, a, st);
+    if (le != cudaSuccess) {  // a shape the launch refuses: next candidate
+      (void)cudaGetLastError();
+      continue;
     }
+    SG_CUDA(cudaEventRecord(ts.e1, st));
+    ts.pending = (int)c;
+    g_tune_trials += 1;
+    return Status();
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
-  if (!st_out.ok()) return st_out;
-  {
-    std::lock_guard<std::mutex> lk(g_tune_mu);
-    g_tune[key] = best;
-  }
-  // the output of the last trial is already complete; launch again only when the
-  // chosen shape was not the last one tried, so that the result comes from it too
-  if (!have || !(cand.back().sub == best.sub && cand.back().sl == best.sl)) {
-    a.sub = best.sub;
-    a.sl = best.sl;
-    a.sa = best.sa;
-    a.hb = best.hb;
-    SG_CUDA(launch_tc<kPassB>(grid, a, st));
-  }
+  // every candidate has run: keep the fastest
+  int bi = -1;
+  for (size_t c = 0; c < ts.cand.size(); ++c)
+    if (ts.ms[c] >= 0.f && (bi < 0 || ts.ms[c] < ts.ms[(size_t)bi])) bi = (int)c;
+  ts.best = bi >= 0 ? ts.cand[(size_t)bi] : fixed;
+  ts.done = true;
+  use(ts.best);
+  SG_CUDA(launch_tc<kPassB>(grid, a, st));
   return Status();
 }
 

@@ -436,11 +436,12 @@ int32_t saige_grm_reset_stats(saige_grm* h);
 /* Kernels this library has launched in the process so far. */
 int64_t saige_kernel_launches(void);
 
-/* Trial launches of the tensor-core ring-shape autotuner in this process: the first
- * MIXED product of each (pass, column group, size class) of at least ~4 GB of code tiles
- * times every ring shape that fits and keeps the fastest (results are identical for all
- * shapes).  SAIGE_TC_AUTOTUNE=0 in the environment keeps the fixed shape, =2 tunes
- * every size. */
+/* Timed candidate launches of the tensor-core ring-shape autotuner in this process.
+ * The first MIXED products of each (pass, column group, size class) of at least ~4 GB
+ * of code tiles each run with the next candidate ring shape, timed with CUDA events; once
+ * every candidate has run, the fastest is kept.  The candidates are real products —
+ * results are identical for all shapes — so tuning adds no launches.
+ * SAIGE_TC_AUTOTUNE=0 in the environment keeps the fixed shape, =2 tunes every size. */
 int64_t saige_tc_autotune_trials(void);
 
 /* ---------------------------------------------------------------------
