@@ -1,0 +1,82 @@
+"""CPU model of the tensor-core kernel's operand-slot handoff (csrc/kernels_tc.cu,
+tc_grm_kernel): the MMA warp waits on named barrier 1 + ab/hb once per batch of hb
+sub-stages, and the two unpack groups take alternate batches, arriving on the same
+barrier after filling the batch's slots.  A mismatch in the sequence of barriers, slots
+or ring positions between the two sides would leave a bar.sync waiting forever on the
+GPU, so both loops are restated here, step for step, and compared for every ring shape
+the host accepts (launch_tc: hb in {1, 2}, sa a multiple of 2 hb, sl >= 2, sub in
+{1, 2, 4})."""
+import pytest
+
+
+def mma_side(nk, sub, sl, sa, hb):
+    t = s = ab = k = 0
+    out = []
+    while k < nk:
+        bar, batch, j = 1 + (ab >> (hb - 1)), [], 0
+        while j < hb and k < nk:
+            batch.append((k, s, t, ab))
+            t += 1
+            if t == sub:
+                t, s = 0, (s + 1) % sl
+            ab = (ab + 1) % sa
+            j, k = j + 1, k + 1
+        out.append((bar, batch))
+    return out
+
+
+def unpack_side(nk, sub, sl, sa, hb, grp):
+    st = dict(t=0, s=0, ab=0, ph_l=0, ph_a=0)
+
+    def step():
+        st["t"] += 1
+        if st["t"] == sub:
+            st["t"] = 0
+            st["s"] += 1
+            if st["s"] == sl:
+                st["s"], st["ph_l"] = 0, st["ph_l"] ^ 1
+        st["ab"] += 1
+        if st["ab"] == sa:
+            st["ab"], st["ph_a"] = 0, st["ph_a"] ^ 1
+
+    for _ in range(grp * hb):
+        step()
+    out, kb = [], grp * hb
+    while kb < nk:
+        bar, batch = 1 + (st["ab"] >> (hb - 1)), []
+        for j in range(hb):
+            k = kb + j
+            if k < nk:
+                # the incrementally kept positions and mbarrier parities equal the
+                # closed forms the waits rely on
+                assert st["t"] == k % sub and st["s"] == (k // sub) % sl
+                assert st["ph_l"] == ((k // sub) // sl) & 1
+                assert st["ab"] == k % sa and st["ph_a"] == (k // sa) & 1
+                batch.append((k, st["s"], st["t"], st["ab"]))
+            step()
+        out.append((bar, batch))
+        for _ in range(hb):
+            step()
+        kb += 2 * hb
+    return out
+
+
+@pytest.mark.parametrize("sa,hb", [(2, 1), (4, 1), (6, 1), (4, 2)])
+def test_both_sides_take_the_same_handoffs(sa, hb):
+    for nk in list(range(1, 40)) + [141, 1164, 1172, 1564]:
+        for sub in (1, 2, 4):
+            for sl in (2, 3, 5, 8, 24):
+                mma = mma_side(nk, sub, sl, sa, hb)
+                g0 = unpack_side(nk, sub, sl, sa, hb, 0)
+                g1 = unpack_side(nk, sub, sl, sa, hb, 1)
+                merged = []
+                for i in range(max(len(g0), len(g1))):
+                    merged += g0[i:i + 1] + g1[i:i + 1]
+                assert merged == mma, (nk, sub, sl, sa, hb)
+                # barrier ids stay within the sa / hb the kernel initialises, and a
+                # barrier is always reused by the same unpack group (one use ahead at
+                # most, held by the slot-reuse wait)
+                for i, (bar, _) in enumerate(mma):
+                    assert 1 <= bar <= sa // hb
+                    if i + 2 < len(mma) and sa // hb == 2:
+                        assert mma[i + 2][0] == bar
