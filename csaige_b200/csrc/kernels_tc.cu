@@ -115,10 +115,6 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
-}
-
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                : "memory");
@@ -161,12 +157,6 @@ __device__ __forceinline__ bool mbar_wait_impl(uint32_t bar, uint32_t parity,
       }
     }
   }
-}
-
-// Spin wait for the MMA-issuing thread (on the critical path).
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
-                                          unsigned int* err) {
-  return mbar_wait_impl<false>(bar, parity, abort_flag, err);
 }
 
 // Wait with exponential back-off (producer, unpack and epilogue warps).
@@ -1068,11 +1058,6 @@ Rings tc_rings(int ng, bool pass_b) {
   // one sub-stage per handoff (two, a tuner candidate, measured 1-5 % slower)
   g.hb = 1;
   return g;
-}
-
-size_t tc_smem_bytes(int ng, bool pass_b) {
-  const Rings g = tc_rings(ng, pass_b);
-  return tc_fixed_bytes() + (size_t)g.sl * plan_l_stage(ng, pass_b, g.sub);
 }
 
 }  // namespace
