@@ -97,3 +97,46 @@ def test_compute_fails_loudly_without_gpu(golden_dir):
     with pytest.raises(cs.SaigeError) as e:
         cs.bed_marker_stats(bed, 1000, 500)
     assert e.value.code == _lib.ECUDA
+
+
+def test_ctypes_structures_match_the_header(tmp_path):
+    # every struct of include/saige_gpu.h against its ctypes mirror: size and the offset
+    # of each field, as gcc lays the C struct out (a mismatch would let the library
+    # write past a caller's struct)
+    import ctypes as C
+    import shutil
+    import subprocess
+    from pathlib import Path
+    from csaige_b200 import _lib
+
+    if shutil.which("gcc") is None:
+        pytest.skip("no C compiler")
+    pairs = {"saige_pcg_options": _lib.PcgOptions, "saige_ai_reml_config": _lib.AiRemlConfigC,
+             "saige_ai_reml_summary": _lib.AiRemlSummaryC,
+             "saige_explicit_grm_config": _lib.ExplicitGrmConfigC,
+             "saige_explicit_grm_info": _lib.ExplicitGrmInfoC,
+             "saige_vr_config": _lib.VrConfigC, "saige_vr_summary": _lib.VrSummaryC,
+             "saige_null_model": _lib.NullModelC, "saige_grm_stats": _lib.GrmStatsC,
+             "saige_cohort_spec": _lib.CohortSpecC}
+    header = Path(__file__).resolve().parents[1] / "include" / "saige_gpu.h"
+    lines = ["#include <stdio.h>", "#include <stddef.h>", f'#include "{header}"', "int main(void) {"]
+    for cname, py in pairs.items():
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", str(src), "-o", str(exe)], check=True)
+    got = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    want = {}
+    for cname, py in pairs.items():
+        want[f"{cname} size"] = C.sizeof(py)
+        for fname, _ in py._fields_:
+            want[f"{cname} {fname}"] = getattr(py, fname).offset
+    for ln in got:
+        if ln:
+            key, val = ln.rsplit(" ", 1)
+            assert int(val) == want[key], (key, int(val), want[key])
+    assert len([ln for ln in got if ln]) == len(want)
