@@ -103,11 +103,8 @@ def test_ctypes_structures_match_the_header(tmp_path):
     # every struct of include/saige_gpu.h against its ctypes mirror: size and the offset
     # of each field, as gcc lays the C struct out (a mismatch would let the library
     # write past a caller's struct)
-    import ctypes as C
     import shutil
     import subprocess
-    from pathlib import Path
-    from csaige_b200 import _lib
 
     if shutil.which("gcc") is None:
         pytest.skip("no C compiler")
