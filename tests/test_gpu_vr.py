@@ -181,9 +181,13 @@ def test_pinned_upload_path_gives_the_same_fit(subset, trait):
     assert a.variance_ratio.variance_ratio == b.variance_ratio.variance_ratio
 
 
-@pytest.mark.parametrize("concurrent", [True, False])
-def test_sub_cohort_fits_equal_their_own_fits(concurrent):
-    # fit_null::run per sub-cohort of one .bed, concurrently on threads and streams
+@pytest.mark.parametrize("concurrent,tune", [(True, False), (False, False), (True, True)])
+def test_sub_cohort_fits_equal_their_own_fits(concurrent, tune, monkeypatch):
+    # fit_null::run per sub-cohort of one .bed, concurrently on threads and streams; with
+    # tune, the ring-shape autotuner runs on every launch size, so the concurrent fits'
+    # products share its per-key candidate state (results are the same for every shape)
+    if tune:
+        monkeypatch.setenv("SAIGE_TC_AUTOTUNE", "2")
     n, m = 3000, 2000
     spec = cs.CohortSpec(n=n, m=m, seed=37, missing_rate=0.01, prevalence=0.3, h2=0.3, n_covar=2)
     bed = cs.gen_bed(spec)
