@@ -97,10 +97,17 @@ struct Extra {
   double* out = nullptr;
   int n = 0;
 };
+// search directions of the leading columns kept by the solve (with K-images)
+struct Keep {
+  double* p = nullptr;
+  double* kp = nullptr;
+  int cols = 0, cap = 0, kept = 0;
+};
 
 Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const double tau[2],
              const double* ax0 = nullptr, double* r_out = nullptr, double* kx = nullptr,
-             const double* kx0 = nullptr, bool* kx_valid = nullptr, Extra extra = Extra()) {
+             const double* kx0 = nullptr, bool* kx_valid = nullptr, Extra extra = Extra(),
+             Keep* keep = nullptr) {
   PcgRun run;
   run.b = b;
   run.x0 = x0;
@@ -121,7 +128,14 @@ Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const 
   run.precision = f.cfg->precision;
   run.x = x;
   run.force_step = x0 != nullptr;
+  if (keep) {
+    run.keep_p = keep->p;
+    run.keep_kp = keep->kp;
+    run.keep_cols = keep->cols;
+    run.keep_cap = keep->cap;
+  }
   SG_TRY(pcg_run(f.h, run, f.st));
+  if (keep) keep->kept = run.kept;
   f.pcg_iters += run.total_iters;
   if (kx_valid) *kx_valid = run.kx_valid;
   return Status();
@@ -171,6 +185,11 @@ struct Recycle {
   // basis only while tau1 = 0, where its Sigma-image needs no K, and the Hutchinson
   // trace takes K P u from the block solutions' K-images.
   bool kxu_ok = true;
+  // the block solve's search directions of its y and X columns with their K-images
+  // (a Krylov basis for K P y, whose Sigma^-1-image the AI solve wants); valid as
+  // basis vectors at any tau since their Sigma-images come from the K-images
+  double *keep_p = nullptr, *keep_kp = nullptr;
+  int keep_cap = 0, n_keep = 0;
   bool with_pw = false;                 // the fit has the W^-1 AI solve (quantitative)
   int64_t fallbacks = 0, kpy_launches_saved = 0;
   // learned correction (SAIGE_WARM_LEARNED): an MLP trained on the change of the
@@ -189,12 +208,15 @@ struct Recycle {
 
 // Held-out R^2 at or above which the prediction joins the basis.
 constexpr double kLearnR2Min = 0.25;
+// PCG iterations of the block solve whose y and X search directions are kept
+constexpr int kKeepIters = 3;
 
 Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint64_t seed) {
   const size_t ld = (size_t)f.ld, q = (size_t)f.q;
   rc.learned = learned;
   rc.diagk = diagk;
-  rc.mb_max = learned ? 3 * f.q + 1 : 2 * f.q + 1;
+  rc.keep_cap = (1 + f.p) * kKeepIters;
+  rc.mb_max = (learned ? 3 * f.q + 1 : 2 * f.q + 1) + rc.keep_cap;
   rc.nk = learned ? 2 * f.q + 3 : f.q + 3;
   if (learned) {
     const size_t nq = (size_t)f.n * q;
@@ -213,7 +235,7 @@ Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint
     SG_TRY(mlp_init(rc.mlp, seed, f.st));
   }
   const size_t mb = (size_t)rc.mb_max, nk = (size_t)rc.nk;
-  const size_t ncol = mb + (mb + q) + 3 * q + 2 * nk + mb + q + q + 2;
+  const size_t ncol = mb + (mb + q) + 3 * q + 2 * nk + mb + q + q + 2 + 2 * (size_t)rc.keep_cap;
   const size_t nsmall = mb * q + gram_partial_doubles(f.n, (int)mb, (int)(mb + q)) + mb * (mb + q);
   SG_TRY(rc.mem.reserve((ncol * ld + nsmall) * 8));
   double* b = rc.mem.as<double>();
@@ -230,6 +252,8 @@ Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint
   rc.kblock = b;            b += q * ld;
   rc.kpk = b;               b += ld;
   rc.kpw = b;               b += ld;
+  rc.keep_p = b;            b += (size_t)rc.keep_cap * ld;
+  rc.keep_kp = b;           b += (size_t)rc.keep_cap * ld;
   rc.gam = b;               b += mb * q;
   rc.gout = b;              b += mb * (mb + q);
   rc.gpart = b;
@@ -301,6 +325,7 @@ Status galerkin_start(Fit& f, Recycle& rc, int mb, int q, bool& ok) {
 Status basis_cols(Fit& f, Recycle& rc, int at, const double* x, const double* kx, int k,
                   const double tau[2]) {
   const int64_t ld = f.ld;
+  if (at + k > rc.mb_max) return fail(SAIGE_EINVAL, "start basis beyond its %d columns", rc.mb_max);
   SG_TRY(copy_cols(f, x, rc.v + (size_t)at * ld, k));
   SG_TRY(copy_cols(f, kx, rc.kv + (size_t)at * ld, k));
   SG_CUDA(sigma_image(x, kx, f.wmax, tau[0], tau[1], rc.av + (size_t)at * ld, f.n, ld, k, f.st));
@@ -325,6 +350,10 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
     SG_TRY(basis_cols(f, rc, mb, f.sol, rc.kblock, f.q, tau));
     mb += f.q;
   }
+  if (rc.n_keep > 0) {  // the previous block solve's directions (their K-images known)
+    SG_TRY(basis_cols(f, rc, mb, rc.keep_p, rc.keep_kp, rc.n_keep, tau));
+    mb += rc.n_keep;
+  }
   if (rc.have_delta) {
     // the learned prediction of this iteration's change of the solutions
     SG_TRY(basis_cols(f, rc, mb, rc.delta, rc.kout + (size_t)rc.at_delta * ld, f.q, tau));
@@ -347,11 +376,14 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
     if (need_pk) rc.have_kpk = true;
     if (need_pw) rc.have_kpw = true;
   }
-  if (ok)
-    return solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br, rc.kblock,
-                 rc.kv_ok ? rc.kx0 : nullptr, &kx_ok, ex);
-  return solve(f, f.rhs, f.sol, x0_prev, f.q, tau, nullptr, rc.br, rc.kblock, nullptr, &kx_ok,
-               ex);
+  // keep this solve's y and X directions (overwriting the ones copied into the basis)
+  Keep keep{rc.keep_p, rc.keep_kp, 1 + f.p, rc.keep_cap, 0};
+  Status s = ok ? solve(f, f.rhs, f.sol, rc.x0, f.q, tau, rc.ax0, rc.br, rc.kblock,
+                        rc.kv_ok ? rc.kx0 : nullptr, &kx_ok, ex, &keep)
+                : solve(f, f.rhs, f.sol, x0_prev, f.q, tau, nullptr, rc.br, rc.kblock, nullptr,
+                        &kx_ok, ex, &keep);
+  if (tau[1] != 0.0) rc.n_keep = keep.kept;  // with tau1 = 0 the solve forms no K-images
+  return s;
 }
 
 // K Py, and in the same launch K X*_t (this iteration's block solutions, for the next
@@ -471,6 +503,10 @@ Status ai_solve_recycled(Fit& f, Recycle& rc, const double* b, double* x, double
     SG_TRY(basis_cols(f, rc, mb, f.rhs + ld, f.kxu, f.p + f.nrv, tau));
     mb += f.p + f.nrv;
     if (!rc.kxu_ok) rc.kv_ok = false;
+  }
+  if (rc.n_keep > 0) {  // this iteration's block directions: a Krylov basis for K P y
+    SG_TRY(basis_cols(f, rc, mb, rc.keep_p, rc.keep_kp, rc.n_keep, tau));
+    mb += rc.n_keep;
   }
   if (have) {
     SG_TRY(basis_cols(f, rc, mb, x, kx, 1, tau));

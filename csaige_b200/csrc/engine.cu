@@ -483,6 +483,15 @@ Status pcg_run(saige_grm* h, PcgRun& run, cudaStream_t st) {
       } else if (!no_k) {
         SG_TRY(grm_product(h, s.p, s.kp, q, state.data(), run.precision, st));
       }
+      if (!no_k && run.keep_p && run.keep_kp)
+        for (int c = 0; c < std::min(run.keep_cols, q) && run.kept < run.keep_cap; ++c) {
+          if (state[(size_t)c] != kColActive) continue;
+          SG_CUDA(cudaMemcpyAsync(run.keep_p + (size_t)run.kept * ld, s.p + (size_t)c * ld,
+                                  (size_t)ld * 8, cudaMemcpyDeviceToDevice, st));
+          SG_CUDA(cudaMemcpyAsync(run.keep_kp + (size_t)run.kept * ld, s.kp + (size_t)c * ld,
+                                  (size_t)ld * 8, cudaMemcpyDeviceToDevice, st));
+          ++run.kept;
+        }
       if (run.w_inverse)
         SG_CUDA(pcg_apply(s.p, s.kp, run.wv, run.tau0, run.tau1, s.ap, n, ld, q, s.cols,
                           s.partial, st));

@@ -129,6 +129,12 @@ struct PcgRun {
   const double* extra_in = nullptr;
   double* extra_out = nullptr;
   int n_extra = 0;
+  // optional: the search directions p of the first keep_cols columns, with their
+  // K-images, copied after each product into keep_p / keep_kp (ld apart) while the
+  // column is active, up to keep_cap vectors; kept = how many on return
+  double* keep_p = nullptr;
+  double* keep_kp = nullptr;
+  int keep_cols = 0, keep_cap = 0, kept = 0;
   std::vector<int32_t> iters, state;
   std::vector<double> resid;
   int64_t total_iters = 0;
