@@ -41,7 +41,8 @@ def test_loco_chromosomes_in_reference_order(cohort):
 
 
 @pytest.mark.parametrize("solve,warm", [(cs.SOLVE_SINGLE, cs.WARM_ZERO),
-                                        (cs.SOLVE_BLOCK, cs.WARM_PREVIOUS)])
+                                        (cs.SOLVE_BLOCK, cs.WARM_PREVIOUS),
+                                        (cs.SOLVE_BLOCK, cs.WARM_RECYCLED)])
 def test_mixed_loco_equals_refit_without_the_chromosome(cohort, solve, warm):
     c = cohort
     cfg = cs.AiRemlConfig(max_iter=4, precision=cs.PREC_MIXED, solve=solve, warm_start=warm)
