@@ -25,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import dataclasses
 import json
 import os
 import statistics
@@ -59,6 +60,14 @@ CPU_SAMPLE_MARKERS = 32768
 TC_READ_PER_MARKER_ROW = {"A": 932.4e6 / 18048, "B": 935.2e6 / 18048}
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+# The plain CPU-scale fit-null cohort (the reference's own benchmark size): N = 2,000,
+# M = 5,000, binary at ~10 % prevalence, 2 covariates, 10 % sibling pairs, 1 % missing.
+# The precision-form cohort of the accuracy block (errors against FP64 products).
+ACCURACY = dict(n=50_000, m=100_000)
+# tau tolerance of the fit-null command (saige-cli/src/commands/fit_null.rs:74-80)
+CLI_TOL = 1e-5
+CONFIG1 = dict(seed=12345, n=2000, m=5000, sib_frac=0.10, missing_rate=0.01, prevalence=0.10,
+               n_covar=2, h2=0.2)
 # Explicit GRM (create-sparse-grm) workload: an FP64 SYRK over all sample pairs, so
 # its size is set by N^2 M / 2 products; N = 32,768 and M = 8,192 give 4.4e12.
 EXPLICIT_GRM = dict(n=32_768, m=8_192, min_maf=0.01, cutoff=0.125)
@@ -85,6 +94,10 @@ def parse_args():
                     help="skip the 16 sub-cohort fits")
     ap.add_argument("--no-learned", action="store_true",
                     help="skip the learned-versus-recycled start comparison")
+    ap.add_argument("--no-config1", action="store_true",
+                    help="skip the plain CPU-scale cohort (GPU fits, oracle, measured CPU fit)")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the product and solve errors against the FP64 oracle")
     ap.add_argument("--no-explicit-grm", action="store_true",
                     help="skip the create-sparse-grm workload")
     ap.add_argument("--explicit-grm-only", action="store_true",
@@ -195,13 +208,14 @@ def ref_kv_count(iterations: int, p: int, nrv: int, pcg_iters: int, solves_per_i
 class CpuSample:
     """The oracle's packed f32 OnTheFlyGrm::mat_vec (saige-core/src/glmm/pcg.rs:128-180
     arithmetic, per-thread fold, all host threads) on `markers` synthetic markers of
-    the workload's cohort; products are timed and extrapolated to m_full markers."""
+    the workload's cohort; products are timed and extrapolated to m_full markers.
+    The cohort comes from the oracle's statement of the generator, so nothing of the
+    library is loaded."""
 
     def __init__(self, n: int, markers: int):
         sys.path.insert(0, str(ROOT / "tests"))
         import numpy as np
 
-        import csaige_b200 as cs
         import oracle_ffi as O
 
         O.L.orc_grm_matvec_f32_packed.restype = C.c_int
@@ -210,10 +224,10 @@ class CpuSample:
                                                   O._d, C.c_int]
         self.O, self.np = O, np
         self.n, self.markers = n, markers
-        spec = cs.CohortSpec(n=n, m=markers, seed=WORKLOAD["seed"],
-                             sib_frac=WORKLOAD["sib_frac"], cousin_frac=WORKLOAD["cousin_frac"],
+        spec = O.cohort_spec(n=n, m=markers, seed=WORKLOAD["seed"], sib_frac=WORKLOAD["sib_frac"],
+                             cousin_frac=WORKLOAD["cousin_frac"],
                              missing_rate=WORKLOAD["missing_rate"])
-        bed = cs.gen_bed(spec)  # host generator, no GPU
+        bed = O.gen_bed(spec)
         self.af, _, _ = O.marker_stats(bed, n, markers)
         self.body = np.ascontiguousarray(bed[3:])
         self.rows = np.arange(markers, dtype=np.int64)
@@ -235,6 +249,33 @@ class CpuSample:
         return (f"OnTheFlyGrm::mat_vec arithmetic (f32, per-thread fold) on {self.markers} of "
                 f"{m_full} markers x {self.n} samples, extrapolated x{m_full / self.markers:.1f} "
                 f"per product and x{kv_fit} products per fit (reference strategy count)")
+
+
+def cpu_config1_fit() -> dict:
+    """A whole fit-null measured on the host cores, not extrapolated: the plain cohort
+    (N = 2,000, M = 5,000, binary ~10 %, 2 covariates, seed 12345) from .bed bytes to
+    tau with the oracle — marker statistics, QC and the VR/GRM split, f32 Z
+    (pcg.rs:101-122) and fit_ai_reml (ai_reml.rs:86-427) at the fit-null command's
+    settings (tol 1e-5, max_iter 30) with the f32 product on all threads (the rayon
+    fold and reduce of pcg.rs:149-176)."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import oracle_ffi as O
+
+    spec = O.cohort_spec(**CONFIG1)
+    bed = O.gen_bed(spec)
+    y, x = O.gen_pheno(spec)
+    t0 = time.perf_counter()
+    af, mac, nv = O.marker_stats(bed, spec.n, spec.m)
+    g, _ = O.select_markers(af, mac, nv, spec.n)
+    z = O.standardize(O.dosages(bed, spec.n, g), af[g], 1)
+    t1 = time.perf_counter()
+    o = O.fit_ai_reml(y, x, O.BINARY, O.K_OTF, z, m=len(g), kmode=2, max_iter=30, tol=1e-5)
+    t2 = time.perf_counter()
+    return {"workload": "fit-null binary ~10% prev, N=2000, M=5000, 2 covariates, 30 probes, "
+                        "tol 1e-5 (measured whole fit, oracle f32 product on all host threads)",
+            "pipeline_s": t2 - t0, "fit_s": t2 - t1, "cores": os.cpu_count(),
+            "tau": [float(o["tau"][0]), float(o["tau"][1])], "iterations": int(o["iterations"]),
+            "n_kv": int(o["n_kv"]), "pcg_iters": int(o["pcg_iters"]), "markers_grm": int(len(g))}
 
 
 def explicit_grm_block(cs, gpu_index: int, n: int, m: int, reps: int = 4,
@@ -295,9 +336,116 @@ def explicit_grm_block(cs, gpu_index: int, n: int, m: int, reps: int = 4,
     return out
 
 
+def config1_block(cs) -> dict:
+    """The plain CPU-scale cohort (N = 2,000, M = 5,000): the fast and the plain GPU fits
+    at the command's tolerance, tau against the FP64 oracle (exact GRM), and a whole
+    CPU fit measured beside them."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+
+    import oracle_ffi as O
+
+    spec = cs.CohortSpec(**CONFIG1)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = cs.bed_marker_stats(bed, spec.n, spec.m)
+    g, _ = cs.select_grm_markers(af, mac, nv, spec.n)
+    out = {"workload": "fit-null binary ~10% prev, N=2000, M=5000, 2 covariates, 30 probes, "
+                       "tol 1e-5"}
+    k = O.grm_explicit(O.standardize(O.dosages(bed, spec.n, g), af[g], 0))
+    o = O.fit_ai_reml(y, x, O.BINARY, O.K_EXPLICIT, k, max_iter=30, tol=CLI_TOL)
+    out["oracle_fp64_tau"] = [float(o["tau"][0]), float(o["tau"][1])]
+    for name, prec, solve, warm in (("fast", cs.PREC_MIXED, cs.SOLVE_BLOCK, cs.WARM_RECYCLED),
+                                    ("plain", cs.PREC_FP32, cs.SOLVE_SINGLE, cs.WARM_ZERO)):
+        grm = cs.OnTheFlyGrm.from_bed(bed, spec.n, spec.m, g, af[g], precision=prec)
+        cfg = cs.AiRemlConfig(precision=prec, solve=solve, warm_start=warm, tol=CLI_TOL,
+                              max_iter=30)
+        cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg)  # warm-up
+        rs = [cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg) for _ in range(3)]
+        r = rs[-1]
+        out[name] = {"seconds": statistics.median(q.seconds for q in rs),
+                     "ai_reml_iterations": int(r.iterations), "n_kv": int(r.n_kv),
+                     "n_kv_launches": int(r.n_kv_launches), "pcg_iters": int(r.pcg_iters),
+                     "tau": [float(r.tau[0]), float(r.tau[1])],
+                     "tau_rel_err_vs_fp64_oracle": float(abs(r.tau[1] - o["tau"][1]) /
+                                                         abs(o["tau"][1]))}
+        grm.close()
+    out["cpu_fit"] = cpu_config1_fit()
+    out["speedup_fast_vs_cpu_fit"] = out["cpu_fit"]["fit_s"] / out["fast"]["seconds"]
+    return out
+
+
+def accuracy_block(cs) -> dict:
+    """The precision-form cohort (N = 50,000, M = 100,000, binary at 5 %, 6
+    covariates): errors of the GPU products against the oracle's FP64 product on the
+    same packed genotypes, and the true residual of Sigma^-1 y (FP64 products) at the
+    fast fit's tau and W."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+    import torch
+
+    import oracle_ffi as O
+
+    n, m = ACCURACY["n"], ACCURACY["m"]
+    spec = cs.CohortSpec(n=n, m=m, seed=WORKLOAD["seed"], sib_frac=WORKLOAD["sib_frac"],
+                         cousin_frac=WORKLOAD["cousin_frac"], missing_rate=WORKLOAD["missing_rate"],
+                         trait=cs.TraitType.Binary, n_covar=6, prevalence=0.05, h2=0.2,
+                         n_causal=1000)
+    bed_dev = torch.empty(spec.bed_len, dtype=torch.uint8, device="cuda")
+    cs.gen_bed_dev(spec, bed_dev.data_ptr())
+    bed = bed_dev.cpu().numpy()
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = cs.api.bed_marker_stats_dev(bed_dev.data_ptr(), spec.bed_len, n, m)
+    g, _ = cs.select_grm_markers(af, mac, nv, n)
+    grm = cs.OnTheFlyGrm.from_bed_dev(bed_dev.data_ptr(), spec.bed_len, n, m, g, af[g],
+                                      precision=cs.PREC_MIXED)
+    del bed_dev
+    torch.cuda.empty_cache()
+    rng = np.random.default_rng(7)
+    v = np.vstack([rng.standard_normal(n), y - y.mean(), O.probes(12345, 1, n)[0]])
+    want = O.grm_matmul_f64_packed(bed, n, g, af[g], v)
+
+    def errs(got):
+        return {"max_rel": float(max(np.abs(got[c] - want[c]).max() / np.abs(want[c]).max()
+                                     for c in range(len(v)))),
+                "l2_rel": float(max(np.linalg.norm(got[c] - want[c]) / np.linalg.norm(want[c])
+                                    for c in range(len(v))))}
+
+    out = {"workload": f"binary 5% prev, N={n}, M={m} bed markers ({len(g)} in the GRM), "
+                       f"6 covariates; errors against the oracle's FP64 product",
+           "kv_columns": "N(0,1), y - mean(y), a Rademacher probe",
+           "kv_mixed_tensor_cores": errs(grm.mat_vec(v, precision=cs.PREC_MIXED)),
+           "kv_mixed_one_column": errs(np.vstack([grm.mat_vec(v[c], precision=cs.PREC_MIXED)
+                                                  for c in range(len(v))])),
+           "kv_fp32": errs(grm.mat_vec(v, precision=cs.PREC_FP32))}
+    fits = {}
+    for name, prec, solve, warm in (("fast", cs.PREC_MIXED, cs.SOLVE_BLOCK, cs.WARM_RECYCLED),
+                                    ("plain", cs.PREC_FP32, cs.SOLVE_SINGLE, cs.WARM_ZERO)):
+        cfg = cs.AiRemlConfig(precision=prec, solve=solve, warm_start=warm, tol=CLI_TOL,
+                              max_iter=30)
+        r = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg)
+        fits[name] = r
+        sol = cs.PcgSolver(1e-5, 500).solve(grm, r.working_weights, r.tau, y, precision=prec)
+        kx = O.grm_matmul_f64_packed(bed, n, g, af[g], sol.x)
+        sig_x = r.tau[0] * sol.x / np.maximum(r.working_weights, 1e-30) + r.tau[1] * kx
+        out[f"{name}_fit"] = {
+            "seconds": r.seconds, "ai_reml_iterations": int(r.iterations),
+            "tau": [float(r.tau[0]), float(r.tau[1])], "pcg_iters": int(r.pcg_iters),
+            "sigma_inv_y_true_residual": float(np.linalg.norm(y - sig_x) / np.linalg.norm(y)),
+            "sigma_inv_y_pcg_iters": int(sol.iterations)}
+    out["tau_rel_diff_fast_vs_plain"] = float(abs(fits["fast"].tau[1] - fits["plain"].tau[1]) /
+                                              abs(fits["plain"].tau[1]))
+    out["note"] = ("tau against an FP64 fit is checked on the CPU-scale cohort (config1 block "
+                   "and the tests); here the FP64 oracle provides the products")
+    grm.close()
+    return out
+
+
 def run_reference(args, rank):
     """The reference's strategy on the host cores: each step times one product of the
-    oracle over a bounded marker sample and extrapolates to a whole fit."""
+    oracle over a bounded marker sample and extrapolates it to a whole fit at the
+    benchmark size (labelled extrapolated); a whole fit of the plain CPU-scale cohort
+    is measured once beside it.  Only the oracle is loaded."""
     if rank != 0:
         return
     smp = CpuSample(args.n, min(CPU_SAMPLE_MARKERS, args.m))
@@ -313,9 +461,10 @@ def run_reference(args, rank):
         "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic", "config": _config(args),
         "cpu_baseline": {"value": val, "unit": "s", "cores": smp.threads, "kind": "port",
-                         "sample": smp.describe(args.m, REF_KV_PER_FIT),
+                         "sample": smp.describe(args.m, REF_KV_PER_FIT), "extrapolated": True,
                          "sec_per_kv": val / REF_KV_PER_FIT},
         "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_fit_config1": cpu_config1_fit(),
     }
     print(json.dumps(line), flush=True)
 
@@ -367,7 +516,10 @@ def run_ours(args, world, rank, local):
 
     warm = {"previous": cs.WARM_PREVIOUS, "recycled": cs.WARM_RECYCLED,
             "learned": cs.WARM_LEARNED}[args.warm]
-    fast = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK, warm_start=warm)
+    # the fit-null command's settings (fit_null.rs:74-80, 273-282): tau tolerance 1e-5,
+    # 30 AI-REML iterations at most, PCG tolerance 1e-5
+    fast = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK, warm_start=warm,
+                           tol=CLI_TOL, max_iter=30)
     for _ in range(args.warmup):
         cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, fast)
     grm.reset_stats()
@@ -447,6 +599,15 @@ def run_ours(args, world, rank, local):
         "markers_grm": int(m_grm), "markers_vr": int(len(vidx)),
         "fast_config": f"MIXED + block PCG + {args.warm} warm start",
     }
+
+    # the same fit at AiRemlConfig::default's tau tolerance (0.02, ai_reml.rs:39-51)
+    dcfg = dataclasses.replace(fast, tol=0.02)
+    dres = [cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, dcfg) for _ in range(3)]
+    line["default_tol_fit"] = {
+        "tol": 0.02, "seconds": statistics.mean(r.seconds for r in dres),
+        "ai_reml_iterations": int(dres[-1].iterations),
+        "n_kv_launches": int(dres[-1].n_kv_launches), "pcg_iters": int(dres[-1].pcg_iters),
+        "tau": [float(dres[-1].tau[0]), float(dres[-1].tau[1])]}
 
     # end to end through the host-buffer C ABI
     if host_bed is not None:
@@ -530,7 +691,7 @@ def run_ours(args, world, rank, local):
         cmp_ = {}
         for name, wmode in (("recycled", cs.WARM_RECYCLED), ("learned", cs.WARM_LEARNED)):
             cfg_l = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
-                                    warm_start=wmode, tol=1e-4)
+                                    warm_start=wmode, tol=CLI_TOL)
             r = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg_l)
             cmp_[name] = {"seconds": r.seconds, "ai_reml_iterations": int(r.iterations),
                           "n_kv_launches": int(r.n_kv_launches), "pcg_iters": int(r.pcg_iters),
@@ -541,13 +702,14 @@ def run_ours(args, world, rank, local):
                                    "held_out_r2": float(r.learned_r2),
                                    "mlp_seconds": float(r.learned_seconds)})
         cmp_["launches_saved"] = cmp_["recycled"]["n_kv_launches"] - cmp_["learned"]["n_kv_launches"]
-        cmp_["config"] = "same cohort, AiRemlConfig tol 1e-4, MIXED, block PCG"
+        cmp_["config"] = "same cohort, AiRemlConfig tol 1e-5, MIXED, block PCG"
         line["learned_vs_recycled"] = cmp_
     # the reference's strategy on the same GPU
     plain_kv = None
     if not args.no_plain and world == 1:
         grm.precision = cs.PREC_FP32
-        plain_cfg = cs.AiRemlConfig()  # FP32, one PCG per right-hand side, zero starts
+        # FP32, one PCG per right-hand side, zero starts, the command's tolerance
+        plain_cfg = cs.AiRemlConfig(tol=CLI_TOL, max_iter=30)
         t0 = time.perf_counter()
         pr = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, plain_cfg)
         pw = time.perf_counter() - t0
@@ -559,6 +721,13 @@ def run_ours(args, world, rank, local):
                          "tau": [float(pr.tau[0]), float(pr.tau[1])]}
         line["speedup_vs_plain"] = pr.seconds / step_s
         line["tau_rel_diff_vs_plain"] = abs(float(last.tau[1]) - float(pr.tau[1])) / abs(float(pr.tau[1]))
+        pd = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cs.AiRemlConfig())
+        line["plain"]["default_tol"] = {
+            "tol": 0.02, "seconds": pd.seconds, "pcg_iters": int(pd.pcg_iters),
+            "ai_reml_iterations": int(pd.iterations), "n_kv": int(pd.n_kv),
+            "reference_kv_per_fit": int(ref_kv_count(pd.iterations, p, 30, pd.pcg_iters, solves)),
+            "tau": [float(pd.tau[0]), float(pd.tau[1])]}
+        grm.precision = cs.PREC_MIXED
     # CPU baseline (rank 0): bounded sample, extrapolated with the reference product count
     if rank == 0 and world == 1:
         kv_fit = plain_kv or REF_KV_PER_FIT
@@ -567,7 +736,7 @@ def run_ours(args, world, rank, local):
         per_kv = statistics.median(times) * m / smp.markers
         line["cpu_baseline"] = {
             "value": per_kv * kv_fit, "unit": "s", "cores": smp.threads, "kind": "port",
-            "sample": smp.describe(m, kv_fit), "sec_per_kv": per_kv}
+            "sample": smp.describe(m, kv_fit), "extrapolated": True, "sec_per_kv": per_kv}
         # the same per-product CPU time, times each extra path's reference product count
         if "variance_ratio" in line:
             vr = line["variance_ratio"]
@@ -580,6 +749,11 @@ def run_ours(args, world, rank, local):
                                                      for mc in loco_sizes)
             line["loco"]["cpu_note"] = ("22 fits x the reference strategy's product count x the "
                                         "CPU port's seconds per product, scaled by M - M_chrom")
+    if rank == 0 and world == 1 and not args.no_config1:
+        line["config1"] = config1_block(cs)
+    if rank == 0 and world == 1 and not args.no_accuracy:
+        del grm
+        line["accuracy"] = accuracy_block(cs)
     if rank == 0 and world == 1 and not args.no_explicit_grm:
         line["explicit_grm"] = explicit_grm_block(cs, local, args.grm_n, args.grm_m,
                                                   args.grm_reps)

@@ -232,6 +232,13 @@ class OnTheFlyGrm:
         check(LIB.saige_grm_matvec_dev(self._h, C.c_void_p(v_ptr), C.c_void_p(out_ptr),
                                        self.n_samples, nrhs, prec, C.c_void_p(stream or None)))
 
+    def diag(self) -> np.ndarray:
+        """K_ii = (1/M) sum_m z_im^2 in FP64 (Get_Diagof_StdGeno,
+        src/SAIGE_fitGLMM_fast.cpp:642-680)."""
+        out = np.empty(self.n_samples)
+        check(LIB.saige_grm_diag(self._h, _dptr(out), self.n_samples))
+        return out
+
     def __call__(self, v):
         return self.mat_vec(v)
 

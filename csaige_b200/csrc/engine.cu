@@ -11,6 +11,7 @@
 #include "engine.cuh"
 #include "kernels.cuh"
 #include "kernels_tc.cuh"
+#include "warm.cuh"
 #include "rng.hpp"
 
 namespace saige {
@@ -671,6 +672,11 @@ SG_API int64_t saige_kernel_launches(void) { return launches_total(); }
 
 SG_API int64_t saige_tc_autotune_trials(void) { return tc_autotune_trials(); }
 
+SG_API int32_t saige_tc_set_wait_budget(int64_t cycles) {
+  tc_set_wait_budget((long long)cycles);
+  return SAIGE_OK;
+}
+
 SG_API int32_t saige_release_cached_memory(void) {
   SG_GUARD_BEGIN
   release_cached_blocks();
@@ -1179,6 +1185,25 @@ SG_API int32_t saige_grm_matvec_dev(saige_grm* h, const double* v_dev, double* o
     SG_TRY(grm_product(h, dv, dk, nrhs, nullptr, precision, st));
     SG_TRY(devcopy_block(h, dk, h->n_pad, out_dev, h->n, nrhs, st));
     SG_CUDA(cudaStreamSynchronize(st));
+    return Status();
+  };
+  return body().code;
+  SG_GUARD_END
+}
+
+SG_API int32_t saige_grm_diag(saige_grm* h, double* out, int64_t n) {
+  SG_GUARD_BEGIN
+  set_error("");
+  if (!h || !out) return fail(SAIGE_EINVAL, "null argument").code;
+  if (n != h->n) return fail(SAIGE_EINVAL, "n mismatch").code;
+  std::lock_guard<std::recursive_mutex> lk(h->mu);
+  DeviceGuard dg(h->device);
+  auto body = [&]() -> Status {
+    SG_TRY(h->ws_io.reserve((size_t)h->n_pad * sizeof(double)));
+    double* dd = h->ws_io.as<double>();
+    SG_TRY(grm_diag(h, dd, h->stream));
+    SG_TRY(download_block(h, dd, out, 1, h->stream));
+    SG_CUDA(cudaStreamSynchronize(h->stream));
     return Status();
   };
   return body().code;

@@ -93,6 +93,7 @@ struct TcArgs {
   double out_scale;         // pass B: 1/M
   unsigned int* err;
   unsigned long long* trace;  // optional pipeline trace of CTA 0 (SAIGE_TC_TRACE=1)
+  long long wait_cycles;    // budget of each pipeline wait (0: give up unless already done)
 };
 
 constexpr int kTraceStages = 64;
@@ -133,12 +134,18 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
 }
 
 // Bounded wait: returns false (and raises the CTA abort flag and the error
-// word) when the barrier phase does not complete in time or another role
-// already gave up.
+// word) when the barrier phase does not complete within `budget` cycles or another
+// role already gave up.  A budget of 0 gives up at the first poll that fails.
 template <bool kBackoff>
 __device__ __forceinline__ bool mbar_wait_impl(uint32_t bar, uint32_t parity,
-                                               volatile int* abort_flag, unsigned int* err) {
+                                               volatile int* abort_flag, unsigned int* err,
+                                               long long budget) {
   if (mbar_try_wait(bar, parity)) return true;
+  if (budget <= 0) {
+    *abort_flag = 1;
+    atomicOr(err, 1u);
+    return false;
+  }
   const long long t0 = clock64();
   uint32_t sleep_ns = 32;
   for (uint32_t polls = 1;; ++polls) {
@@ -150,7 +157,7 @@ __device__ __forceinline__ bool mbar_wait_impl(uint32_t bar, uint32_t parity,
     }
     if ((polls & 63u) == 0) {  // the clock and the abort flag are checked every 64 polls
       if (*abort_flag) return false;
-      if (clock64() - t0 > kWaitCycles) {
+      if (clock64() - t0 > budget) {
         *abort_flag = 1;
         atomicOr(err, 1u);
         return false;
@@ -161,8 +168,27 @@ __device__ __forceinline__ bool mbar_wait_impl(uint32_t bar, uint32_t parity,
 
 // Wait with exponential back-off (producer, unpack and epilogue warps).
 __device__ __forceinline__ bool mbar_wait_sleep(uint32_t bar, uint32_t parity,
-                                                volatile int* abort_flag, unsigned int* err) {
-  return mbar_wait_impl<true>(bar, parity, abort_flag, err);
+                                                volatile int* abort_flag, unsigned int* err,
+                                                long long budget) {
+  return mbar_wait_impl<true>(bar, parity, abort_flag, err, budget);
+}
+
+// Wait for asynchronous work this CTA already issued (its bulk copies, its MMAs),
+// which completes whatever the other roles did: the abort flag is not consulted and
+// the budget is the fixed one, so that after an abort no copy or MMA is still in
+// flight when the CTA frees its TMEM and exits.  False (and the error word) only if
+// the hardware does not complete the work within ~2 s.
+__device__ __forceinline__ bool mbar_wait_drain(uint32_t bar, uint32_t parity, unsigned int* err) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const long long t0 = clock64();
+  for (uint32_t polls = 1;; ++polls) {
+    if (mbar_try_wait(bar, parity)) return true;
+    __nanosleep(128);
+    if ((polls & 63u) == 0 && clock64() - t0 > kWaitCycles) {
+      atomicOr(err, 2u);
+      return false;
+    }
+  }
 }
 
 // Non-tensor bulk copy global -> shared (16-byte aligned addresses, size a
@@ -379,9 +405,11 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
       const uint8_t* codes = a.tiles + (size_t)tile * a.tile_ld * kTileBytes;
       int S = 0;
       uint32_t ph = 0;  // (J / sl) & 1
+      int issued = 0;   // load stages whose copies were issued
       for (int J = 0; J < n_load; ++J) {
         // the slot is free once the MMAs of load stage J - sl completed
-        if (J >= a.sl && !mbar_wait_sleep(P.LDONE(S), ph ^ 1u, abort_flag, a.err)) break;
+        if (J >= a.sl && !mbar_wait_sleep(P.LDONE(S), ph ^ 1u, abort_flag, a.err, a.wait_cycles))
+          break;
         if (J < kTraceStages) trace_mark(a, J, 0);  // load issued
         const int k0 = J * a.sub;
         const uint32_t cnt = (uint32_t)min(a.sub, a.nk - k0);
@@ -392,8 +420,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
           if (kPassB)
             bulk_load(P.B_m(S, t), a.img_m + (size_t)(k0 + t) * P.b_bytes, P.b_bytes, P.FULL(S));
         }
+        issued = J + 1;
         if (++S == a.sl) { S = 0; ph ^= 1u; }
       }
+      // Before the CTA exits, every issued copy has landed: load stage J completes
+      // phase (J / sl) & 1 of FULL(J % sl), and only the last sl issued stages can
+      // still be in flight (stage J was issued after stage J - sl was consumed).  On
+      // the normal path these phases completed long ago and the waits return at once.
+      for (int J = issued > a.sl ? issued - a.sl : 0; J < issued; ++J)
+        mbar_wait_drain(P.FULL(J % a.sl), (uint32_t)((J / a.sl) & 1), a.err);
     }
   } else if (warp == 1) {
     // ---------------- MMA issuer ----------------
@@ -417,11 +452,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
       named_bar_sync(1 + (ab >> (kHb - 1)), kHandoffThreads);
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       if (lane == 1) trace_mark(a, k, 4);  // MMA may issue
+      // After an abort no further MMA is issued (the handoffs still run, in step with
+      // the unpack groups).  Lane 1 reads the flag: lane 0, which has MMAs in flight,
+      // makes no memory access.
+      const int aborted = __shfl_sync(0xffffffffu, lane == 1 ? *abort_flag : 0, 1);
       const int k_batch = k;
 #pragma unroll
       for (int j = 0; j < kHb; ++j, ++k) {
         if (kHb > 1 && k >= a.nk) break;
-        if (lane == 0) {
+        if (lane == 0 && !aborted) {
           // genotype and missing-flag MMAs alternate (two independent accumulators
           // pipeline; grouping each accumulator's MMAs measured 15-40 % slower), and
           // each sub-stage is committed as soon as its MMAs are issued, so that its
@@ -480,11 +519,12 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
       for (int j = 0; j < hb; ++j) {
         const int k = kb + j;
         if (hb == 1 || k < a.nk) {
-          if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err);
+          if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err, a.wait_cycles);
           if (live && row == 0) trace_mark(a, k, 1);  // codes landed
           // operand slot ab is free once the MMAs of its previous use (sub-stage k - sa)
           // completed
-          if (live && k >= a.sa) live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err);
+          if (live && k >= a.sa)
+            live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err, a.wait_cycles);
           live = __all_sync(0xffffffffu, live);  // warp-uniform: the barrier calls below must agree
           if (live) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -520,7 +560,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
     __syncwarp();
     const int sub = grp;  // 0 or 1: which half of the column chunks
     const int trow = row;
-    const bool ok = mbar_wait_sleep(P.ACCF(), 0u, abort_flag, a.err);
+    // The MMA warp always commits ACCF after its last MMA (none after an abort), so
+    // this wait also ensures that no MMA is in flight when the TMEM is freed.
+    const bool ok = mbar_wait_drain(P.ACCF(), 0u, a.err) && !*abort_flag;
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const int64_t grow = (int64_t)tile * kRows + trow;  // marker (A) or sample (B)
     double rowa = 0.0, rowb = 0.0;
@@ -1213,8 +1255,13 @@ static Scal carve(TcPlan* p) {
   return s;
 }
 
+// Budget of each pipeline wait in SM cycles; saige_tc_set_wait_budget changes it.
+std::atomic<long long> g_tc_wait_cycles{kWaitCycles};
+
 template <bool kPassB>
-static cudaError_t launch_tc(unsigned grid, const TcArgs& a, cudaStream_t st) {
+static cudaError_t launch_tc(unsigned grid, const TcArgs& args, cudaStream_t st) {
+  TcArgs a = args;
+  a.wait_cycles = g_tc_wait_cycles.load(std::memory_order_relaxed);
   if (a.hb < 1 || a.hb > 2 || a.sa < 2 * a.hb || a.sa % (2 * a.hb) || a.sa > kMaxSA ||
       a.sl < 2 || a.sl > kMaxSL || a.sub < 1 ||
       a.sub > 4)
@@ -1385,6 +1432,10 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
 }
 
 int64_t tc_autotune_trials() { return g_tune_trials.load(); }
+
+void tc_set_wait_budget(long long cycles) {
+  g_tc_wait_cycles.store(cycles < 0 ? kWaitCycles : cycles, std::memory_order_relaxed);
+}
 
 Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
                   cudaStream_t st) {

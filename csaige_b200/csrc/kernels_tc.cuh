@@ -15,5 +15,8 @@ Status tc_stream_begin(saige_grm* h, int64_t rows_cap);
 Status tc_stream_tiles(saige_grm* h, int64_t mt0, int64_t mt1, cudaStream_t st);
 // Trial launches the ring-shape autotuner has timed in this process.
 int64_t tc_autotune_trials();
+// Budget of every pipeline wait of the tensor-core product, in SM cycles (< 0: the
+// default, ~2 s); 0 makes a wait that is not already satisfied give up at once.
+void tc_set_wait_budget(long long cycles);
 
 }  // namespace saige

@@ -265,6 +265,12 @@ int32_t saige_grm_matvec(saige_grm* h, const double* v, double* out, int64_t n, 
 int32_t saige_grm_matvec_dev(saige_grm* h, const double* v_dev, double* out_dev, int64_t n,
                              int32_t nrhs, int32_t precision, void* stream);
 
+/* The diagonal of the GRM, K_ii = (1/M) sum_m z_im^2 with z as OnTheFlyGrm::new
+ * standardises it (missing -> 0), in FP64: Get_Diagof_StdGeno of SAIGE's C++
+ * (src/SAIGE_fitGLMM_fast.cpp:642-680), which saige-rs does not form (its Jacobi
+ * preconditioner takes K_ii = 1, ai_reml.rs:158-164).  out has n doubles. */
+int32_t saige_grm_diag(saige_grm* h, double* out, int64_t n);
+
 /* No counterpart in the reference.  FP32 product like saige_grm_matvec_dev
  * (same kernels, same results) for callers that cannot let a library call
  * cudaMalloc: processes whose own pool already holds nearly all of the GPU's
@@ -443,6 +449,15 @@ int64_t saige_kernel_launches(void);
  * results are identical for all shapes — so tuning adds no launches.
  * SAIGE_TC_AUTOTUNE=0 in the environment keeps the fixed shape, =2 tunes every size. */
 int64_t saige_tc_autotune_trials(void);
+
+/* No counterpart in the reference (fault handling).  Every wait of the tensor-core
+ * product's pipeline (on its copies and on its MMAs) is bounded; when one runs out,
+ * the kernel stops issuing work, lets what it already issued complete, frees its
+ * tensor memory and returns, and the call reports SAIGE_TIMEOUT; the handle and the
+ * context stay usable.  This sets the bound in SM cycles for the whole process:
+ * cycles < 0 restores the default (~2 s), 0 makes every wait that is not already
+ * satisfied give up at once (how the timeout path is tested). */
+int32_t saige_tc_set_wait_budget(int64_t cycles);
 
 /* ---------------------------------------------------------------------
  * Explicit GRM: replaces compute_dense_grm (saige-core/src/grm/dense.rs:22-112),

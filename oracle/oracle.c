@@ -376,6 +376,65 @@ int orc_grm_matvec_f32_packed(const uint8_t* bed_body, int64_t bpm, int64_t n,
   return nt;
 }
 
+int orc_grm_matmul_f64_packed(const uint8_t* bed_body, int64_t bpm, int64_t n,
+                              const int64_t* rows, int64_t m, const double* af, const double* v,
+                              int nrhs, double* out) {
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  const int R = nrhs;
+  double* lut = (double*)malloc(sizeof(double) * 4 * (size_t)(m > 0 ? m : 1));
+  double* u = (double*)calloc((size_t)(m > 0 ? m : 1) * (size_t)R, sizeof(double));
+  double* accs = (double*)calloc((size_t)n * (size_t)R * (size_t)nt, sizeof(double));
+  for (int64_t j = 0; j < m; ++j) {
+    const double p = af[j], denom = sqrt(2.0 * p * (1.0 - p));
+    double* l = lut + 4 * j;
+    l[0] = l[1] = l[2] = l[3] = 0.0;
+    if (denom > 1e-10) {
+      l[0] = (2.0 - 2.0 * p) / denom;
+      l[2] = (1.0 - 2.0 * p) / denom;
+      l[3] = (0.0 - 2.0 * p) / denom;
+    }
+  }
+#pragma omp parallel num_threads(nt)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* acc = accs + (size_t)tid * (size_t)n * (size_t)R;
+    double d[64];
+#pragma omp for schedule(dynamic, 16)
+    for (int64_t j = 0; j < m; ++j) {
+      const uint8_t* row = bed_body + rows[j] * bpm;
+      const double* l = lut + 4 * j;
+      for (int c = 0; c < R; ++c) d[c] = 0.0;
+      for (int64_t i = 0; i < n; ++i) {
+        const double z = l[(row[i >> 2] >> ((i & 3) * 2)) & 3];
+        if (z != 0.0)
+          for (int c = 0; c < R; ++c) d[c] += z * v[(int64_t)c * n + i];
+      }
+      for (int c = 0; c < R; ++c) u[j * R + c] = d[c];
+      for (int64_t i = 0; i < n; ++i) {
+        const double z = l[(row[i >> 2] >> ((i & 3) * 2)) & 3];
+        if (z != 0.0)
+          for (int c = 0; c < R; ++c) acc[(int64_t)c * n + i] += z * d[c];
+      }
+    }
+  }
+  const double scale = m > 0 ? 1.0 / (double)m : 0.0;
+  for (int64_t k = 0; k < n * R; ++k) {
+    double s = 0.0;
+    for (int t = 0; t < nt; ++t) s += accs[(size_t)t * (size_t)n * (size_t)R + (size_t)k];
+    out[k] = s * scale;
+  }
+  free(lut);
+  free(u);
+  free(accs);
+  return nt;
+}
+
 /* ===================================================================== */
 /* Dense linear algebra (saige-linalg/src/decomposition.rs)               */
 /* ===================================================================== */
@@ -599,12 +658,69 @@ typedef struct {
   int64_t n, m;
   int kmode;
   int64_t n_kv;
+  float* z32;  /* kmode 2: Z as f32, built once per fit (OnTheFlyGrm::new, pcg.rs:101-122) */
 } grm_ctx;
+
+/* kmode 2 of ORC_K_OTF: the saige-rs product as it runs, on all host threads —
+ * f32 Z (marker-major), per marker an f32 dot then an f32 axpy into the thread's
+ * accumulator, chunks of >= 64 markers per task (the rayon fold of pcg.rs:149-169),
+ * the per-thread accumulators summed in f32 (the reduce, :170-176), then x(1/M). */
+static void grm_matvec_f32_parallel(const float* z32, int64_t n, int64_t m, const double* v,
+                                    double* out) {
+  int nt = 1;
+#ifdef _OPENMP
+  nt = omp_get_max_threads();
+#endif
+  float* v32 = (float*)malloc(sizeof(float) * (size_t)n);
+  float* accs = (float*)calloc((size_t)n * (size_t)nt, sizeof(float));
+  for (int64_t i = 0; i < n; ++i) v32[i] = (float)v[i];
+#pragma omp parallel num_threads(nt)
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    float* acc = accs + (size_t)tid * (size_t)n;
+#pragma omp for schedule(dynamic, 64)
+    for (int64_t j = 0; j < m; ++j) {
+      const float* zj = z32 + j * n;
+      float dot = 0.0f;
+      for (int64_t i = 0; i < n; ++i) dot += zj[i] * v32[i];
+      for (int64_t i = 0; i < n; ++i) acc[i] += zj[i] * dot;
+    }
+  }
+  const float scale = 1.0f / (float)m;
+  for (int64_t i = 0; i < n; ++i) {
+    float s = 0.0f;
+    for (int t = 0; t < nt; ++t) s += accs[(size_t)t * (size_t)n + i];
+    out[i] = (double)(s * scale);
+  }
+  free(v32);
+  free(accs);
+}
+
+static void grm_ctx_init(grm_ctx* g, int kind, const double* grm, int64_t n, int64_t m,
+                         int kmode) {
+  g->kind = kind;
+  g->grm = grm;
+  g->n = n;
+  g->m = m;
+  g->kmode = kmode;
+  g->n_kv = 0;
+  g->z32 = NULL;
+  if (kind == ORC_K_OTF && kmode == 2 && m > 0) {
+    g->z32 = (float*)malloc(sizeof(float) * (size_t)n * (size_t)m);
+#pragma omp parallel for schedule(static)
+    for (int64_t k = 0; k < n * m; ++k) g->z32[k] = (float)grm[k];
+  }
+}
 
 static void grm_apply(grm_ctx* g, const double* v, double* out) {
   g->n_kv += 1;
   if (g->kind == ORC_K_IDENTITY) {
     for (int64_t i = 0; i < g->n; ++i) out[i] = v[i];
+  } else if (g->kind == ORC_K_OTF && g->z32) {
+    grm_matvec_f32_parallel(g->z32, g->n, g->m, v, out);
   } else if (g->kind == ORC_K_OTF) {
     orc_grm_matvec(g->grm, g->n, g->m, v, out, g->kmode);
   } else {
@@ -650,11 +766,13 @@ int orc_pcg_sigma(const double* y_unused, int kind, const double* grm, int64_t n
                   const double* x0, double tol, int max_iter, double* x, int* iters,
                   double* resid, int* converged) {
   (void)y_unused;
-  grm_ctx g = {kind, grm, n, m, kmode, 0};
+  grm_ctx g;
+  grm_ctx_init(&g, kind, grm, n, m, kmode);
   double* tmp = (double*)malloc(sizeof(double) * (size_t)n);
   sigma_ctx s = {&g, w, tau[0], tau[1], tmp};
   *converged = orc_pcg_core(sigma_op, &s, sigma_pre, &s, n, b, x0, tol, max_iter, x, iters, resid);
   free(tmp);
+  free(g.z32);
   return 0;
 }
 
@@ -711,7 +829,8 @@ int orc_fit_ai_reml(const double* y, const double* x, int64_t n, int p, int t, i
     mu[i] = orc_update_mu(t, e);
   }
 
-  grm_ctx g = {kind, grm, n, m, kmode, 0};
+  grm_ctx g;
+  grm_ctx_init(&g, kind, grm, n, m, kmode);
   int64_t pcg_total = 0;
   int converged = 0, n_iter = 0;
   double l[64 * 64], c[64 * 64];
@@ -878,6 +997,7 @@ int orc_fit_ai_reml(const double* y, const double* x, int64_t n, int p, int t, i
   if (w_out) memcpy(w_out, w, nb);
   free(eta); free(mu); free(w); free(ytil); free(sinvy); free(sinvx); free(xcol); free(py);
   free(kpy); free(su); free(ku); free(pk); free(invw_py); free(tmp); free(probes);
+  free(g.z32);
   return 0;
 }
 
@@ -1139,4 +1259,202 @@ void orc_grm_from_dosages(const double* dosages, const double* af, int64_t n, in
   orc_grm_accumulate(z, n, used, out);
   *n_used = used;
   free(z);
+}
+
+/* ===================================================================== */
+/* Synthetic cohorts (no reference counterpart; test and benchmark input) */
+/* ===================================================================== */
+/* A second statement of the library's seeded generator: every draw is a
+ * splitmix64-based hash of (seed, tag, indices); relatives share founder
+ * haplotypes (sibling pairs, first-cousin pairs); MCAR missing calls. */
+enum { GEN_MAF = 1, GEN_HAP = 2, GEN_REC = 3, GEN_REC2 = 4, GEN_MISS = 5, GEN_COV = 6,
+       GEN_EFFECT = 7, GEN_Y = 8, GEN_NOISE = 9 };
+
+static uint64_t gen_mix(uint64_t z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+static uint64_t gen_hash(uint64_t seed, uint64_t tag, uint64_t a, uint64_t b) {
+  uint64_t h = gen_mix(seed ^ (tag * 0xD6E8FEB86659FD93ull));
+  h = gen_mix(h ^ (a * 0x9FB21C651E98DF25ull));
+  return gen_mix(h + b);
+}
+
+static double gen_u01(uint64_t h) { return (double)(h >> 11) * (1.0 / 9007199254740992.0); }
+
+typedef struct {
+  int64_t n, m, n_sib, n_cous, block;
+  uint64_t seed;
+  double maf_lo, maf_hi, miss;
+} gen_layout;
+
+static gen_layout gen_make_layout(const orc_cohort_spec* s) {
+  gen_layout L;
+  int64_t ns = (int64_t)(s->sib_frac * (double)s->n) / 2 * 2;
+  int64_t nc = (int64_t)(s->cousin_frac * (double)s->n) / 2 * 2;
+  if (ns < 0) ns = 0;
+  if (nc < 0) nc = 0;
+  if (ns > s->n / 2 * 2) ns = s->n / 2 * 2;
+  if (ns + nc > s->n) nc = (s->n - ns) / 2 * 2;
+  L.n = s->n;
+  L.m = s->m;
+  L.n_sib = ns;
+  L.n_cous = nc;
+  L.block = s->m > 64 ? (s->m + 63) / 64 : 1;  /* markers per recombination segment */
+  L.seed = s->seed;
+  L.maf_lo = s->maf_lo;
+  L.maf_hi = s->maf_hi;
+  L.miss = s->missing_rate;
+  return L;
+}
+
+static double gen_af(const gen_layout* L, int64_t m) {
+  return L->maf_lo + (L->maf_hi - L->maf_lo) * gen_u01(gen_hash(L->seed, GEN_MAF, (uint64_t)m, 0));
+}
+
+/* founder haplotype slot (0..7) of the family anchored at sample `base` */
+static int gen_hap(const gen_layout* L, int64_t m, double p, int64_t base, int slot) {
+  uint64_t f = ((uint64_t)base << 3) | (uint64_t)slot;
+  return gen_u01(gen_hash(L->seed, GEN_HAP, (uint64_t)m, f)) < p ? 1 : 0;
+}
+
+static int gen_rec(const gen_layout* L, uint64_t tag, uint64_t who, int64_t m) {
+  return (int)(gen_hash(L->seed, tag, who, (uint64_t)(m / L->block)) & 1ull);
+}
+
+/* alternate-allele count 0..2 of sample i at marker m */
+static int gen_genotype(const gen_layout* L, int64_t m, int64_t i, double p) {
+  if (i < L->n_sib) {  /* a sibling pair shares parents A (slots 0,1) and B (2,3) */
+    int64_t base = i & ~(int64_t)1;
+    int a = gen_rec(L, GEN_REC, ((uint64_t)i << 1) | 0u, m);
+    int b = gen_rec(L, GEN_REC, ((uint64_t)i << 1) | 1u, m);
+    return gen_hap(L, m, p, base, a) + gen_hap(L, m, p, base, 2 + b);
+  }
+  if (i < L->n_sib + L->n_cous) {  /* cousins: children of two children of G (0,1) x H (2,3) */
+    int64_t j = L->n_sib + ((i - L->n_sib) & ~(int64_t)1);
+    int c = (int)((i - L->n_sib) & 1);
+    int which = gen_rec(L, GEN_REC, ((uint64_t)i << 1) | 0u, m);
+    int slot = which == 0
+                   ? gen_rec(L, GEN_REC2, ((uint64_t)j << 2) | ((uint64_t)c << 1) | 0u, m)
+                   : 2 + gen_rec(L, GEN_REC2, ((uint64_t)j << 2) | ((uint64_t)c << 1) | 1u, m);
+    return gen_hap(L, m, p, j, slot) + gen_hap(L, m, p, j, 4 + c);
+  }
+  return gen_hap(L, m, p, i, 0) + gen_hap(L, m, p, i, 1);
+}
+
+static uint32_t gen_code(const gen_layout* L, int64_t m, int64_t i, double p) {
+  if (L->miss > 0.0 && gen_u01(gen_hash(L->seed, GEN_MISS, (uint64_t)m, (uint64_t)i)) < L->miss)
+    return 1u;  /* 01: missing */
+  int g = gen_genotype(L, m, i, p);
+  return g == 2 ? 0u : (g == 1 ? 2u : 3u);
+}
+
+void orc_gen_bed(const orc_cohort_spec* spec, uint8_t* bed_out) {
+  gen_layout L = gen_make_layout(spec);
+  const int64_t bpm = (spec->n + 3) / 4;
+  bed_out[0] = 0x6C;
+  bed_out[1] = 0x1B;
+  bed_out[2] = 0x01;
+#pragma omp parallel for schedule(dynamic, 16)
+  for (int64_t m = 0; m < spec->m; ++m) {
+    const double p = gen_af(&L, m);
+    uint8_t* row = bed_out + 3 + m * bpm;
+    for (int64_t b = 0; b < bpm; ++b) {
+      uint32_t v = 0;
+      for (int k = 0; k < 4; ++k) {
+        int64_t i = b * 4 + k;
+        if (i < L.n) v |= gen_code(&L, m, i, p) << (2 * k);
+      }
+      row[b] = (uint8_t)v;
+    }
+  }
+}
+
+static double gen_normal(uint64_t h1, uint64_t h2) {  /* Box-Muller, u1 in (0, 1] */
+  const double u1 = 1.0 - gen_u01(h1);
+  const double u2 = gen_u01(h2);
+  return sqrt(-2.0 * log(u1)) * cos(6.283185307179586 * u2);
+}
+
+void orc_gen_pheno(const orc_cohort_spec* spec, double* y, double* x) {
+  gen_layout L = gen_make_layout(spec);
+  const int64_t n = spec->n;
+  const int p = 1 + spec->n_covar;
+  double beta[64] = {0};
+  /* covariates: intercept, N(0,1) (effect 0.3), Bernoulli(0.5) (0.2), then N(0,1) (0.1) */
+  for (int64_t i = 0; i < n; ++i) x[i] = 1.0;
+  for (int k = 1; k < p; ++k) {
+    beta[k] = k == 1 ? 0.3 : (k == 2 ? 0.2 : 0.1);
+    for (int64_t i = 0; i < n; ++i) {
+      double v;
+      if (k == 2) v = gen_u01(gen_hash(L.seed, GEN_COV, (uint64_t)i, (uint64_t)(2 * k))) < 0.5 ? 1.0 : 0.0;
+      else v = gen_normal(gen_hash(L.seed, GEN_COV, (uint64_t)i, (uint64_t)(2 * k)),
+                          gen_hash(L.seed, GEN_COV, (uint64_t)i, (uint64_t)(2 * k + 1)));
+      x[(int64_t)k * n + i] = v;
+    }
+  }
+  /* polygenic score over evenly spaced causal markers (true genotypes), standardised */
+  int64_t nc = spec->n_causal > 0 ? spec->n_causal : 500;
+  if (nc > spec->m) nc = spec->m;
+  if (nc < 1) nc = 1;
+  const int64_t stride = spec->m / nc;
+  double* pgs = (double*)calloc((size_t)n, sizeof(double));
+#pragma omp parallel for schedule(static)
+  for (int64_t i = 0; i < n; ++i) {
+    double acc = 0.0;
+    for (int64_t c = 0; c < nc; ++c) {
+      const int64_t m = c * stride;
+      const double pm = gen_af(&L, m);
+      const double sd = sqrt(2.0 * pm * (1.0 - pm));
+      const double b = gen_normal(gen_hash(L.seed, GEN_EFFECT, (uint64_t)m, 0),
+                                  gen_hash(L.seed, GEN_EFFECT, (uint64_t)m, 1));
+      acc += b * ((double)gen_genotype(&L, m, i, pm) - 2.0 * pm) / sd;
+    }
+    pgs[i] = acc;
+  }
+  double mean = 0.0, var = 0.0;
+  for (int64_t i = 0; i < n; ++i) mean += pgs[i];
+  mean /= (double)n;
+  for (int64_t i = 0; i < n; ++i) var += (pgs[i] - mean) * (pgs[i] - mean);
+  var /= (double)n;
+  const double sdv = var > 0 ? sqrt(var) : 1.0;
+  for (int64_t i = 0; i < n; ++i) pgs[i] = (pgs[i] - mean) / sdv;
+  double* lin = (double*)calloc((size_t)n, sizeof(double));
+  for (int64_t i = 0; i < n; ++i) {
+    double e = 0.0;
+    for (int k = 1; k < p; ++k) e += beta[k] * x[(int64_t)k * n + i];
+    lin[i] = e;
+  }
+  if (spec->trait == 1 /* quantitative */) {
+    const double h2 = spec->h2;
+    for (int64_t i = 0; i < n; ++i) {
+      const double eps = gen_normal(gen_hash(L.seed, GEN_NOISE, (uint64_t)i, 0),
+                                    gen_hash(L.seed, GEN_NOISE, (uint64_t)i, 1));
+      y[i] = lin[i] + sqrt(h2) * pgs[i] + sqrt(1.0 - h2) * eps;
+    }
+  } else {
+    /* binary: genetic sd on the logistic liability scale for h2, intercept by
+     * bisection so that the mean risk equals the prevalence */
+    const double h2 = spec->h2 < 0.99 ? spec->h2 : 0.99;
+    const double sg = sqrt(h2 * (M_PI * M_PI / 3.0) / (1.0 - h2));
+    const double prev = spec->prevalence > 0 && spec->prevalence < 1 ? spec->prevalence : 0.1;
+    double lo = -30.0, hi = 30.0;
+    for (int it = 0; it < 100; ++it) {
+      const double mid = 0.5 * (lo + hi);
+      double s = 0.0;
+      for (int64_t i = 0; i < n; ++i) s += 1.0 / (1.0 + exp(-(mid + lin[i] + sg * pgs[i])));
+      if (s / (double)n < prev) lo = mid;
+      else hi = mid;
+    }
+    const double b0 = 0.5 * (lo + hi);
+    for (int64_t i = 0; i < n; ++i) {
+      const double mu = 1.0 / (1.0 + exp(-(b0 + lin[i] + sg * pgs[i])));
+      y[i] = gen_u01(gen_hash(L.seed, GEN_Y, (uint64_t)i, 0)) < mu ? 1.0 : 0.0;
+    }
+  }
+  free(pgs);
+  free(lin);
 }

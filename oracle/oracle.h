@@ -72,6 +72,14 @@ void orc_grm_explicit(const double* z, int64_t n, int64_t m, double* k_out);
  * fold/reduce does) on packed PLINK rows: markers rows[0..m) of the .bed
  * body (bed points past the 3-byte header), all n_fam samples in order.
  * threads <= 0 uses every OpenMP thread.  Returns the threads used. */
+/* The product K V = Z (Z' V) / M of pcg.rs:101-180 in FP64 (its own summation order)
+ * (z = (g - 2p)/sqrt(2p(1-p)) in f64, missing -> 0, zero rows when the denominator is
+ * <= 1e-10) on packed rows, nrhs columns of n (column-major) at once, all threads:
+ * the FP64 reference for the accuracy of the GPU products at sizes where an explicit
+ * Z does not fit in host memory.  Returns the threads used. */
+int orc_grm_matmul_f64_packed(const uint8_t* bed_body, int64_t bytes_per_marker, int64_t n,
+                              const int64_t* rows, int64_t m, const double* af, const double* v,
+                              int nrhs, double* out);
 int orc_grm_matvec_f32_packed(const uint8_t* bed_body, int64_t bytes_per_marker, int64_t n,
                               const int64_t* rows, int64_t m, const double* af, const double* v,
                               double* out, int threads);
@@ -115,7 +123,9 @@ typedef struct {
 /* GRM operator kinds for the AI-REML oracle. */
 enum { ORC_K_IDENTITY = 0, ORC_K_OTF = 1, ORC_K_EXPLICIT = 2 };
 
-/* grm: for ORC_K_OTF the standardized z (m x n, marker-major) with kmode 0/1;
+/* grm: for ORC_K_OTF the standardized z (m x n, marker-major) with kmode 0 (FP64),
+ * 1 (saige-rs f32 arithmetic, one thread) or 2 (saige-rs f32 arithmetic on all host
+ * threads: the rayon fold and reduce of pcg.rs:149-176);
  * for ORC_K_EXPLICIT the dense n x n K (row-major).  tau_trace (optional,
  * length 2*max_iter) receives tau after each iteration.  alpha/mu/eta/w
  * (optional) receive the final state. */
@@ -185,6 +195,26 @@ int orc_dense_grm_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t
  * NaN = missing), af as given, only the 2 af (1 - af) < 1e-10 skip. */
 void orc_grm_from_dosages(const double* dosages, const double* af, int64_t n, int64_t m,
                           double* out, int64_t* n_used);
+
+/* ---------------------------------------------------------------------
+ * The seeded synthetic cohort of the tests and the benchmark (no reference
+ * counterpart), restated from the library's generator so that the CPU arm of the
+ * benchmark needs nothing from the library; the tests check both byte for byte.
+ * Same fields and layout as saige_cohort_spec.
+ * ------------------------------------------------------------------- */
+typedef struct {
+  uint64_t seed;
+  int64_t n, m;
+  double sib_frac, cousin_frac, missing_rate, maf_lo, maf_hi;
+  int32_t trait, n_covar;
+  double prevalence, h2;
+  int32_t n_causal, reserved;
+} orc_cohort_spec;
+
+/* .bed bytes (3-byte header + m * ceil(n/4)), all host threads. */
+void orc_gen_bed(const orc_cohort_spec* spec, uint8_t* bed_out);
+/* y (n) and x (n x (1 + n_covar), column-major, intercept first). */
+void orc_gen_pheno(const orc_cohort_spec* spec, double* y, double* x);
 
 #ifdef __cplusplus
 }

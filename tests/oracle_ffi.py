@@ -353,3 +353,54 @@ def chacha8(seed: int) -> ChaChaRng:
     r = ChaChaRng()
     L.orc_chacha_seed_from_u64(C.byref(r), seed, 8)
     return r
+
+
+# ---- synthetic cohorts (the library's generator, restated) ------------------
+class CohortSpec(C.Structure):
+    _fields_ = [("seed", C.c_uint64), ("n", C.c_int64), ("m", C.c_int64),
+                ("sib_frac", C.c_double), ("cousin_frac", C.c_double),
+                ("missing_rate", C.c_double), ("maf_lo", C.c_double), ("maf_hi", C.c_double),
+                ("trait", C.c_int32), ("n_covar", C.c_int32), ("prevalence", C.c_double),
+                ("h2", C.c_double), ("n_causal", C.c_int32), ("reserved", C.c_int32)]
+
+
+L.orc_gen_bed.argtypes = [P(CohortSpec), P(C.c_uint8)]
+L.orc_gen_pheno.argtypes = [P(CohortSpec), _d, _d]
+
+
+def cohort_spec(seed=12345, n=2000, m=5000, sib_frac=0.10, cousin_frac=0.0, missing_rate=0.01,
+                maf_lo=0.01, maf_hi=0.5, trait=BINARY, n_covar=2, prevalence=0.10, h2=0.2,
+                n_causal=500) -> CohortSpec:
+    return CohortSpec(seed, n, m, sib_frac, cousin_frac, missing_rate, maf_lo, maf_hi, trait,
+                      n_covar, prevalence, h2, n_causal, 0)
+
+
+def gen_bed(spec: CohortSpec) -> np.ndarray:
+    out = np.empty(3 + spec.m * ((spec.n + 3) // 4), dtype=np.uint8)
+    L.orc_gen_bed(C.byref(spec), out.ctypes.data_as(P(C.c_uint8)))
+    return out
+
+
+def gen_pheno(spec: CohortSpec):
+    y = np.empty(spec.n)
+    x = np.empty(spec.n * (1 + spec.n_covar))
+    L.orc_gen_pheno(C.byref(spec), dp(y), dp(x))
+    return y, x.reshape(1 + spec.n_covar, spec.n).T
+
+
+L.orc_grm_matmul_f64_packed.restype = C.c_int
+L.orc_grm_matmul_f64_packed.argtypes = [P(C.c_uint8), C.c_int64, C.c_int64, _i64, C.c_int64, _d,
+                                        _d, C.c_int, _d]
+
+
+def grm_matmul_f64_packed(bed: np.ndarray, n: int, rows, af, v: np.ndarray) -> np.ndarray:
+    """FP64 K V on the packed .bed rows `rows` (all n samples in file order); v is
+    (nrhs, n) or (n,); af per row."""
+    vv = np.ascontiguousarray(np.atleast_2d(v), dtype=np.float64)
+    assert vv.shape[0] <= 64
+    rows = np.ascontiguousarray(rows, dtype=np.int64)
+    out = np.empty_like(vv)
+    body = np.ascontiguousarray(bed[3:])
+    L.orc_grm_matmul_f64_packed(body.ctypes.data_as(P(C.c_uint8)), (n + 3) // 4, n, ip(rows),
+                                rows.size, dp(f64(af)), dp(vv), vv.shape[0], dp(out))
+    return out if np.ndim(v) == 2 else out[0]

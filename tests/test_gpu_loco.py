@@ -69,4 +69,4 @@ def test_fp32_loco_matches_refit_and_oracle(cohort):
     z = O.standardize(O.dosages(c["bed"], c["n"], rest), c["af"][rest], 0)
     orc = O.fit_ai_reml(c["y"], c["x"], O.BINARY, O.K_EXPLICIT, O.grm_explicit(z), max_iter=6,
                         tol=1e-5)
-    assert abs(res[chrom].tau[1] - orc["tau"][1]) <= 1e-3 * abs(orc["tau"][1])
+    assert abs(res[chrom].tau[1] - orc["tau"][1]) <= 1e-4 * abs(orc["tau"][1])

@@ -203,9 +203,9 @@ def test_ai_reml_matches_fp64_oracle(trait):
     o = O.fit_ai_reml(y, x, trait, O.K_EXPLICIT, k, max_iter=6, tol=1e-5)
     assert r.iterations == o["iterations"]
     print("tau gpu", r.tau, "oracle", o["tau"], "rel", np.abs(r.tau - o["tau"]) / o["tau"])
-    assert np.all(np.abs(r.tau - o["tau"]) <= 1e-3 * np.abs(o["tau"]))
-    assert np.abs(r.tau_trace - o["tau_trace"]).max() <= 1e-3 * np.abs(o["tau_trace"]).max()
-    assert _rel(r.alpha, o["alpha"]) < 1e-3
+    assert np.all(np.abs(r.tau - o["tau"]) <= 1e-4 * np.abs(o["tau"]))
+    assert np.abs(r.tau_trace - o["tau_trace"]).max() <= 1e-4 * np.abs(o["tau_trace"]).max()
+    assert _rel(r.alpha, o["alpha"]) < 1e-4
 
 
 def test_ai_reml_block_and_warm_start_agree():
@@ -215,5 +215,16 @@ def test_ai_reml_block_and_warm_start_agree():
                          cs.AiRemlConfig(max_iter=5, tol=1e-5, solve=cs.SOLVE_BLOCK,
                                          warm_start=cs.WARM_PREVIOUS))
     print("tau single", base.tau, "block+warm", blk.tau, base.pcg_iters, blk.pcg_iters)
-    assert np.all(np.abs(blk.tau - base.tau) <= 1e-3 * np.abs(base.tau))
+    assert np.all(np.abs(blk.tau - base.tau) <= 1e-4 * np.abs(base.tau))
     assert blk.n_kv_launches < base.n_kv_launches
+
+
+# ---------------------------------------------------------------- diag K
+@pytest.mark.parametrize("n,m,sub", [(1001, 300, False), (1500, 257, True)])
+def test_grm_diag_matches_oracle(n, m, sub):
+    """Get_Diagof_StdGeno (src/SAIGE_fitGLMM_fast.cpp:642-680): diag of the FP64 GRM."""
+    sidx = np.random.default_rng(n).permutation(n)[: n - 137] if sub else None
+    grm, dos, afs = _grm_case(n=n, m=m, sidx=sidx)
+    k = O.grm_explicit(O.standardize(dos, afs, 0))
+    got = grm.diag()
+    assert np.abs(got - np.diag(k)).max() <= 1e-12 * np.abs(np.diag(k)).max()

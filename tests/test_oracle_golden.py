@@ -151,3 +151,16 @@ def test_standardize_missing_is_exact_zero():
     assert z[0, 1] == 0.0
     z0 = O.standardize(dos, [0.0], 0)  # denominator 0 -> zero column
     assert np.all(z0 == 0.0)
+
+
+def test_packed_f64_product_equals_dense_fp64_product():
+    spec = O.cohort_spec(n=701, m=300, seed=9, missing_rate=0.03)
+    bed = O.gen_bed(spec)
+    af, mac, nv = O.marker_stats(bed, 701, 300)
+    keep = np.nonzero((af > 0.01) & (af < 0.99))[0]
+    z = O.standardize(O.dosages(bed, 701, keep), af[keep], 0)
+    v = np.random.default_rng(4).standard_normal((3, 701))
+    got = O.grm_matmul_f64_packed(bed, 701, keep, af[keep], v)
+    for c in range(3):
+        want = O.grm_matvec(z, v[c], 0)
+        assert np.abs(got[c] - want).max() <= 1e-12 * np.abs(want).max()

@@ -80,3 +80,41 @@ def test_both_sides_take_the_same_handoffs(sa, hb):
                     assert 1 <= bar <= sa // hb
                     if i + 2 < len(mma) and sa // hb == 2:
                         assert mma[i + 2][0] == bar
+
+
+def producer_side(nk, sub, sl, abort_at):
+    """The producer's loop with the slot-reuse wait giving up at load stage abort_at
+    (no abort when abort_at >= the stage count), then its drain: the (slot, parity)
+    pairs of FULL it waits on before the CTA exits."""
+    n_load = (nk + sub - 1) // sub
+    S = ph = issued = 0
+    for J in range(n_load):
+        if J >= sl and J >= abort_at:
+            break  # mbar_wait_sleep(LDONE) gave up
+        assert S == J % sl and ph == (J // sl) & 1
+        issued = J + 1
+        S += 1
+        if S == sl:
+            S, ph = 0, ph ^ 1
+    drain = [(J, J % sl, (J // sl) & 1) for J in range(max(0, issued - sl), issued)]
+    return n_load, issued, drain
+
+
+@pytest.mark.parametrize("sub", [1, 2, 4])
+@pytest.mark.parametrize("sl", [2, 3, 5, 24])
+def test_producer_drain_covers_every_copy_in_flight(sub, sl):
+    for nk in list(range(1, 30)) + [141, 1564]:
+        n_load = (nk + sub - 1) // sub
+        for abort_at in sorted({0, 1, sl - 1, sl, sl + 1, 2 * sl, n_load - 1, n_load, 10 ** 9}):
+            n, issued, drain = producer_side(nk, sub, sl, abort_at)
+            if abort_at >= n:
+                assert issued == n  # no abort: every stage issued
+            # stage J was issued only after stage J - sl was consumed (its LDONE phase),
+            # so the stages not in the drain list are complete; the drain waits on
+            # distinct slots, each at the parity of its one outstanding phase
+            consumed = set(range(0, max(0, issued - sl)))
+            drained = {J for J, _, _ in drain}
+            assert consumed | drained == set(range(issued))
+            assert len({slot for _, slot, _ in drain}) == len(drain) <= sl
+            for J, slot, par in drain:
+                assert slot == J % sl and par == (J // sl) & 1
