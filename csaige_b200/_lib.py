@@ -229,6 +229,7 @@ SIGNATURES = {
     ),
     "saige_grm_diag": (C.c_int32, [_vp, _d, C.c_int64]),
     "saige_tc_set_wait_budget": (C.c_int32, [C.c_int64]),
+    "saige_grm_noalloc_scratch_bytes": (C.c_int32, [_vp, P(_sz), P(_sz)]),
     "saige_release_cached_memory": (C.c_int32, []),
     "saige_write_null_model": (C.c_int32, [C.c_char_p, P(NullModelC)]),
     "saige_xvx_inv_xv": (C.c_int32, [_d, _d, C.c_int64, C.c_int32, _d]),

@@ -210,12 +210,17 @@ struct Recycle {
 constexpr double kLearnR2Min = 0.25;
 // PCG iterations of the block solve whose y and X search directions are kept
 constexpr int kKeepIters = 3;
+// At most this many kept directions (each costs two n-vectors of workspace plus a
+// column of every recycled basis and Galerkin system): the first kKeepIters
+// iterations of y and up to 15 covariates; with more covariates the later columns'
+// directions are not kept.
+constexpr int kKeepMaxCols = 48;
 
 Status recycle_init(Fit& f, Recycle& rc, bool learned, const double* diagk, uint64_t seed) {
   const size_t ld = (size_t)f.ld, q = (size_t)f.q;
   rc.learned = learned;
   rc.diagk = diagk;
-  rc.keep_cap = (1 + f.p) * kKeepIters;
+  rc.keep_cap = std::min((1 + f.p) * kKeepIters, kKeepMaxCols);
   rc.mb_max = (learned ? 3 * f.q + 1 : 2 * f.q + 1) + rc.keep_cap;
   rc.nk = learned ? 2 * f.q + 3 : f.q + 3;
   if (learned) {
@@ -930,12 +935,11 @@ SG_API int32_t saige_fit_ai_reml(saige_grm* h, const double* y, const double* x,
     if (c.n_random_vectors <= 0) return fail(SAIGE_EINVAL, "n_random_vectors must be positive").code;
     if (c.max_iter < 0) return fail(SAIGE_EINVAL, "max_iter must be >= 0").code;
     std::lock_guard<std::recursive_mutex> lk(h->mu);
-    int prev = -1;
-    cudaGetDevice(&prev);
-    cudaSetDevice(h->device);
-    Status s = fit_impl(h, y, x, n, p, trait, &c, out, alpha, mu, eta, w, tau_trace);
-    if (prev >= 0) cudaSetDevice(prev);
-    return s.code;
+    DeviceGuard dg(h->device);
+    if (!dg.ok) return fail(SAIGE_ECUDA, "cannot make device %d current", h->device).code;
+    // the fit's work is ordered on the handle's stream
+    ReleaseScope rs(ReleaseMode::kStream, h->stream);
+    return fit_impl(h, y, x, n, p, trait, &c, out, alpha, mu, eta, w, tau_trace).code;
   } catch (const std::bad_alloc&) {
     return fail(SAIGE_ENOMEM, "host allocation failed").code;
   } catch (...) {
@@ -977,9 +981,9 @@ SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t
     if (cfg) c = *cfg;
     else saige_ai_reml_config_default(&c);
     std::lock_guard<std::recursive_mutex> lk(h->mu);
-    int prev = -1;
-    cudaGetDevice(&prev);
-    cudaSetDevice(h->device);
+    DeviceGuard dg(h->device);
+    if (!dg.ok) return fail(SAIGE_ECUDA, "cannot make device %d current", h->device).code;
+    ReleaseScope rs(ReleaseMode::kStream, h->stream);
     Status s;
     {
       MaskGuard guard(h);
@@ -1003,7 +1007,6 @@ SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t
         h->masked = false;
       }
     }
-    if (prev >= 0) cudaSetDevice(prev);
     return s.code;
   } catch (const std::bad_alloc&) {
     return fail(SAIGE_ENOMEM, "host allocation failed").code;

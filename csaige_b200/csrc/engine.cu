@@ -111,7 +111,7 @@ Status DevBuf::reserve(size_t want) {
   if (want == 0) return Status();
   int d = 0;
   if (cudaGetDevice(&d) != cudaSuccess) d = 0;
-  if (want >= kCacheMinBytes && cache_take(d, want, &ptr, &bytes)) {
+  if (cache_take(d, want, &ptr, &bytes)) {
     dev = d;
     return Status();
   }
@@ -131,15 +131,37 @@ Status DevBuf::reserve(size_t want) {
   return Status();
 }
 
+namespace {
+thread_local ReleaseMode tl_release_mode = ReleaseMode::kDevice;
+thread_local cudaStream_t tl_release_stream = nullptr;
+}  // namespace
+
+ReleaseScope::ReleaseScope(ReleaseMode mode, cudaStream_t stream)
+    : prev_mode(tl_release_mode), prev_stream(tl_release_stream) {
+  tl_release_mode = mode;
+  tl_release_stream = stream;
+}
+
+ReleaseScope::~ReleaseScope() {
+  tl_release_mode = prev_mode;
+  tl_release_stream = prev_stream;
+}
+
 void DevBuf::release() {
   if (ptr) {
-    if (bytes >= kCacheMinBytes && dev >= 0) {
-      // as cudaFree would, wait for the device's work before the block can be reused
-      int cur = -1;
-      cudaGetDevice(&cur);
-      if (cur != dev) cudaSetDevice(dev);
-      cudaDeviceSynchronize();
-      if (cur >= 0 && cur != dev) cudaSetDevice(cur);
+    const ReleaseMode mode = tl_release_mode;
+    if (dev >= 0 && (bytes >= kCacheMinBytes || mode != ReleaseMode::kDevice)) {
+      // as cudaFree would, wait for the work that may still use the block before it
+      // can be reused: the device's, the scope's stream, or none when it is idle
+      if (mode == ReleaseMode::kStream) {
+        cudaStreamSynchronize(tl_release_stream);
+      } else if (mode == ReleaseMode::kDevice) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != dev) cudaSetDevice(dev);
+        cudaDeviceSynchronize();
+        if (cur >= 0 && cur != dev) cudaSetDevice(cur);
+      }
       std::lock_guard<std::mutex> lk(g_cache_mu);
       g_cache.push_back(CachedBlock{dev, bytes, ptr});
     } else {
@@ -177,16 +199,6 @@ Status pick_device(int32_t want, int* dev) {
   return Status();
 }
 
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int d) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != d) cudaSetDevice(d);
-  }
-  ~DeviceGuard() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
 
 // ---------------------------------------------------------------------------
 // per-marker metadata (pcg.rs:101-122 arithmetic, done on the host in f64)
@@ -262,6 +274,8 @@ static void grm_free(saige_grm* h) {
   if (!h) return;
   cudaSetDevice(h->device);
   if (h->stream) cudaStreamSynchronize(h->stream);
+  // every buffer of the handle is used on its stream only, now idle
+  ReleaseScope idle(ReleaseMode::kIdle, nullptr);
   tc_destroy(h);
   h->v32.release();
   h->u32.release();
@@ -1223,6 +1237,7 @@ static int32_t pcg_entry(saige_grm* h, const double* w, const double tau[2], con
   std::lock_guard<std::recursive_mutex> lk(h->mu);
   DeviceGuard dg(h->device);
   cudaStream_t st = h->stream;
+  ReleaseScope rs(ReleaseMode::kStream, st);
   auto body = [&]() -> Status {
     const int64_t ld = h->n_pad;
     const size_t blk = (size_t)ld * nrhs;

@@ -12,13 +12,29 @@
 
 namespace saige {
 
-// Growable device buffer.
-// Device buffer.  Blocks of at least kCacheMinBytes go through a per-device cache:
-// release() keeps them (after synchronising their device, as cudaFree would) and
-// reserve() reuses a cached block of the same device of 1 to 1.25 times the size,
+// Growable device buffer.  Blocks of at least kCacheMinBytes go through a per-device
+// cache: release() keeps them (after synchronising their device, as cudaFree would)
+// and reserve() reuses a cached block of the same device of 1 to 1.25 times the size,
 // so that repeated fits of one cohort shape do not map and unmap tens of GB each
 // time.  release_cached_blocks() hands the cache back to the driver.
+//
+// Inside a ReleaseScope on the calling thread, release() knows more about the work
+// that may still use a block: kStream — all of it is ordered on one stream, which is
+// synchronised instead of the whole device; kIdle — none is in flight.  Such blocks
+// are cached whatever their size (cudaFree would synchronise the device), so that
+// fits running side by side on their own streams do not wait for one another.
 constexpr size_t kCacheMinBytes = (size_t)1 << 20;
+
+enum class ReleaseMode { kDevice, kStream, kIdle };
+
+struct ReleaseScope {
+  ReleaseMode prev_mode;
+  cudaStream_t prev_stream;
+  ReleaseScope(ReleaseMode mode, cudaStream_t stream);
+  ~ReleaseScope();
+  ReleaseScope(const ReleaseScope&) = delete;
+  ReleaseScope& operator=(const ReleaseScope&) = delete;
+};
 
 struct DevBuf {
   void* ptr = nullptr;
@@ -31,6 +47,28 @@ struct DevBuf {
 };
 
 void release_cached_blocks();
+
+// Makes device d current for the scope and gives the caller's device back at the
+// end, on every return path.  ok is false when d could not be made current.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = true;
+  explicit DeviceGuard(int d) {
+    if (cudaGetDevice(&prev) != cudaSuccess) {
+      prev = -1;
+      (void)cudaGetLastError();
+    }
+    if (prev != d && cudaSetDevice(d) != cudaSuccess) {
+      ok = false;
+      (void)cudaGetLastError();
+    }
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+  DeviceGuard(const DeviceGuard&) = delete;
+  DeviceGuard& operator=(const DeviceGuard&) = delete;
+};
 
 struct TcPlan;  // tensor-core path state (kernels_tc.cu)
 

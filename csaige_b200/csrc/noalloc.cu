@@ -19,6 +19,7 @@
 // GPU (different streams, or host threads enqueueing at the same time without
 // ordering their streams) race on it.  Every element a call reads is written
 // earlier in the same call, so nothing carries over between calls.
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -30,43 +31,65 @@
 namespace saige {
 namespace {
 
-// 32 MiB: enough for N up to about 1.5 million samples at any marker count
-// (the partial-sum planes shrink as N grows, see fp32_z_splits).
+// 32 MiB.  A handle needs align256(4 n_pad) + align256(4 m_pad) + 4 n_splits n_pad
+// bytes of it (noalloc_bytes): the f32 copy of v, u = Z'v and the per-split partial
+// sums of Z u, with n_pad = n rounded up to 512, m_pad = m rounded up to 128 and
+// n_splits from fp32_z_splits (fewer splits as n grows).  At 150,000 markers that
+// admits up to about 2.7 million samples; saige_grm_noalloc_scratch_bytes reports the
+// figure of a given handle.
 constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
 constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 std::mutex g_setup_mu;
-void* g_scratch_addr[kMaxDevices] = {};
+struct ScratchAddr {
+  CUcontext ctx = nullptr;  // the context the address belongs to
+  void* addr = nullptr;
+};
+ScratchAddr g_scratch_addr[kMaxDevices];
 
-// Device address of g_noalloc_scratch on `device`, looked up once per device.
+// Device address of g_noalloc_scratch on `device` (current), looked up on the first
+// call in each context: a device reset or a new primary context reloads the module,
+// and the array may then live elsewhere.
 Status scratch_address(int device, void** out) {
   if (device < 0 || device >= kMaxDevices)
     return fail(SAIGE_EINVAL, "device %d out of range for the static scratch table", device);
+  // the driver's cuCtxGetCurrent through the runtime, so that the library does not
+  // link libcuda (it must load on machines without a GPU driver)
+  static CUresult (*ctx_get_current)(CUcontext*) = nullptr;
   std::lock_guard<std::mutex> lk(g_setup_mu);
-  if (!g_scratch_addr[device]) {
+  if (!ctx_get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn) {
+      (void)cudaGetLastError();
+      return fail(SAIGE_ECUDA, "cuCtxGetCurrent is not available from the driver");
+    }
+    ctx_get_current = reinterpret_cast<CUresult (*)(CUcontext*)>(fn);
+  }
+  CUcontext ctx = nullptr;
+  if (ctx_get_current(&ctx) != CUDA_SUCCESS || !ctx)
+    return fail(SAIGE_ECUDA, "no current CUDA context on device %d", device);
+  ScratchAddr& e = g_scratch_addr[device];
+  if (!e.addr || e.ctx != ctx) {
     void* p = nullptr;
     SG_CUDA(cudaGetSymbolAddress(&p, g_noalloc_scratch));
     if (!p) return fail(SAIGE_ECUDA, "cudaGetSymbolAddress returned a null address");
-    g_scratch_addr[device] = p;
+    e.addr = p;
+    e.ctx = ctx;
   }
-  *out = g_scratch_addr[device];
+  *out = e.addr;
   return Status();
 }
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
-struct CurrentDevice {
-  int prev = -1;
-  explicit CurrentDevice(int d) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != d) cudaSetDevice(d);
-  }
-  ~CurrentDevice() {
-    if (prev >= 0) cudaSetDevice(prev);
-  }
-};
+size_t noalloc_bytes(const saige_grm* h) {
+  return align256((size_t)h->n_pad * sizeof(float)) + align256((size_t)h->m_pad * sizeof(float)) +
+         (size_t)h->n_splits * h->n_pad * sizeof(float);
+}
 
 Status matvec_noalloc(saige_grm* h, const double* v, double* out, int64_t n, int nrhs,
                       cudaStream_t st) {
@@ -76,8 +99,7 @@ Status matvec_noalloc(saige_grm* h, const double* v, double* out, int64_t n, int
   }
   const size_t v_bytes = align256((size_t)h->n_pad * sizeof(float));
   const size_t u_bytes = align256((size_t)h->m_pad * sizeof(float));
-  const size_t y_bytes = (size_t)h->n_splits * h->n_pad * sizeof(float);
-  const size_t need = v_bytes + u_bytes + y_bytes;
+  const size_t need = noalloc_bytes(h);
   if (need > kNoAllocScratchBytes)
     return fail(SAIGE_EINVAL,
                 "saige_grm_matvec_dev_noalloc: this GRM (n=%lld, m=%lld) needs %zu bytes of "
@@ -120,10 +142,20 @@ extern "C" __attribute__((visibility("default"))) int32_t saige_grm_matvec_dev_n
                                (long long)h->n).code;
     if (nrhs <= 0) return fail(SAIGE_EINVAL, "nrhs must be positive").code;
     std::lock_guard<std::recursive_mutex> lk(h->mu);
-    CurrentDevice dg(h->device);
+    DeviceGuard dg(h->device);
+    if (!dg.ok) return fail(SAIGE_ECUDA, "cannot make device %d current", h->device).code;
     cudaStream_t st = stream ? (cudaStream_t)stream : h->stream;
     return matvec_noalloc(h, v_dev, out_dev, n, nrhs, st).code;
   } catch (...) {
     return fail(SAIGE_EINVAL, "unexpected C++ exception").code;
   }
+}
+
+extern "C" __attribute__((visibility("default"))) int32_t saige_grm_noalloc_scratch_bytes(
+    const saige_grm* h, size_t* need, size_t* limit) {
+  set_error("");
+  if (!h) return fail(SAIGE_EINVAL, "null argument").code;
+  if (need) *need = noalloc_bytes(h);
+  if (limit) *limit = kNoAllocScratchBytes;
+  return SAIGE_OK;
 }

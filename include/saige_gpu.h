@@ -277,15 +277,24 @@ int32_t saige_grm_diag(saige_grm* h, double* out, int64_t n);
  * memory, and latency-critical callers that cannot afford the device
  * synchronisation cudaMalloc/cudaFree may cause.  It allocates nothing: its
  * scratch is a 32 MiB array compiled into the library, which every GPU that
- * loads the library holds until the process exits.  The GRM must fit in it
- * (about 1.5 million samples); larger ones get SAIGE_EINVAL with the sizes in
- * saige_last_error().  The first call on a device looks up the array's device
- * address, so make that call before any stream capture.  v_dev/out_dev hold
+ * loads the library holds until the process exits.  The GRM must fit in it:
+ * it needs 4 n_pad (v) + 4 m_pad (u) + 4 n_splits n_pad (partial sums) bytes,
+ * each part rounded up to 256, with n_pad = n rounded up to 512, m_pad = m rounded
+ * up to 128 and 1 to ~6 splits, fewer as n grows (about 2.7 million samples at
+ * 150,000 markers); saige_grm_noalloc_scratch_bytes gives a handle's figure.
+ * Larger ones get SAIGE_EINVAL with the sizes in saige_last_error().  The first
+ * call on a device (and the first after a device reset) looks up the array's
+ * device address, so make that call before any stream capture.  v_dev/out_dev hold
  * nrhs columns of n doubles; the work is enqueued on `stream` (NULL: the
  * handle's stream) and the call returns without waiting for it.  All calls on
  * one device share the array: calls that overlap on the GPU race. */
 int32_t saige_grm_matvec_dev_noalloc(saige_grm* h, const double* v_dev, double* out_dev,
                                      int64_t n, int32_t nrhs, void* stream);
+
+/* No counterpart in the reference.  The static scratch that
+ * saige_grm_matvec_dev_noalloc would use for this handle (need) and the size of the
+ * array (limit), so that a caller can check ahead of time.  Host only. */
+int32_t saige_grm_noalloc_scratch_bytes(const saige_grm* h, size_t* need, size_t* limit);
 
 /* ---------------------------------------------------------------------
  * PCG solves

@@ -1,7 +1,6 @@
 """Regenerate the golden fixtures under tests/golden/ from the frhl/CSAIGE tree.
 
-Run in a container where the reference tree is mounted (default
-/root/reference, or pass its path).  Writes:
+Usage: python make_golden.py <path of the frhl/CSAIGE tree>.  Writes:
   plink1000_500.bed/.frq  — the first 500 markers of
       extdata/input/plinkforGRM_1000samples_10kMarkers.{bed,frq}
       (1000 samples, no missing calls; PLINK's own MAF column pins the
@@ -9,17 +8,19 @@ Run in a container where the reference tree is mounted (default
   decode_kat.json         — the 2-bit decode known answers of
       saige-geno/src/plink.rs:288-303, transcribed as data.
 """
+import argparse
 import json
-import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF = Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
-BASE = REF / "extdata/input/plinkforGRM_1000samples_10kMarkers"
 N_MARKERS = 500
 
 
 def main() -> None:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("reference", type=Path, help="root of the frhl/CSAIGE source tree")
+    ref = ap.parse_args().reference
+    BASE = ref / "extdata/input/plinkforGRM_1000samples_10kMarkers"
     n_fam = sum(1 for _ in open(BASE.with_suffix(".fam")))
     bpm = (n_fam + 3) // 4
     bed = BASE.with_suffix(".bed").read_bytes()

@@ -6,10 +6,10 @@ that cannot afford the device synchronisation cudaMalloc/cudaFree may cause.
 For them the library exports a variant of the FP32 product whose scratch is a
 fixed array compiled into the library.  These tests call it through the C ABI
 (ctypes, device pointers from torch tensors allocated before the calls) and hold
-it to the existing entry point, saige_grm_matvec_dev, at the FP32 product
-tolerance used throughout the GPU tests (2e-5 relative), on two calls in a row
-with different vectors, so that a call that reused the previous call's scratch
-contents would be caught.  The file is named to be collected last and works
+it to the existing entry point, saige_grm_matvec_dev, and to the FP64 oracle at
+the FP32 product tolerance used throughout the GPU tests (2e-5 relative), on two
+calls in a row with different vectors, so that a call that reused the previous
+call's scratch contents would be caught.  The file is named to be collected last and works
 both on its own in a fresh process and after the rest of the suite.
 """
 import ctypes as C
@@ -35,7 +35,14 @@ def _grm(n, m, seed):
     bed = cs.gen_bed(spec)
     af, _, _ = O.marker_stats(bed, n, m)
     keep = np.nonzero((af >= 0.01) & (af <= 0.99))[0]
-    return cs.OnTheFlyGrm.from_bed(bed, n, m, keep, af[keep])
+    grm = cs.OnTheFlyGrm.from_bed(bed, n, m, keep, af[keep])
+    return grm, bed, keep, af[keep]
+
+
+def _scratch_bytes(grm):
+    need, limit = C.c_size_t(), C.c_size_t()
+    check(LIB.saige_grm_noalloc_scratch_bytes(grm._h, C.byref(need), C.byref(limit)))
+    return need.value, limit.value
 
 
 def _noalloc(grm, v, out, nrhs):
@@ -46,7 +53,7 @@ def _noalloc(grm, v, out, nrhs):
 
 @pytest.mark.parametrize("n,m,seed", [(1001, 300, 7), (20000, 3000, 5)])
 def test_noalloc_matches_matvec_dev_on_two_calls(n, m, seed):
-    grm = _grm(n, m, seed)
+    grm, bed, keep, afs = _grm(n, m, seed)
     g = torch.Generator(device="cpu").manual_seed(seed)
     v1 = torch.randn(2, n, dtype=torch.float64, generator=g).cuda()  # two columns
     v2 = torch.randn(1, n, dtype=torch.float64, generator=g).cuda()
@@ -73,6 +80,14 @@ def test_noalloc_matches_matvec_dev_on_two_calls(n, m, seed):
     assert _rel(r2[0], w2[0]) < 2e-5
     # The second call found its scratch set up and allocated nothing.
     assert free_after_second == free_after_first
+    # ... and both calls equal the FP64 oracle's product to the FP32 tolerance
+    z = O.standardize(O.dosages(bed, n, keep), afs, 0)
+    v1h, v2h = v1.cpu().numpy(), v2.cpu().numpy()
+    for c in range(2):
+        assert _rel(r1[c], O.grm_matvec(z, v1h[c], 0)) < 2e-5
+    assert _rel(r2[0], O.grm_matvec(z, v2h[0], 0)) < 2e-5
+    need, limit = _scratch_bytes(grm)
+    assert 0 < need <= limit == 32 << 20
 
 
 def test_noalloc_rejects_grm_beyond_static_scratch():
@@ -88,6 +103,8 @@ def test_noalloc_rejects_grm_beyond_static_scratch():
     del bed
     v = torch.zeros(1, n, dtype=torch.float64, device="cuda")
     out = torch.zeros_like(v)
+    need, limit = _scratch_bytes(grm)
+    assert need > limit
     rc = _noalloc(grm, v, out, 1)
     assert rc == EINVAL
     msg = LIB.saige_last_error().decode()
