@@ -133,19 +133,34 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
+// Non-blocking test of a phase (mbarrier.try_wait may suspend the thread for a while).
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
 // Bounded wait: returns false (and raises the CTA abort flag and the error
 // word) when the barrier phase does not complete within `budget` cycles or another
-// role already gave up.  A budget of 0 gives up at the first poll that fails.
+// role already gave up.  A budget of 0 gives up unless the phase has already
+// completed (a non-blocking test).
 template <bool kBackoff>
 __device__ __forceinline__ bool mbar_wait_impl(uint32_t bar, uint32_t parity,
                                                volatile int* abort_flag, unsigned int* err,
                                                long long budget) {
-  if (mbar_try_wait(bar, parity)) return true;
   if (budget <= 0) {
+    if (mbar_test_wait(bar, parity)) return true;
     *abort_flag = 1;
     atomicOr(err, 1u);
     return false;
   }
+  if (mbar_try_wait(bar, parity)) return true;
   const long long t0 = clock64();
   uint32_t sleep_ns = 32;
   for (uint32_t polls = 1;; ++polls) {
