@@ -46,10 +46,10 @@ WORKLOAD = dict(n=200_000, m=150_000, prevalence=0.02, n_covar=10, sib_frac=0.10
 # 30 probe products repeated every iteration, ai_reml.rs:175-306), measured with
 # the FP32 path of this library; used to extrapolate the CPU per-product time.
 # Counted from a fit of this library's FP32 path with the reference strategy on the
-# default workload (N=200,000, M=150,000; 2 AI-REML iterations, 172 PCG iterations:
-# 172 + 2*(11+2) + 2*31 = 320, see ref_kv_count); the run without --no-plain
-# recounts it on the spot.
-REF_KV_PER_FIT = 320
+# default workload at the fit-null command's tolerance (N=200,000, M=150,000; 5 AI-REML
+# iterations, 559 PCG iterations: 559 + 5*(11+2) + 5*31 = 929, see ref_kv_count); the
+# run without --no-plain recounts it on the spot.
+REF_KV_PER_FIT = 929
 # Markers in the bounded CPU sample (~1.6 GB of packed rows at N=200,000; about a
 # second per product on 16 cores).
 CPU_SAMPLE_MARKERS = 32768
