@@ -78,6 +78,7 @@ struct TcArgs {
   int sl;                   // load-ring depth in load stages (>= 2)
   int sa;                   // TMEM operand slots, one per sub-stage (a multiple of 2 hb)
   int hb;                   // sub-stages per handoff to the MMA warp (1 or 2)
+  int merged;               // 1: one commit per batch (hb == sub == 2, sa == 4, sl >= 3)
   const uint8_t* tiles;     // this pass's code tiles, tile t at (t*tile_ld + k)*4 KB
   int64_t tile_ld;          // tiles from one output tile's row of tiles to the next (>= nk)
   const uint8_t* img_g;     // nk x ng x 128 bytes
@@ -371,8 +372,13 @@ __device__ __forceinline__ void expand_word(uint32_t w, uint32_t* g, uint32_t* m
 }
 
 // kHb: sub-stages per handoff (a.hb), a template parameter so that the batch loops
-// unroll to straight-line code.
-template <bool kPassB, int kHb>
+// unroll to straight-line code.  kMerged (with kHb == 2 and two sub-stages per load
+// stage): one commit per batch, on the load stage's LDONE barrier, frees both the load
+// slot and the batch's two operand slots.  A tcgen05.commit leaves the tensor pipe idle
+// for ~200 cycles (measured: 8 MMAs of M=128, N=128, K=32 per sub-stage took ~830
+// cycles with 1.5 commits per sub-stage and no handoff at all, 32 MMAs ~2,300), so the
+// merged batches — 16 MMAs per commit instead of 8 per 1.5 — keep it busier.
+template <bool kPassB, int kHb, bool kMerged>
 __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
   extern __shared__ uint8_t smem_raw[];
   const uint32_t raw = smem_u32(smem_raw);
@@ -490,7 +496,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
             mma_i8_ts(tmem_g, ag + 8u * kk, bg + 2u * kk, idesc, acc);
             mma_i8_ts(tmem_m, am + 8u * kk, bm + 2u * kk, idesc, acc);
           }
-          mma_commit(P.ADONE(ab));
+          if (!kMerged) mma_commit(P.ADONE(ab));
           if (t == a.sub - 1 || k == a.nk - 1) mma_commit(P.LDONE(s));
         }
         if (++t == a.sub) {
@@ -537,9 +543,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
           if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err, a.wait_cycles);
           if (live && row == 0) trace_mark(a, k, 1);  // codes landed
           // operand slot ab is free once the MMAs of its previous use (sub-stage k - sa)
+          // completed; merged: both slots of the batch once the MMAs of the batch two
+          // before (this group's previous batch, load stage kb/2 - 2, in the slot two
+          // back; the ring has at least three stages, so that phase is the latest)
           // completed
-          if (live && k >= a.sa)
-            live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err, a.wait_cycles);
+          if (!kMerged) {
+            if (live && k >= a.sa)
+              live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err, a.wait_cycles);
+          } else if (j == 0 && live && kb >= 2 * hb) {
+            const int s2 = s >= 2 ? s - 2 : s - 2 + a.sl;
+            const uint32_t ph2 = s >= 2 ? ph_l : (ph_l ^ 1u);
+            live = mbar_wait_sleep(P.LDONE(s2), ph2, abort_flag, a.err, a.wait_cycles);
+          }
           live = __all_sync(0xffffffffu, live);  // warp-uniform: the barrier calls below must agree
           if (live) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -561,9 +576,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
         step();
       }
       // Every batch is handed over, also after an abort, so that the MMA warp never
-      // waits for an arrival that does not come.  While live, the wait on ADONE of the
-      // slots' previous use keeps this group at most one use ahead of the MMA warp on
-      // its named barrier; after an abort bar.sync does that instead.
+      // waits for an arrival that does not come.  While live, the wait on the slots'
+      // previous use keeps this group at most one use ahead of the MMA warp on its
+      // named barrier; after an abort bar.sync does that instead.
       if (live)
         named_bar_arrive(bar, kHandoffThreads);
       else
@@ -1094,6 +1109,7 @@ size_t tc_fixed_bytes() { return 1024 + 8 * (2 * kMaxSL + kMaxSA + 1) + 16; }
 
 struct Rings {
   int sub, sl, sa, hb;
+  bool merged = false;  // one commit per batch of two sub-stages (kMerged)
 };
 
 // Ring shapes for a launch: load stages of up to four sub-stages (16 KB of
@@ -1104,6 +1120,17 @@ struct Rings {
 Rings tc_rings(int ng, bool pass_b) {
   Rings g;
   const size_t room = kSmemBudget - tc_fixed_bytes();
+  // batches of two sub-stages with one commit each (the load stage = the batch), where
+  // four operand slots and a ring of three such stages fit
+  const int slots = std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols));
+  if (slots >= 4 && room / plan_l_stage(ng, pass_b, 2) >= 3) {
+    g.sub = 2;
+    g.sl = (int)std::min<size_t>(kMaxSL, room / plan_l_stage(ng, pass_b, 2));
+    g.sa = 4;
+    g.hb = 2;
+    g.merged = true;
+    return g;
+  }
   // the most sub-stages per load stage that still leave a ring of four load stages:
   // at the bench size the autotuner's trials put the shapes with a 2-3 stage ring
   // 2-25 % behind (pass B at 43-64 columns most), and no deeper ring of fewer
@@ -1183,8 +1210,9 @@ static Status tc_plan_new(TcPlan** out) {
     delete p;
     return s;
   };
-  for (auto kern : {tc_grm_kernel<false, 1>, tc_grm_kernel<true, 1>, tc_grm_kernel<false, 2>,
-                    tc_grm_kernel<true, 2>}) {
+  for (auto kern : {tc_grm_kernel<false, 1, false>, tc_grm_kernel<true, 1, false>,
+                    tc_grm_kernel<false, 2, false>, tc_grm_kernel<true, 2, false>,
+                    tc_grm_kernel<false, 2, true>, tc_grm_kernel<true, 2, true>}) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSmemBudget);
     if (e != cudaSuccess)
@@ -1281,12 +1309,16 @@ static cudaError_t launch_tc(unsigned grid, const TcArgs& args, cudaStream_t st)
       a.sl < 2 || a.sl > kMaxSL || a.sub < 1 ||
       a.sub > 4)
     return cudaErrorInvalidValue;
+  if (a.merged && !(a.hb == 2 && a.sub == 2 && a.sa == 4 && a.sl >= 3))
+    return cudaErrorInvalidValue;
   const size_t smem = tc_fixed_bytes() + (size_t)a.sl * plan_l_stage(a.ng, kPassB, a.sub);
   if (smem > kSmemBudget) return cudaErrorInvalidValue;
-  if (a.hb == 2)
-    tc_grm_kernel<kPassB, 2><<<grid, kThreads, smem, st>>>(a);
+  if (a.merged)
+    tc_grm_kernel<kPassB, 2, true><<<grid, kThreads, smem, st>>>(a);
+  else if (a.hb == 2)
+    tc_grm_kernel<kPassB, 2, false><<<grid, kThreads, smem, st>>>(a);
   else
-    tc_grm_kernel<kPassB, 1><<<grid, kThreads, smem, st>>>(a);
+    tc_grm_kernel<kPassB, 1, false><<<grid, kThreads, smem, st>>>(a);
   count_launches(1);
   return cudaGetLastError();
 }
@@ -1353,18 +1385,34 @@ std::vector<Rings> tc_candidates(int ng, bool pass_b) {
   const size_t room = kSmemBudget - tc_fixed_bytes();
   const Rings base = tc_rings(ng, pass_b);
   out.push_back(base);  // the fixed choice first
+  const int slots = std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols)) & ~1;
   for (int sub : {4, 2, 1}) {
     const size_t ls = plan_l_stage(ng, pass_b, sub);
     if (2 * ls > room) continue;
-    Rings g = base;
+    Rings g;
     g.sub = sub;
     g.sl = (int)std::min<size_t>(kMaxSL, room / ls);
-    if (!(g.sub == base.sub && g.sl == base.sl)) out.push_back(g);
+    g.sa = slots;
+    g.hb = 1;
+    out.push_back(g);
     if (g.sa >= 4) {  // the same ring with two sub-stages per handoff (four slots)
       g.hb = 2;
       g.sa = 4;
       out.push_back(g);
+      if (sub == 2 && g.sl >= 3) {  // and one commit per batch
+        g.merged = true;
+        out.push_back(g);
+      }
     }
+  }
+  // the fixed choice appears once
+  for (size_t i = 1; i < out.size();) {
+    const Rings& g = out[i];
+    if (g.sub == base.sub && g.sl == base.sl && g.sa == base.sa && g.hb == base.hb &&
+        g.merged == base.merged)
+      out.erase(out.begin() + (std::ptrdiff_t)i);
+    else
+      ++i;
   }
   return out;
 }
@@ -1383,6 +1431,7 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     a.sl = fixed.sl;
     a.sa = fixed.sa;
     a.hb = fixed.hb;
+    a.merged = fixed.merged ? 1 : 0;
     SG_CUDA(launch_tc<kPassB>(grid, a, st));
     return Status();
   }
@@ -1392,6 +1441,7 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     a.sl = g.sl;
     a.sa = g.sa;
     a.hb = g.hb;
+    a.merged = g.merged ? 1 : 0;
   };
   // the state is held under the lock through the (asynchronous) launch, so that one
   // key's candidates and events are used by one launch at a time
@@ -1417,8 +1467,8 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
     ts.ms[(size_t)ts.pending] = ms;
     const Rings& g = ts.cand[(size_t)ts.pending];
     if (log)
-      fprintf(stderr, "[saige tune] pass %c ng %d grid %u nk %d: sub %d sl %d hb %d -> %.3f ms\n",
-              kPassB ? 'B' : 'A', a.ng, grid, a.nk, g.sub, g.sl, g.hb, ms);
+      fprintf(stderr, "[saige tune] pass %c ng %d grid %u nk %d: sub %d sl %d hb %d merged %d -> %.3f ms\n",
+              kPassB ? 'B' : 'A', a.ng, grid, a.nk, g.sub, g.sl, g.hb, g.merged ? 1 : 0, ms);
     ts.pending = -1;
   }
   while (ts.next < ts.cand.size()) {

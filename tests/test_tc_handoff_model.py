@@ -118,3 +118,59 @@ def test_producer_drain_covers_every_copy_in_flight(sub, sl):
             assert len({slot for _, slot, _ in drain}) == len(drain) <= sl
             for J, slot, par in drain:
                 assert slot == J % sl and par == (J // sl) & 1
+
+
+def merged_unpack_waits(nk, sl, grp):
+    """The unpack loop of the merged mode (two sub-stages per batch and per load stage):
+    at the start of each of the group's batches, the LDONE slot and parity it waits on
+    for its operand slots (computed as the kernel does, from the current ring position)."""
+    st = dict(t=0, s=0, ph_l=0)
+
+    def step():
+        st["t"] += 1
+        if st["t"] == 2:
+            st["t"] = 0
+            st["s"] += 1
+            if st["s"] == sl:
+                st["s"], st["ph_l"] = 0, st["ph_l"] ^ 1
+
+    for _ in range(grp * 2):
+        step()
+    out, kb = [], grp * 2
+    while kb < nk:
+        assert st["t"] == 0
+        if kb >= 4:
+            s, ph = st["s"], st["ph_l"]
+            out.append((kb // 2, s - 2 if s >= 2 else s - 2 + sl, ph if s >= 2 else ph ^ 1))
+        for _ in range(4):  # this batch and the other group's
+            step()
+        kb += 4
+    return out
+
+
+def merged_mma_commits(nk, sl):
+    """The MMA warp's commits in the merged mode: (load stage, LDONE slot) in order."""
+    t = s = 0
+    out = []
+    for k in range(nk):
+        if t == 1 or k == nk - 1:
+            out.append((k // 2, s))
+        t += 1
+        if t == 2:
+            t, s = 0, (s + 1) % sl
+    return out
+
+
+@pytest.mark.parametrize("sl", [3, 4, 5, 24])
+def test_merged_batches_wait_on_the_commit_of_their_previous_batch(sl):
+    for nk in list(range(1, 40)) + [1164, 1565]:
+        commits = merged_mma_commits(nk, sl)
+        # one commit per batch (load stage), on LDONE(stage % sl)
+        assert commits == [(b, b % sl) for b in range((nk + 1) // 2)]
+        for grp in (0, 1):
+            for b, slot, par in merged_unpack_waits(nk, sl, grp):
+                # the group's previous batch b - 2, whose commit is phase (b-2)//sl of its slot
+                assert slot == (b - 2) % sl and par == ((b - 2) // sl) & 1
+                # that phase is still the barrier's latest when the wait runs: the next use
+                # of the slot is load stage b - 2 + sl > b, whose MMAs follow batch b's
+                assert b - 2 + sl > b
