@@ -244,8 +244,8 @@ SIGNATURES = {
     "saige_mlp_eval": (C.c_int32, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64,
                                    P(C.c_float), P(C.c_float), _d, C.c_int32]),
     "saige_mlp_train": (C.c_int32, [P(C.c_float), P(C.c_float), P(C.c_float), C.c_int64,
-                                    C.c_int32, C.c_int32, C.c_int32, C.c_float, C.c_int32, _d, _d,
-                                    _d, C.c_int32]),
+                                    C.c_int32, C.c_int32, C.c_float, C.c_int32, _d, _d, _d,
+                                    C.c_int32]),
     "saige_explicit_grm_config_default": (C.c_int32, [P(ExplicitGrmConfigC)]),
     "saige_dense_grm_from_bed": (
         C.c_int32,

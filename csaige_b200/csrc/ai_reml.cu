@@ -208,6 +208,10 @@ struct Recycle {
 
 // Held-out R^2 at or above which the prediction joins the basis.
 constexpr double kLearnR2Min = 0.25;
+// Adam steps of the first and of every later training round, and the learning rate.
+constexpr int kLearnSteps0 = 100;
+constexpr int kLearnSteps = 50;
+constexpr float kLearnRate = 1e-3f;
 // PCG iterations of the block solve whose y and X search directions are kept
 constexpr int kKeepIters = 3;
 // At most this many kept directions (each costs two n-vectors of workspace plus a
@@ -439,15 +443,15 @@ Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k) {
   const auto t0 = std::chrono::steady_clock::now();
   const int64_t ld = f.ld, n = f.n;
   const int q = f.q;
-  std::vector<double> sc((size_t)(2 * q + 2)), dd;
+  std::vector<double> sc((size_t)(2 * q + 8)), dd;
   if (rc.have_F) {
     SG_CUDA(sub_cols(f.sol, rc.xprev, rc.x0, n, ld, q, f.st));
     SG_TRY(coldots(f, rc.x0, rc.x0, q, dd));
     for (int c = 0; c < q; ++c) sc[(size_t)c] = sqrt(dd[(size_t)c] / (double)n);
     SG_CUDA(cudaMemcpyAsync(rc.scales, sc.data(), (size_t)q * 8, cudaMemcpyHostToDevice, f.st));
     SG_CUDA(learn_targets(f.sol, rc.xprev, rc.scales, n, ld, q, rc.T, f.st));
-    SG_TRY(mlp_train(rc.mlp, rc.F0, rc.T, n, q, rc.trainings == 0 ? 100 : 50, 32768, 3e-3f, 8,
-                     f.st));
+    SG_TRY(mlp_train(rc.mlp, rc.F0, rc.T, n, q, rc.trainings == 0 ? kLearnSteps0 : kLearnSteps,
+                     kLearnRate, 8, f.st));
     double mse = 0.0, tms = 0.0;
     SG_TRY(mlp_validate(rc.mlp, rc.F0, rc.T, n, q, 8, &mse, &tms, f.st));
     rc.r2 = tms > 0.0 ? 1.0 - mse / tms : 0.0;
@@ -459,19 +463,20 @@ Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k) {
   std::vector<double> a, b, u, w;
   SG_TRY(coldots(f, f.sol, f.sol, q, a));
   SG_TRY(coldots(f, f.rhs, f.rhs, q, b));
-  SG_TRY(coldots(f, f.ku, f.ku, 2, u));
+  const int n_sk = std::min(f.nrv, 8);  // sketches: the GRM applied to the first probes
+  SG_TRY(coldots(f, f.ku, f.ku, n_sk, u));
   SG_TRY(coldots(f, f.w, f.w, 1, w));
   for (int c = 0; c < q; ++c) {
     sc[(size_t)c] = sqrt(a[(size_t)c] / (double)n);
     sc[(size_t)(q + c)] = sqrt(b[(size_t)c] / (double)n);
   }
-  sc[(size_t)(2 * q)] = sqrt(u[0] / (double)n);
-  sc[(size_t)(2 * q + 1)] = sqrt(u[1] / (double)n);
+  for (int s2 = 0; s2 < 8; ++s2)
+    sc[(size_t)(2 * q + s2)] = s2 < n_sk ? sqrt(u[(size_t)s2] / (double)n) : 0.0;
   const double wr = sqrt(w[0] / (double)n);
   const double dmean = 1.0 / (tau[0] / (wr > 1e-30 ? wr : 1e-30) + tau[1]);
   SG_CUDA(cudaMemcpyAsync(rc.scales, sc.data(), sc.size() * 8, cudaMemcpyHostToDevice, f.st));
-  SG_CUDA(learn_features(f.sol, f.rhs, rc.bnext, f.w, rc.wnext, rc.diagk, f.ku, f.ku + ld,
-                         rc.scales, tau[0], tau[1], dmean, n, ld, q, rc.F1, f.st));
+  SG_CUDA(learn_features(f.sol, f.rhs, rc.bnext, f.w, rc.wnext, rc.diagk, f.ku, n_sk, rc.scales,
+                         tau[0], tau[1], dmean, n, ld, q, rc.F1, f.st));
   rc.have_delta = false;
   if (rc.trainings > 0 && rc.r2 >= kLearnR2Min) {
     SG_TRY(mlp_forward(rc.mlp, rc.F1, n * q, rc.yhat, f.st));

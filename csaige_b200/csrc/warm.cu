@@ -111,8 +111,7 @@ __global__ void learn_features_kernel(const double* __restrict__ x, const double
                                       const double* __restrict__ w,
                                       const double* __restrict__ wnext,
                                       const double* __restrict__ diagk,
-                                      const double* __restrict__ ku0,
-                                      const double* __restrict__ ku1,
+                                      const double* __restrict__ ku, int n_sk,
                                       const double* __restrict__ scales, double tau0, double tau1,
                                       double dmean, int64_t n, int64_t ld, int q,
                                       float* __restrict__ F) {
@@ -120,20 +119,26 @@ __global__ void learn_features_kernel(const double* __restrict__ x, const double
   const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int64_t e = (int64_t)c * n + i, a = (int64_t)c * ld + i;
-  const double sx = scales[c], sb = scales[q + c], sk0 = scales[2 * q], sk1 = scales[2 * q + 1];
+  const double sx = scales[c], sb = scales[q + c];
   const double wi = w[i] > 1e-30 ? w[i] : 1e-30, wn = wnext[i] > 1e-30 ? wnext[i] : 1e-30;
   const double d = 1.0 / (tau0 / wi + tau1);
-  float4 f0, f1;
-  f0.x = (float)(sx > 0.0 ? x[a] / sx : 0.0);
-  f0.y = (float)(sb > 0.0 ? b[a] / sb : 0.0);
-  f0.z = (float)(sb > 0.0 ? (bnext[a] - b[a]) / sb : 0.0);
-  f0.w = (float)log(wn / wi);
-  f1.x = (float)(d / dmean - 1.0);
-  f1.y = (float)(diagk[i] - 1.0);
-  f1.z = (float)(sk0 > 0.0 ? ku0[i] / sk0 : 0.0);
-  f1.w = (float)(sk1 > 0.0 ? ku1[i] / sk1 : 0.0);
-  reinterpret_cast<float4*>(F + e * 8)[0] = f0;
-  reinterpret_cast<float4*>(F + e * 8)[1] = f1;
+  float f[16];
+  f[0] = (float)(sx > 0.0 ? x[a] / sx : 0.0);
+  f[1] = (float)(sb > 0.0 ? b[a] / sb : 0.0);
+  f[2] = (float)(sb > 0.0 ? (bnext[a] - b[a]) / sb : 0.0);
+  f[3] = (float)log(wn / wi);
+  f[4] = (float)(d / dmean - 1.0);
+  f[5] = (float)(diagk[i] - 1.0);
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const double sk = scales[2 * q + s];
+    f[6 + s] = (float)(s < n_sk && sk > 0.0 ? ku[(int64_t)s * ld + i] / sk : 0.0);
+  }
+  f[14] = (float)tau1;
+  f[15] = 0.f;
+  float4* dst = reinterpret_cast<float4*>(F + e * 16);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) dst[k] = make_float4(f[4 * k], f[4 * k + 1], f[4 * k + 2], f[4 * k + 3]);
 }
 
 __global__ void learn_targets_kernel(const double* __restrict__ x1, const double* __restrict__ x0,
@@ -224,11 +229,11 @@ cudaError_t sub_cols(const double* a, const double* b, double* out, int64_t n, i
 }
 
 cudaError_t learn_features(const double* x, const double* b, const double* bnext, const double* w,
-                           const double* wnext, const double* diagk, const double* ku0,
-                           const double* ku1, const double* scales, double tau0, double tau1,
-                           double dmean, int64_t n, int64_t ld, int q, float* F, cudaStream_t st) {
+                           const double* wnext, const double* diagk, const double* ku, int n_sk,
+                           const double* scales, double tau0, double tau1, double dmean,
+                           int64_t n, int64_t ld, int q, float* F, cudaStream_t st) {
   learn_features_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)q), 256, 0, st>>>(
-      x, b, bnext, w, wnext, diagk, ku0, ku1, scales, tau0, tau1, dmean, n, ld, q, F);
+      x, b, bnext, w, wnext, diagk, ku, n_sk, scales, tau0, tau1, dmean, n, ld, q, F);
   count_launches(1);
   return cudaGetLastError();
 }

@@ -31,14 +31,16 @@ cudaError_t sub_cols(const double* a, const double* b, double* out, int64_t n, i
                      cudaStream_t st);
 
 // Learned start: features of example e = c * n + i (sample i, column c) for the
-// prediction of the next solution change, 8 floats each:
+// prediction of the next solution change, 16 floats each:
 //   x[i,c] / sx[c], b[i,c] / sb[c], (bnext[i,c] - b[i,c]) / sb[c], log(wnext[i] / w[i]),
-//   d[i] / dmean - 1, diagk[i] - 1, ku0[i] / sk0, ku1[i] / sk1
-// (x, b, bnext: ld apart; d the Jacobi scale 1 / (tau0 / w + tau1)).
+//   d[i] / dmean - 1, diagk[i] - 1, the sketches ku[i, s] / sk[s] for s < n_sk (the GRM
+//   applied to the first n_sk <= 8 probes; zero past n_sk), tau1, 0
+// (x, b, bnext, ku: ld apart; d the Jacobi scale 1 / (tau0 / w + tau1); scales =
+// [sx (q), sb (q), sk (8)]).
 cudaError_t learn_features(const double* x, const double* b, const double* bnext, const double* w,
-                           const double* wnext, const double* diagk, const double* ku0,
-                           const double* ku1, const double* scales, double tau0, double tau1,
-                           double dmean, int64_t n, int64_t ld, int q, float* F, cudaStream_t st);
+                           const double* wnext, const double* diagk, const double* ku, int n_sk,
+                           const double* scales, double tau0, double tau1, double dmean,
+                           int64_t n, int64_t ld, int q, float* F, cudaStream_t st);
 // T[c*n + i] = (x1[i,c] - x0[i,c]) / s[c]
 cudaError_t learn_targets(const double* x1, const double* x0, const double* s, int64_t n,
                           int64_t ld, int q, float* T, cudaStream_t st);

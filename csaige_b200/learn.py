@@ -1,7 +1,8 @@
 """The MLP of the learned PCG start (SAIGE_WARM_LEARNED), exposed for checking:
-8 inputs, three tanh layers of 64 units, one linear output; BF16 weights in the
-forward pass, FP32 master weights and arithmetic.  Parameter layout
-W1[64][8], b1[64], W2[64][64], b2[64], W3[64][64], b3[64], w4[64], b4."""
+16 inputs, three tanh layers of 256 units, one linear output; BF16 weights and
+activations in the forward pass (the 256 x 256 layers on the tensor cores), FP32
+master weights and arithmetic.  Parameter layout W1[256][16], b1[256], W2[256][256],
+b2[256], W3[256][256], b3[256], w4[256], b4."""
 from __future__ import annotations
 
 import ctypes as C
@@ -11,7 +12,7 @@ import numpy as np
 
 from ._lib import LIB, check
 
-N_IN, N_HIDDEN = 8, 64
+N_IN, N_HIDDEN = 16, 256
 
 
 def _fp(a: np.ndarray):
@@ -43,13 +44,13 @@ def mlp_eval(params, features, targets=None, want_grad: bool = False, device: in
     return out, grad, (sse.value if t is not None else None)
 
 
-def mlp_train(params, features, targets, n: int, q: int, steps: int = 200, batch: int = 32768,
-              lr: float = 3e-3, holdout: int = 8, device: int = -1):
+def mlp_train(params, features, targets, n: int, q: int, steps: int = 200, lr: float = 1e-3,
+              holdout: int = 8, device: int = -1):
     """Trains a copy of params; returns (params, held-out MSE before, after, mean square target)."""
     p = np.ascontiguousarray(params, np.float32).copy()
     f = np.ascontiguousarray(features, np.float32).reshape(-1, N_IN)
     t = np.ascontiguousarray(targets, np.float32).reshape(-1)
     b, a, m = C.c_double(), C.c_double(), C.c_double()
-    check(LIB.saige_mlp_train(_fp(p), _fp(f), _fp(t), n, q, steps, batch, lr, holdout,
+    check(LIB.saige_mlp_train(_fp(p), _fp(f), _fp(t), n, q, steps, lr, holdout,
                               C.byref(b), C.byref(a), C.byref(m), device))
     return p, b.value, a.value, m.value

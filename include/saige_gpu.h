@@ -573,26 +573,27 @@ int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_t n_fam
 
 /* ---------------------------------------------------------------------
  * The MLP of the learned PCG start (SAIGE_WARM_LEARNED; no reference
- * counterpart).  8 inputs, three tanh layers of 64, a linear output; BF16
- * weights in the forward pass, FP32 arithmetic and FP32 master weights.
- * Parameter layout: W1[64][8], b1[64], W2[64][64], b2[64], W3[64][64], b3[64],
- * w4[64], b4.  These entry points expose the network's own kernels so that
- * they can be checked against a CPU reference.
+ * counterpart).  16 inputs, three tanh layers of 256, a linear output; BF16
+ * weights and activations in the forward pass (the two 256 x 256 layers on the
+ * tensor cores), FP32 arithmetic and FP32 master weights.
+ * Parameter layout: W1[256][16], b1[256], W2[256][256], b2[256], W3[256][256],
+ * b3[256], w4[256], b4.  These entry points expose the network's own kernels so
+ * that they can be checked against a CPU reference.
  * ------------------------------------------------------------------- */
 int32_t saige_mlp_param_count(void);
 /* The initial weights the fit uses for a seed (uniform +-1/sqrt(fan_in)). */
 int32_t saige_mlp_initial_params(uint64_t seed, float* params);
-/* n_ex examples of 8 features (row-major): out[e] = MLP(features[e]) (may be NULL);
+/* n_ex examples of 16 features (row-major): out[e] = MLP(features[e]) (may be NULL);
  * grad (may be NULL) = gradient of mean_e (out[e] - targets[e])^2 with respect to
- * params (through the BF16 rounding); sse (may be NULL) = sum_e (out[e] - targets[e])^2. */
+ * params (through the BF16 roundings); sse (may be NULL) = sum_e (out[e] - targets[e])^2. */
 int32_t saige_mlp_eval(const float* params, const float* features, const float* targets,
                        int64_t n_ex, float* out, float* grad, double* sse, int32_t device);
 /* Trains params in place with the fit's trainer: steps Adam steps (lr) on
- * mini-batches of batch examples from e = c * n + i (q columns of n samples),
+ * mini-batches of 8192 examples from e = c * n + i (q columns of n samples),
  * samples i % holdout == 0 held out; held-out mean squared error before and after
  * and the held-out mean squared target. */
 int32_t saige_mlp_train(float* params, const float* features, const float* targets, int64_t n,
-                        int32_t q, int32_t steps, int32_t batch, float lr, int32_t holdout,
+                        int32_t q, int32_t steps, float lr, int32_t holdout,
                         double* val_mse_before, double* val_mse_after, double* val_target_ms,
                         int32_t device);
 

@@ -68,6 +68,12 @@ def test_learned_start_same_fit_and_reports_its_gain(capsys):
     assert lrn.iterations == zero.iterations >= 4
     assert np.allclose(lrn.tau, zero.tau, rtol=1e-4, atol=0)
     assert np.allclose(lrn.alpha, zero.alpha, rtol=1e-4, atol=1e-6)
+    # against the method without the network (the recycled start): the same fit within
+    # the PCG tolerance, and no more than one extra product launch per AI-REML iteration
+    # (the learned start keeps the K U launch that its sketch features need)
+    assert rec.iterations == lrn.iterations
+    assert np.allclose(lrn.tau, rec.tau, rtol=1e-4, atol=0)
+    assert lrn.n_kv_launches <= rec.n_kv_launches + lrn.iterations
     assert lrn.learned_trainings == lrn.iterations - 1
     assert 0.0 < lrn.learned_r2 <= 1.0
     with capsys.disabled():
