@@ -64,6 +64,9 @@ FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # M = 5,000, binary at ~10 % prevalence, 2 covariates, 10 % sibling pairs, 1 % missing.
 # The precision-form cohort of the accuracy block (errors against FP64 products).
 ACCURACY = dict(n=50_000, m=100_000)
+# The learned-start cohort: N = 400,000, M = 100,000 (10 GB packed), binary at 1 %,
+# 10 covariates, twelve AI-REML iterations.
+STARTS = dict(n=400_000, m=100_000, seed=4242, iterations=12)
 # tau tolerance of the fit-null command (saige-cli/src/commands/fit_null.rs:74-80)
 CLI_TOL = 1e-5
 CONFIG1 = dict(seed=12345, n=2000, m=5000, sib_frac=0.10, missing_rate=0.01, prevalence=0.10,
@@ -93,7 +96,7 @@ def parse_args():
     ap.add_argument("--no-cohorts", action="store_true",
                     help="skip the 16 sub-cohort fits")
     ap.add_argument("--no-learned", action="store_true",
-                    help="skip the learned-versus-recycled start comparison")
+                    help="skip the zero / recycled / learned start comparison (N=400k, M=100k)")
     ap.add_argument("--no-config1", action="store_true",
                     help="skip the plain CPU-scale cohort (GPU fits, oracle, measured CPU fit)")
     ap.add_argument("--no-accuracy", action="store_true",
@@ -441,6 +444,62 @@ def accuracy_block(cs) -> dict:
     return out
 
 
+def starts_block(cs) -> dict:
+    """The learned-start cohort (N = 400,000, M = 100,000, binary at 1 %, 10
+    covariates): twelve AI-REML iterations of the fast configuration (MIXED, block PCG
+    to 1e-5, the reference's diagonal preconditioner) from the zero, the recycled and
+    the learned start; products launched, PCG iterations and seconds of each."""
+    import torch
+
+    n, m = STARTS["n"], STARTS["m"]
+    spec = cs.CohortSpec(n=n, m=m, seed=STARTS["seed"], sib_frac=WORKLOAD["sib_frac"],
+                         cousin_frac=WORKLOAD["cousin_frac"], missing_rate=WORKLOAD["missing_rate"],
+                         trait=cs.TraitType.Binary, n_covar=10, prevalence=0.01, h2=0.2,
+                         n_causal=1000)
+    bed_dev = torch.empty(spec.bed_len, dtype=torch.uint8, device="cuda")
+    cs.gen_bed_dev(spec, bed_dev.data_ptr())
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = cs.api.bed_marker_stats_dev(bed_dev.data_ptr(), spec.bed_len, n, m)
+    g, _ = cs.select_grm_markers(af, mac, nv, n)
+    grm = cs.OnTheFlyGrm.from_bed_dev(bed_dev.data_ptr(), spec.bed_len, n, m, g, af[g],
+                                      precision=cs.PREC_MIXED)
+    del bed_dev
+    torch.cuda.empty_cache()
+    out = {"workload": f"fit-null binary 1% prev (cases {int(y.sum())}), N={n}, M={m} bed "
+                       f"markers ({len(g)} in the GRM), 10 covariates, 30 probes, PCG tol 1e-5, "
+                       f"{STARTS['iterations']} AI-REML iterations (tau tolerance 0)",
+           "config": "MIXED tensor-core products, block PCG over y, X and the probes, "
+                     "diagonal (tau0/W + tau1) preconditioner"}
+    for name, wmode in (("zero", cs.WARM_ZERO), ("recycled", cs.WARM_RECYCLED),
+                        ("learned", cs.WARM_LEARNED)):
+        cfg = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK, warm_start=wmode,
+                              tol=0.0, max_iter=STARTS["iterations"])
+        t0 = time.perf_counter()
+        r = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg)
+        wall = time.perf_counter() - t0
+        out[name] = {"seconds": r.seconds, "wall_s": wall, "ai_reml_iterations": int(r.iterations),
+                     "n_kv_launches": int(r.n_kv_launches), "n_kv": int(r.n_kv),
+                     "pcg_iters": int(r.pcg_iters), "tau": [float(r.tau[0]), float(r.tau[1])]}
+        if wmode == cs.WARM_LEARNED:
+            out[name].update({"trainings": int(r.learned_trainings),
+                              "prediction_used": int(r.learned_uses),
+                              "held_out_r2": float(r.learned_r2),
+                              "mlp_seconds": float(r.learned_seconds)})
+    for name in ("recycled", "learned"):
+        out[f"{name}_vs_zero"] = {
+            "launches_saved": out["zero"]["n_kv_launches"] - out[name]["n_kv_launches"],
+            "pcg_iters_saved": out["zero"]["pcg_iters"] - out[name]["pcg_iters"],
+            "speedup": out["zero"]["seconds"] / out[name]["seconds"]}
+    out["learned_vs_recycled"] = {
+        "launches_saved": out["recycled"]["n_kv_launches"] - out["learned"]["n_kv_launches"],
+        "pcg_iters_saved": out["recycled"]["pcg_iters"] - out["learned"]["pcg_iters"],
+        "speedup": out["recycled"]["seconds"] / out["learned"]["seconds"],
+        "tau_rel_diff": abs(out["learned"]["tau"][1] - out["recycled"]["tau"][1]) /
+                        abs(out["recycled"]["tau"][1])}
+    grm.close()
+    return out
+
+
 def run_reference(args, rank):
     """The reference's strategy on the host cores: each step times one product of the
     oracle over a bounded marker sample and extrapolates it to a whole fit at the
@@ -684,26 +743,6 @@ def run_ours(args, world, rank, local):
             "speedup": seq_wall / con_wall, "fits_per_s": len(cohorts) / con_wall,
             "same_tau": all(np.array_equal(a.tau, b.tau) for a, b in zip(seq, con)),
             "config": "fit_null::run per cohort (counts, QC, GRM, AI-REML), .bed uploaded once"}
-    # the learned start against the recycled one on the same cohort, to an AI-REML
-    # tolerance tight enough for several iterations (the default 0.02 stops after the
-    # first iteration with tau1 > 0, before the network has a transition to learn from)
-    if not args.no_learned and world == 1:
-        cmp_ = {}
-        for name, wmode in (("recycled", cs.WARM_RECYCLED), ("learned", cs.WARM_LEARNED)):
-            cfg_l = cs.AiRemlConfig(precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
-                                    warm_start=wmode, tol=CLI_TOL)
-            r = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg_l)
-            cmp_[name] = {"seconds": r.seconds, "ai_reml_iterations": int(r.iterations),
-                          "n_kv_launches": int(r.n_kv_launches), "pcg_iters": int(r.pcg_iters),
-                          "tau": [float(r.tau[0]), float(r.tau[1])]}
-            if wmode == cs.WARM_LEARNED:
-                cmp_[name].update({"trainings": int(r.learned_trainings),
-                                   "prediction_used": int(r.learned_uses),
-                                   "held_out_r2": float(r.learned_r2),
-                                   "mlp_seconds": float(r.learned_seconds)})
-        cmp_["launches_saved"] = cmp_["recycled"]["n_kv_launches"] - cmp_["learned"]["n_kv_launches"]
-        cmp_["config"] = "same cohort, AiRemlConfig tol 1e-5, MIXED, block PCG"
-        line["learned_vs_recycled"] = cmp_
     # the reference's strategy on the same GPU
     plain_kv = None
     if not args.no_plain and world == 1:
@@ -754,6 +793,8 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_accuracy:
         del grm
         line["accuracy"] = accuracy_block(cs)
+    if rank == 0 and world == 1 and not args.no_learned:
+        line["config5_starts"] = starts_block(cs)
     if rank == 0 and world == 1 and not args.no_explicit_grm:
         line["explicit_grm"] = explicit_grm_block(cs, local, args.grm_n, args.grm_m,
                                                   args.grm_reps)
