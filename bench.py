@@ -55,9 +55,9 @@ REF_KV_PER_FIT = 929
 CPU_SAMPLE_MARKERS = 32768
 # DRAM bytes read per marker row by one tensor-core launch (packed genotype tile rows
 # plus the vector-limb tiles), from the ncu capture at N=200,000, m_pad=18,048:
-# pass A 932.4 MB, pass B 935.2 MB.  Reads scale with m_pad; the output writes
+# pass A 929.2 MB, pass B 939.4 MB.  Reads scale with m_pad; the output writes
 # (pass A: m_pad*R*8 bytes, pass B: N*R*8 bytes) are added per launch.
-TC_READ_PER_MARKER_ROW = {"A": 932.4e6 / 18048, "B": 935.2e6 / 18048}
+TC_READ_PER_MARKER_ROW = {"A": 929.2e6 / 18048, "B": 939.4e6 / 18048}
 
 FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
 # The plain CPU-scale fit-null cohort (the reference's own benchmark size): N = 2,000,

@@ -6,11 +6,11 @@
 
 #include <cstdlib>
 #include <chrono>
-#include <cstdlib>
 #include <thread>
 #include <vector>
 
 #include "engine.cuh"
+#include "kernels_tc.cuh"
 #include "kernels.cuh"
 #include "rng.hpp"
 #include "vr.cuh"
@@ -377,6 +377,8 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
   // in the first product of this solve, for this iteration's AI starts
   Extra ex;
   if (!rc.learned && tau[1] != 0.0) {
+    // (measured: leaving them out to keep this product at kTcFastCols columns cost the
+    // AI solve one more product than the slower launch shape costs)
     const bool need_pk = f.have_prev_pk && !rc.have_kpk;
     const bool need_pw = rc.with_pw && f.have_prev_pw && !rc.have_kpw;
     if (need_pk && need_pw) ex = Extra{f.pk_raw, rc.kpk, 2};  // adjacent columns
@@ -395,26 +397,36 @@ Status block_solve_recycled(Fit& f, Recycle& rc, const double* x0_prev, const do
   return s;
 }
 
-// K Py, and in the same launch K X*_t (this iteration's block solutions, for the next
-// block start) and K of the previous AI solutions pk', pw' (for this iteration's AI
-// starts).  Writes f.kpy.
+// K Py = K (Sinv y - Sinv X alpha) = kblock[:, 0] - kblock[:, 1..p] alpha from the
+// K-images of this iteration's block solutions (alpha uploaded again: the device
+// scratch also takes dot results).
+Status kpy_combine(Fit& f, Recycle& rc, const std::vector<double>& alpha) {
+  SG_CUDA(cudaMemcpyAsync(f.dsmall, alpha.data(), (size_t)f.p * 8, cudaMemcpyHostToDevice, f.st));
+  SG_TRY(copy_cols(f, rc.kblock, f.kpy, 1));
+  SG_CUDA(sub_combo(f.kpy, 1, rc.kblock + f.ld, f.p, f.dsmall, f.n, f.ld, f.st));
+  return Status();
+}
+
+// K X*_t (this iteration's block solutions, for the next block start) and K of the
+// previous AI solutions pk', pw' (for this iteration's AI starts) in one launch; K Py
+// then follows from K X*_t, so that the launch holds q columns (+ the AI solutions),
+// not 1 + q.  Writes f.kpy.
 Status learn_step(Fit& f, Recycle& rc, int trait, const double tau[2], int& k);
 
 Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw, int trait,
-                    const double tau[2]) {
+                    const double tau[2], const std::vector<double>& alpha) {
   const int64_t ld = f.ld;
-  SG_TRY(copy_cols(f, f.py, rc.kin, 1));
-  SG_TRY(copy_cols(f, f.sol, rc.kin + ld, f.q));
-  int k = 1 + f.q;
+  SG_TRY(copy_cols(f, f.sol, rc.kin, f.q));
+  int k = f.q;
   const int at_pk = k;
   if (with_pk) SG_TRY(copy_cols(f, f.pk_raw, rc.kin + (size_t)k++ * ld, 1));
   const int at_pw = k;
   if (with_pw) SG_TRY(copy_cols(f, f.pw_raw, rc.kin + (size_t)k++ * ld, 1));
   if (rc.learned) SG_TRY(learn_step(f, rc, trait, tau, k));
   SG_TRY(grm_product(f.h, rc.kin, rc.kout, k, nullptr, f.cfg->precision, f.st));
-  SG_TRY(copy_cols(f, rc.kout, f.kpy, 1));
-  SG_TRY(copy_cols(f, rc.kout + ld, rc.kblock, f.q));
+  SG_TRY(copy_cols(f, rc.kout, rc.kblock, f.q));
   rc.have_kblock = true;
+  SG_TRY(kpy_combine(f, rc, alpha));
   if (with_pk) SG_TRY(copy_cols(f, rc.kout + (size_t)at_pk * ld, rc.kpk, 1));
   if (with_pw) SG_TRY(copy_cols(f, rc.kout + (size_t)at_pw * ld, rc.kpw, 1));
   rc.have_kpk = with_pk;
@@ -422,12 +434,9 @@ Status kpy_recycled(Fit& f, Recycle& rc, bool with_pk, bool with_pw, int trait,
   return Status();
 }
 
-// K Py without a product: the block solve kept K X*_t beside X*_t, so
-// K Py = K (Sinv y - Sinv X alpha) = kblock[:, 0] - kblock[:, 1..p] alpha (alpha on the
-// device in f.dsmall, as for Py).
-Status kpy_from_block(Fit& f, Recycle& rc) {
-  SG_TRY(copy_cols(f, rc.kblock, f.kpy, 1));
-  SG_CUDA(sub_combo(f.kpy, 1, rc.kblock + f.ld, f.p, f.dsmall, f.n, f.ld, f.st));
+// K Py without a product: the block solve kept K X*_t beside X*_t.
+Status kpy_from_block(Fit& f, Recycle& rc, const std::vector<double>& alpha) {
+  SG_TRY(kpy_combine(f, rc, alpha));
   ++rc.kpy_launches_saved;
   return Status();
 }
@@ -752,9 +761,10 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     SG_TRY(copy_cols(f, SinvY, f.py, 1));
     SG_CUDA(sub_combo(f.py, 1, SinvX, p, f.dsmall, n, ld, f.st));
     if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK && block_kx && !rc.learned) {
-      SG_TRY(kpy_from_block(f, rc));  // K X*_t and K Py without a launch
+      SG_TRY(kpy_from_block(f, rc, alpha));  // K X*_t and K Py without a launch
     } else if (recyc && cfg->solve == SAIGE_SOLVE_BLOCK) {
-      SG_TRY(kpy_recycled(f, rc, f.have_prev_pk, !fix_tau_e && f.have_prev_pw, trait, tau));
+      SG_TRY(kpy_recycled(f, rc, f.have_prev_pk, !fix_tau_e && f.have_prev_pw, trait, tau,
+                          alpha));
     } else
       SG_TRY(grm_product(h, f.py, f.kpy, 1, nullptr, cfg->precision, f.st));
     tm.mark("  kpy");

@@ -581,27 +581,39 @@ static int32_t marker_stats_impl(const uint8_t* bed, bool on_device, size_t bed_
   if (!bed || !af || !mac || !n_valid || m_tot < 0) return fail(SAIGE_EINVAL, "null argument").code;
   uint8_t hdr[3] = {0, 0, 0};
   Status s;
+  cudaStream_t st = nullptr;
+  // a host .bed is checked before any device call (errors need no GPU)
   if (!on_device) {
     if (bed_len >= 3) memcpy(hdr, bed, 3);
   } else {
     s = pick_device(-1, nullptr);
     if (!s.ok()) return s.code;
-    if (bed_len >= 3 && cudaMemcpy(hdr, bed, 3, cudaMemcpyDeviceToHost) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+      return fail(SAIGE_ECUDA, "stream creation failed").code;
+    // on this call's own stream: a legacy-stream copy would wait for other work
+    if (bed_len >= 3 && (cudaMemcpyAsync(hdr, bed, 3, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                         cudaStreamSynchronize(st) != cudaSuccess)) {
+      cudaStreamDestroy(st);
       return fail(SAIGE_ECUDA, "reading the bed header from device memory failed").code;
+    }
   }
   s = check_bed_header(hdr, bed_len, n_fam, m_tot);
-  if (!s.ok()) return s.code;
   std::vector<int32_t> sidx;
-  bool identity;
-  s = check_subset(sample_idx, n, n_fam, sidx, identity);
-  if (!s.ok()) return s.code;
-  s = pick_device(-1, nullptr);
-  if (!s.ok()) return s.code;
+  bool identity = true;
+  if (s.ok()) s = check_subset(sample_idx, n, n_fam, sidx, identity);
+  if (s.ok() && !st) {
+    s = pick_device(-1, nullptr);
+    if (s.ok() && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
+      s = fail(SAIGE_ECUDA, "stream creation failed");
+  }
+  if (!s.ok()) {
+    if (st) cudaStreamDestroy(st);
+    return s.code;
+  }
   const int64_t bpm = (n_fam + 3) / 4;
   const size_t used = (size_t)(3 + bpm * m_tot);
-  cudaStream_t st;
-  if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess)
-    return fail(SAIGE_ECUDA, "stream creation failed").code;
+  // every buffer below is used on st only: its release waits for st, not the device
+  ReleaseScope rs(ReleaseMode::kStream, st);
   DevBuf d_bed, d_cnt;
   auto body = [&]() -> Status {
     SG_TRY(d_cnt.reserve((size_t)std::max<int64_t>(m_tot, 1) * 2 * sizeof(int64_t)));
@@ -784,8 +796,16 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
   Status s = pick_device(device, &dev);
   if (!s.ok()) return s.code;
   if (on_device) {
-    if (bed_len >= 3 && cudaMemcpy(hdr.data(), bed, 3, cudaMemcpyDeviceToHost) != cudaSuccess)
-      return fail(SAIGE_ECUDA, "reading the bed header from device memory failed").code;
+    if (bed_len >= 3) {
+      // on a stream of this call: a legacy-stream copy would wait for other work
+      cudaStream_t hs;
+      if (cudaStreamCreateWithFlags(&hs, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(SAIGE_ECUDA, "stream creation failed").code;
+      const bool ok = cudaMemcpyAsync(hdr.data(), bed, 3, cudaMemcpyDeviceToHost, hs) == cudaSuccess &&
+                      cudaStreamSynchronize(hs) == cudaSuccess;
+      cudaStreamDestroy(hs);
+      if (!ok) return fail(SAIGE_ECUDA, "reading the bed header from device memory failed").code;
+    }
   } else if (bed_len >= 3) {
     memcpy(hdr.data(), bed, 3);
   }
@@ -805,6 +825,8 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
   h->device = dev;
   PhaseTimer tm;
   auto body = [&]() -> Status {
+    // the gather's temporaries are used on the handle's stream only
+    ReleaseScope rs(ReleaseMode::kStream, h->stream);
     SG_TRY(grm_alloc(h, n, m));
     tm.mark(" grm alloc");
     SG_TRY(grm_upload_meta(h, allele_freqs));

@@ -54,16 +54,35 @@ __global__ void __launch_bounds__(kThreads)
                       const int64_t* __restrict__ src_rows, const int32_t* __restrict__ sidx,
                       int64_t n, uint32_t* __restrict__ out, int64_t wpr,
                       int64_t* __restrict__ counts, int use_smem) {
-  extern __shared__ uint8_t row_s[];
+  extern __shared__ __align__(16) uint8_t row_s[];
   __shared__ long long red[2][kThreads / 32];
   const int64_t r = blockIdx.x;
   const uint8_t* row = bed + 3 + src_rows[r] * bpm;
   const uint8_t* src = row;
   if (use_smem) {
-    for (int64_t b = threadIdx.x; b < bpm; b += blockDim.x) row_s[b] = row[b];
+    // Stage the raw row in 16-byte chunks of its aligned span (row byte b at
+    // row_s[off + b]); the chunks that reach past either end of the row, at most two,
+    // are copied byte by byte, so no load leaves the row.  Several independent chunk
+    // loads per thread are in flight at once.
+    const int off = (int)(reinterpret_cast<uintptr_t>(row) & 15u);
+    const uint4* base = reinterpret_cast<const uint4*>(row - off);
+    const int64_t n16 = (off + bpm + 15) / 16;
+#pragma unroll 4
+    for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) {
+      const int64_t lo = 16 * i - off;
+      if (lo >= 0 && lo + 16 <= bpm) {
+        reinterpret_cast<uint4*>(row_s)[i] = __ldg(base + i);
+      } else {
+        for (int k = 0; k < 16; ++k) {
+          const int64_t b = lo + k;
+          if (b >= 0 && b < bpm) row_s[16 * i + k] = row[b];
+        }
+      }
+    }
     __syncthreads();
-    src = row_s;
+    src = row_s + off;
   }
+  const bool sidx16 = (reinterpret_cast<uintptr_t>(sidx) & 15u) == 0;
   long long alt = 0, miss = 0;
   const int64_t n_words_real = (n + 15) / 16;
   const int64_t n_words = out ? wpr : n_words_real;
@@ -82,6 +101,19 @@ __global__ void __launch_bounds__(kThreads)
           const int64_t bi = 4 * j + b;
           const uint32_t byte = bi < bpm ? (uint32_t)src[bi] : 0u;
           word |= byte << (8 * b);
+        }
+      } else if (kn == 16 && sidx16) {
+        // the word's 16 sample indices as four 16-byte loads
+        const int4* s4 = reinterpret_cast<const int4*>(sidx + k0);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int4 v = __ldg(s4 + g);
+          const int32_t ss[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const uint32_t code = (src[ss[e] >> 2] >> ((ss[e] & 3) * 2)) & 3u;
+            word |= code << (2 * (4 * g + e));
+          }
         }
       } else {
         for (int k = 0; k < kn; ++k) {
@@ -125,7 +157,7 @@ cudaError_t launch_bed_gather(const uint8_t* bed, int64_t bpm, const int64_t* sr
                               cudaStream_t st) {
   if (n_rows <= 0) return cudaSuccess;
   const int use_smem = bpm <= kSmemRowMax ? 1 : 0;
-  const size_t smem = use_smem ? (size_t)round_up(bpm, 16) : 0;
+  const size_t smem = use_smem ? (size_t)round_up(bpm + 16, 16) : 0;
   if (sample_idx) {
     auto k = bed_gather_kernel<false>;
     if (smem > 48 * 1024) {

@@ -4,6 +4,12 @@
 
 namespace saige {
 
+// Columns of one tensor-core launch that keep its fastest ring shape: with 3 r limb
+// columns rounded up to 16 at most 128, the two accumulators leave the TMEM room for
+// four operand slots and pass B's load stages of two sub-stages fit three deep (43
+// columns take 144 MMA columns: two slots and a slower shape).
+constexpr int kTcFastCols = 42;
+
 // Kv for q columns (ld = h->n_pad) through the int8-limb tensor-core kernels.
 Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,
                   cudaStream_t st);
