@@ -1010,7 +1010,11 @@ SG_API int32_t saige_fit_loco(saige_grm* h, const int32_t* marker_chrom, int32_t
           ex[(size_t)j] = marker_chrom[j] == k ? 1 : 0;
           active += ex[(size_t)j] ? 0 : 1;
         }
-        if (cudaMemcpy(h->excl.ptr, ex.data(), ex.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+        // ordered on the handle's stream (which a legacy-stream copy would not be), and
+        // complete before ex is rewritten for the next chromosome
+        if (cudaMemcpyAsync(h->excl.ptr, ex.data(), ex.size(), cudaMemcpyHostToDevice,
+                            h->stream) != cudaSuccess ||
+            cudaStreamSynchronize(h->stream) != cudaSuccess) {
           s = fail(SAIGE_ECUDA, "mask upload failed");
           break;
         }

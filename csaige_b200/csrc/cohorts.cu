@@ -1,10 +1,16 @@
 // Fit-null of several sub-cohorts of one .bed (different sample subsets, the same
 // markers), as fit_null::run would do for each (saige-cli/src/commands/fit_null.rs:
 // 199-287: counts, QC and the VR/GRM split over the cohort's samples, the GRM, the
-// AI-REML fit).  The .bed is uploaded once.  Run concurrently, each cohort's fit owns
-// a handle with its own stream on its own host thread, so that the launches of small
-// cohorts — whose sample-side pass fills a fraction of the GPU and whose PCG steps
-// are latency-bound — overlap with those of the others.
+// AI-REML fit).  The .bed is uploaded once.
+//
+// Sequential: each cohort in turn, every step its own (as fit_null::run per cohort).
+// Concurrent: the .bed streams in by marker chunks, and one launch per chunk counts
+// every cohort's alleles and missing calls of the chunk's markers (each raw row staged
+// once for all cohorts), all under the PCIe-bound transfer; then each cohort's marker
+// selection, GRM and fit run on its own host thread and stream, so that the launches of
+// small cohorts — whose sample-side pass fills a fraction of the GPU and whose PCG
+// steps are latency-bound — overlap with those of the others.  The counts are exact
+// integers either way, so both orders give the same fits.
 #include <stdint.h>
 #include <string.h>
 
@@ -14,6 +20,7 @@
 
 #include "common.cuh"
 #include "engine.cuh"
+#include "kernels.cuh"
 
 using namespace saige;
 
@@ -28,6 +35,10 @@ struct CohortJob {
   const double* x;
   saige_ai_reml_summary* out;
   double* alpha;
+  // marker statistics over the cohort's samples, when counted beforehand
+  bool have_stats = false;
+  std::vector<double> af, mac;
+  std::vector<int64_t> nv;
   int64_t m_grm = 0;
   int32_t rc = SAIGE_OK;
   std::string err;
@@ -37,19 +48,24 @@ void run_cohort(int device, const uint8_t* d_bed, size_t bed_len, int64_t n_fam,
                 int32_t p, int32_t trait, double min_maf, double max_missing,
                 const saige_ai_reml_config* cfg, CohortJob& job) {
   cudaSetDevice(device);
-  std::vector<double> af((size_t)m_tot), mac((size_t)m_tot);
-  std::vector<int64_t> nv((size_t)m_tot);
-  int32_t rc = saige_bed_marker_stats_dev(d_bed, bed_len, n_fam, m_tot, job.sidx, job.n,
-                                          af.data(), mac.data(), nv.data());
+  int32_t rc = SAIGE_OK;
+  if (!job.have_stats) {
+    job.af.resize((size_t)m_tot);
+    job.mac.resize((size_t)m_tot);
+    job.nv.resize((size_t)m_tot);
+    rc = saige_bed_marker_stats_dev(d_bed, bed_len, n_fam, m_tot, job.sidx, job.n, job.af.data(),
+                                    job.mac.data(), job.nv.data());
+  }
   std::vector<int64_t> gidx((size_t)m_tot), vidx((size_t)m_tot);
   int64_t m_grm = 0, m_vr = 0;
   if (rc == SAIGE_OK)
-    rc = saige_select_grm_markers(af.data(), mac.data(), nv.data(), m_tot, job.n, min_maf,
-                                  max_missing, cfg->seed, gidx.data(), &m_grm, vidx.data(), &m_vr);
+    rc = saige_select_grm_markers(job.af.data(), job.mac.data(), job.nv.data(), m_tot, job.n,
+                                  min_maf, max_missing, cfg->seed, gidx.data(), &m_grm,
+                                  vidx.data(), &m_vr);
   saige_grm* h = nullptr;
   if (rc == SAIGE_OK) {
     std::vector<double> gaf((size_t)m_grm);
-    for (int64_t j = 0; j < m_grm; ++j) gaf[(size_t)j] = af[(size_t)gidx[(size_t)j]];
+    for (int64_t j = 0; j < m_grm; ++j) gaf[(size_t)j] = job.af[(size_t)gidx[(size_t)j]];
     rc = saige_grm_create_from_bed_dev(d_bed, bed_len, n_fam, m_tot, job.sidx, job.n, gidx.data(),
                                        m_grm, gaf.data(), device, &h);
   }
@@ -60,6 +76,98 @@ void run_cohort(int device, const uint8_t* d_bed, size_t bed_len, int64_t n_fam,
   if (h) saige_grm_destroy(h);
   job.m_grm = m_grm;
   job.rc = rc;
+}
+
+// Uploads the .bed into d_bed in marker chunks on a copy stream while, chunk by chunk,
+// one launch counts every cohort's alleles and missing calls of the chunk's markers;
+// fills each job's marker statistics.  Rows too long to stage in shared memory return
+// with have_stats false (each cohort then counts on its own).
+Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
+                        DevBuf& d_bed, std::vector<CohortJob>& jobs) {
+  const int64_t bpm = (n_fam + 3) / 4;
+  const int k = (int)jobs.size();
+  // every cohort's sample list, each padded to a multiple of 16 entries
+  std::vector<int32_t> all;
+  std::vector<int64_t> offs((size_t)k), ns((size_t)k);
+  for (int c = 0; c < k; ++c) {
+    std::vector<int32_t> s;
+    bool identity = true;
+    SG_TRY(check_subset(jobs[(size_t)c].sidx, jobs[(size_t)c].n, n_fam, s, identity));
+    offs[(size_t)c] = (int64_t)all.size();
+    ns[(size_t)c] = jobs[(size_t)c].n;
+    if (jobs[(size_t)c].sidx) {
+      all.insert(all.end(), s.begin(), s.end());
+    } else {
+      for (int64_t i = 0; i < n_fam; ++i) all.push_back((int32_t)i);
+    }
+    all.resize((size_t)round_up((int64_t)all.size(), 16), 0);
+  }
+  cudaStream_t cp = nullptr, kst = nullptr;
+  std::vector<cudaEvent_t> ev;
+  DevBuf d_sidx, d_offs, d_ns, d_cnt;
+  std::vector<long long> cnt;
+  auto body = [&]() -> Status {
+    SG_CUDA(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking));
+    SG_CUDA(cudaStreamCreateWithFlags(&kst, cudaStreamNonBlocking));
+    SG_TRY(d_sidx.reserve(all.size() * 4));
+    SG_TRY(d_offs.reserve((size_t)k * 8));
+    SG_TRY(d_ns.reserve((size_t)k * 8));
+    SG_TRY(d_cnt.reserve((size_t)k * m_tot * 16));
+    SG_CUDA(cudaMemcpyAsync(d_sidx.ptr, all.data(), all.size() * 4, cudaMemcpyHostToDevice, kst));
+    SG_CUDA(cudaMemcpyAsync(d_offs.ptr, offs.data(), (size_t)k * 8, cudaMemcpyHostToDevice, kst));
+    SG_CUDA(cudaMemcpyAsync(d_ns.ptr, ns.data(), (size_t)k * 8, cudaMemcpyHostToDevice, kst));
+    // every chunk's copy is queued first; the counts follow chunk by chunk
+    constexpr int kChunks = 32;
+    const int64_t per = std::max<int64_t>(1, ceil_div(m_tot, (int64_t)kChunks));
+    uint8_t* dst = d_bed.as<uint8_t>();
+    std::vector<std::pair<int64_t, int64_t>> spans;
+    for (int64_t j0 = 0; j0 < m_tot; j0 += per) {
+      const int64_t j1 = std::min(m_tot, j0 + per);
+      const size_t lo = j0 == 0 ? 0 : (size_t)(3 + j0 * bpm);
+      const size_t hi = j1 == m_tot ? bed_len : (size_t)(3 + j1 * bpm);
+      SG_CUDA(cudaMemcpyAsync(dst + lo, bed + lo, hi - lo, cudaMemcpyHostToDevice, cp));
+      cudaEvent_t e = nullptr;
+      SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev.push_back(e);
+      SG_CUDA(cudaEventRecord(e, cp));
+      spans.emplace_back(j0, j1);
+    }
+    for (size_t i = 0; i < spans.size(); ++i) {
+      SG_CUDA(cudaStreamWaitEvent(kst, ev[i], 0));
+      SG_CUDA(launch_bed_count_cohorts(dst, bpm, spans[i].first, spans[i].second - spans[i].first,
+                                       d_sidx.as<int32_t>(), d_offs.as<int64_t>(),
+                                       d_ns.as<int64_t>(), k, m_tot, d_cnt.as<long long>(), kst));
+    }
+    cnt.resize((size_t)k * m_tot * 2);
+    SG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost, kst));
+    SG_CUDA(cudaStreamSynchronize(kst));
+    SG_CUDA(cudaStreamSynchronize(cp));
+    return Status();
+  };
+  Status s = body();
+  if (cp) cudaStreamSynchronize(cp);
+  if (kst) cudaStreamSynchronize(kst);
+  {
+    ReleaseScope idle(ReleaseMode::kIdle, nullptr);  // both streams have drained
+    d_sidx.release();
+    d_offs.release();
+    d_ns.release();
+    d_cnt.release();
+  }
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  if (cp) cudaStreamDestroy(cp);
+  if (kst) cudaStreamDestroy(kst);
+  SG_TRY(s);
+  for (int c = 0; c < k; ++c) {
+    CohortJob& j = jobs[(size_t)c];
+    j.af.resize((size_t)m_tot);
+    j.mac.resize((size_t)m_tot);
+    j.nv.resize((size_t)m_tot);
+    stats_from_counts(cnt.data() + (size_t)c * m_tot * 2, m_tot, j.n, j.af.data(), j.mac.data(),
+                      j.nv.data());
+    j.have_stats = true;
+  }
+  return Status();
 }
 
 }  // namespace
@@ -79,17 +187,14 @@ SG_API int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_
     for (int32_t c = 0; c < n_cohorts; ++c)
       if (!sample_idx[c] || n[c] <= 0 || !y[c] || !x[c])
         return fail(SAIGE_EINVAL, "cohort %d: null argument or empty", c).code;
+    Status hs = check_bed_header(bed, bed_len, n_fam, m_tot);
+    if (!hs.ok()) return hs.code;
     saige_ai_reml_config cf;
     if (cfg) cf = *cfg;
     else saige_ai_reml_config_default(&cf);
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return fail(SAIGE_ECUDA, "no CUDA device").code;
     const auto t0 = std::chrono::steady_clock::now();
-    DevBuf d_bed;
-    Status s = d_bed.reserve(bed_len);
-    if (!s.ok()) return s.code;
-    if (cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice) != cudaSuccess)
-      return fail(SAIGE_ECUDA, "bed upload failed: %s", cudaGetErrorString(cudaGetLastError())).code;
     std::vector<CohortJob> jobs((size_t)n_cohorts);
     for (int32_t c = 0; c < n_cohorts; ++c) {
       CohortJob& j = jobs[(size_t)c];
@@ -99,6 +204,16 @@ SG_API int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_
       j.x = x[c];
       j.out = out + c;
       j.alpha = alpha ? alpha[c] : nullptr;
+    }
+    DevBuf d_bed;
+    Status s = d_bed.reserve(bed_len);
+    if (!s.ok()) return s.code;
+    const int64_t bpm = (n_fam + 3) / 4;
+    if (concurrent && bpm <= 200 * 1024) {
+      s = upload_and_count(bed, bed_len, n_fam, m_tot, d_bed, jobs);
+      if (!s.ok()) return s.code;
+    } else if (cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice) != cudaSuccess) {
+      return fail(SAIGE_ECUDA, "bed upload failed: %s", cudaGetErrorString(cudaGetLastError())).code;
     }
     const uint8_t* db = d_bed.as<uint8_t>();
     if (concurrent) {

@@ -252,9 +252,15 @@ static Status grm_upload_meta(saige_grm* h, const double* af) {
   std::vector<float4> zl;
   std::vector<double> tp, is;
   marker_meta(af, h->m, h->m_pad, zl, tp, is);
-  SG_CUDA(cudaMemcpy(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice));
-  SG_CUDA(cudaMemcpy(h->two_p, tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice));
-  SG_CUDA(cudaMemcpy(h->inv_s, is.data(), is.size() * sizeof(double), cudaMemcpyHostToDevice));
+  // on the handle's stream: a legacy-stream copy from pageable memory may still be in
+  // flight when it returns, and the handle's (non-blocking) stream would not wait for it
+  SG_CUDA(cudaMemcpyAsync(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                          h->stream));
+  SG_CUDA(cudaMemcpyAsync(h->two_p, tp.data(), tp.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          h->stream));
+  SG_CUDA(cudaMemcpyAsync(h->inv_s, is.data(), is.size() * sizeof(double), cudaMemcpyHostToDevice,
+                          h->stream));
+  SG_CUDA(cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
   return Status();
 }
 
@@ -325,6 +331,19 @@ Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam,
   }
   if (n != n_fam) identity = false;
   return Status();
+}
+
+void stats_from_counts(const long long* cnt, int64_t m, int64_t n, double* af, double* mac,
+                       int64_t* n_valid) {
+  for (int64_t j = 0; j < m; ++j) {
+    const int64_t alt = cnt[2 * j], miss = cnt[2 * j + 1];
+    const int64_t nv = n - miss;
+    const double sum = (double)alt;
+    af[j] = nv > 0 ? sum / (2.0 * (double)nv) : 0.0;
+    const double other = 2.0 * (double)nv - sum;
+    mac[j] = sum < other ? sum : other;
+    n_valid[j] = nv;
+  }
 }
 
 // Gather rows of a device-resident .bed into the handle (or count only).
@@ -633,16 +652,7 @@ static int32_t marker_stats_impl(const uint8_t* bed, bool on_device, size_t bed_
       SG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost, st));
       SG_CUDA(cudaStreamSynchronize(st));
     }
-    for (int64_t j = 0; j < m_tot; ++j) {
-      const int64_t alt = cnt[(size_t)(2 * j)], miss = cnt[(size_t)(2 * j + 1)];
-      const int64_t nv = n - miss;
-      // traits.rs:42-54, the same f64 operations on the same exact integers
-      const double sum = (double)alt;
-      af[j] = nv > 0 ? sum / (2.0 * (double)nv) : 0.0;
-      const double other = 2.0 * (double)nv - sum;
-      mac[j] = sum < other ? sum : other;
-      n_valid[j] = nv;
-    }
+    stats_from_counts(reinterpret_cast<const long long*>(cnt.data()), m_tot, n, af, mac, n_valid);
     return Status();
   };
   s = body();
@@ -825,9 +835,9 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
   h->device = dev;
   PhaseTimer tm;
   auto body = [&]() -> Status {
+    SG_TRY(grm_alloc(h, n, m));  // creates the handle's stream
     // the gather's temporaries are used on the handle's stream only
     ReleaseScope rs(ReleaseMode::kStream, h->stream);
-    SG_TRY(grm_alloc(h, n, m));
     tm.mark(" grm alloc");
     SG_TRY(grm_upload_meta(h, allele_freqs));
     tm.mark(" grm meta");

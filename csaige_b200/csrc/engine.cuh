@@ -76,6 +76,11 @@ struct TcPlan;  // tensor-core path state (kernels_tc.cu)
 Status pick_device(int32_t want, int* dev);
 // PLINK .bed magic, SNP-major mode and size (plink.rs:80-98).
 Status check_bed_header(const uint8_t* hdr, size_t bed_len, int64_t n_fam, int64_t m_tot);
+// MarkerData::compute_af (saige-geno/src/traits.rs:42-54) from exact counts of n
+// samples: cnt[2j] alt-allele count, cnt[2j + 1] missing calls of marker j; the same
+// f64 operations on the same integers as the reference's dosage sums.
+void stats_from_counts(const long long* cnt, int64_t m, int64_t n, double* af, double* mac,
+                       int64_t* n_valid);
 // Validates a sample subset (NULL = all n_fam samples in order).
 Status check_subset(const int64_t* sidx, int64_t n, int64_t n_fam, std::vector<int32_t>& out,
                     bool& identity);

@@ -335,7 +335,8 @@ Status run_syrk(SyrkArgs a, int64_t n, int64_t n_pad, bool packed, int32_t arith
       a.count = d_cnt.as<unsigned long long>();
       a.cap = cap;
       SG_TRY(timed_launch(true));
-      SG_CUDA(cudaMemcpy(&cnt, d_cnt.ptr, sizeof(cnt), cudaMemcpyDeviceToHost));
+      SG_CUDA(cudaMemcpyAsync(&cnt, d_cnt.ptr, sizeof(cnt), cudaMemcpyDeviceToHost, st));
+      SG_CUDA(cudaStreamSynchronize(st));
       if ((int64_t)cnt <= cap) break;
       // more entries passed the cutoff than the first guess holds: size exactly and redo
       cap = (int64_t)cnt;
@@ -424,7 +425,8 @@ Status grm_from_bed(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m
     SG_TRY(d_cnt.reserve((size_t)m_tot * 2 * sizeof(int64_t)));
     SG_TRY(bed_gather_dev(d_bed.as<uint8_t>(), n_fam, all, sidx, identity, n, nullptr, 0,
                           d_cnt.as<int64_t>(), st));
-    SG_CUDA(cudaMemcpy(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost));
+    SG_CUDA(cudaMemcpyAsync(cnt.data(), d_cnt.ptr, cnt.size() * 8, cudaMemcpyDeviceToHost, st));
+    SG_CUDA(cudaStreamSynchronize(st));
     d_cnt.release();
   }
   // dense.rs:34-58: the af window, the variance floor, and the z of each code

@@ -16,6 +16,15 @@ cudaError_t launch_bed_gather(const uint8_t* bed, int64_t bytes_per_marker, cons
                               uint32_t* geno_out, int64_t words_per_row, int64_t* counts,
                               cudaStream_t st);
 
+// Alt-allele and missing counts of rows j0 .. j0 + n_rows of the raw .bed for several
+// sample subsets at once: subset c is sidx[offs[c] .. offs[c] + ns[c]) (offs[c] a
+// multiple of 16); counts[(c m_tot + j) 2 + {0, 1}].  Rows of more than 200 KB are
+// refused (cudaErrorInvalidValue).
+cudaError_t launch_bed_count_cohorts(const uint8_t* bed, int64_t bytes_per_marker, int64_t j0,
+                                     int64_t n_rows, const int32_t* sidx, const int64_t* offs,
+                                     const int64_t* ns, int n_cohorts, int64_t m_tot,
+                                     long long* counts, cudaStream_t st);
+
 // ---- synthetic cohort ------------------------------------------------------
 struct CohortDev;
 cudaError_t launch_gen_bed(const void* layout, uint8_t* bed, int64_t bytes_per_marker,

@@ -48,6 +48,60 @@ __device__ __forceinline__ long long warp_sum_ll(long long v) {
   return v;
 }
 
+// Stages raw row `row` (bpm bytes) in shared memory in 16-byte chunks of its aligned
+// span (row byte b at row_s[off + b]); the chunks that reach past either end of the
+// row, at most two, are copied byte by byte, so no load leaves the row.  Several
+// independent chunk loads per thread are in flight at once.  Returns row_s + off.
+// row_s holds round_up(bpm + 16, 16) bytes, 16-byte aligned.
+__device__ __forceinline__ const uint8_t* stage_row(const uint8_t* row, int64_t bpm,
+                                                    uint8_t* row_s) {
+  const int off = (int)(reinterpret_cast<uintptr_t>(row) & 15u);
+  const uint4* base = reinterpret_cast<const uint4*>(row - off);
+  const int64_t n16 = (off + bpm + 15) / 16;
+#pragma unroll 4
+  for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) {
+    const int64_t lo = 16 * i - off;
+    if (lo >= 0 && lo + 16 <= bpm) {
+      reinterpret_cast<uint4*>(row_s)[i] = __ldg(base + i);
+    } else {
+      for (int k = 0; k < 16; ++k) {
+        const int64_t b = lo + k;
+        if (b >= 0 && b < bpm) row_s[16 * i + k] = row[b];
+      }
+    }
+  }
+  __syncthreads();
+  return row_s + off;
+}
+
+// The codes of samples sidx[0 .. kn) (kn <= 16) of a raw row as one PLINK-order
+// word (sample k at bits 2k); vec: sidx is 16-byte aligned and kn == 16, so the
+// indices are read as four 16-byte loads.
+__device__ __forceinline__ uint32_t gather_word(const uint8_t* src, const int32_t* sidx, int kn,
+                                                bool vec) {
+  uint32_t word = 0;
+  if (vec) {
+    const int4* s4 = reinterpret_cast<const int4*>(sidx);
+#pragma unroll
+    for (int g = 0; g < 4; ++g) {
+      const int4 v = __ldg(s4 + g);
+      const int32_t ss[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const uint32_t code = (src[ss[e] >> 2] >> ((ss[e] & 3) * 2)) & 3u;
+        word |= code << (2 * (4 * g + e));
+      }
+    }
+  } else {
+    for (int k = 0; k < kn; ++k) {
+      const int32_t s = sidx[k];
+      const uint32_t code = (src[s >> 2] >> ((s & 3) * 2)) & 3u;
+      word |= code << (2 * k);
+    }
+  }
+  return word;
+}
+
 template <bool kIdentity>
 __global__ void __launch_bounds__(kThreads)
     bed_gather_kernel(const uint8_t* __restrict__ bed, int64_t bpm,
@@ -58,30 +112,7 @@ __global__ void __launch_bounds__(kThreads)
   __shared__ long long red[2][kThreads / 32];
   const int64_t r = blockIdx.x;
   const uint8_t* row = bed + 3 + src_rows[r] * bpm;
-  const uint8_t* src = row;
-  if (use_smem) {
-    // Stage the raw row in 16-byte chunks of its aligned span (row byte b at
-    // row_s[off + b]); the chunks that reach past either end of the row, at most two,
-    // are copied byte by byte, so no load leaves the row.  Several independent chunk
-    // loads per thread are in flight at once.
-    const int off = (int)(reinterpret_cast<uintptr_t>(row) & 15u);
-    const uint4* base = reinterpret_cast<const uint4*>(row - off);
-    const int64_t n16 = (off + bpm + 15) / 16;
-#pragma unroll 4
-    for (int64_t i = threadIdx.x; i < n16; i += blockDim.x) {
-      const int64_t lo = 16 * i - off;
-      if (lo >= 0 && lo + 16 <= bpm) {
-        reinterpret_cast<uint4*>(row_s)[i] = __ldg(base + i);
-      } else {
-        for (int k = 0; k < 16; ++k) {
-          const int64_t b = lo + k;
-          if (b >= 0 && b < bpm) row_s[16 * i + k] = row[b];
-        }
-      }
-    }
-    __syncthreads();
-    src = row_s + off;
-  }
+  const uint8_t* src = use_smem ? stage_row(row, bpm, row_s) : row;
   const bool sidx16 = (reinterpret_cast<uintptr_t>(sidx) & 15u) == 0;
   long long alt = 0, miss = 0;
   const int64_t n_words_real = (n + 15) / 16;
@@ -102,25 +133,8 @@ __global__ void __launch_bounds__(kThreads)
           const uint32_t byte = bi < bpm ? (uint32_t)src[bi] : 0u;
           word |= byte << (8 * b);
         }
-      } else if (kn == 16 && sidx16) {
-        // the word's 16 sample indices as four 16-byte loads
-        const int4* s4 = reinterpret_cast<const int4*>(sidx + k0);
-#pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          const int4 v = __ldg(s4 + g);
-          const int32_t ss[4] = {v.x, v.y, v.z, v.w};
-#pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            const uint32_t code = (src[ss[e] >> 2] >> ((ss[e] & 3) * 2)) & 3u;
-            word |= code << (2 * (4 * g + e));
-          }
-        }
       } else {
-        for (int k = 0; k < kn; ++k) {
-          const int32_t s = sidx[k0 + k];
-          const uint32_t code = (src[s >> 2] >> ((s & 3) * 2)) & 3u;
-          word |= code << (2 * k);
-        }
+        word = gather_word(src, sidx + k0, kn, kn == 16 && sidx16);
       }
       const uint32_t keep = kn >= 16 ? 0xFFFFFFFFu : ((1u << (2 * kn)) - 1u);
       count_word(word, keep & 0x55555555u, alt, miss);
@@ -149,7 +163,72 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// Counts of several sample subsets ("cohorts") of the same raw rows in one pass:
+// block = marker j0 + blockIdx.x, staged once in shared memory; for cohort c, the
+// samples sidx[offs[c] .. offs[c] + n_c) (offs[c] a multiple of 16) are gathered 16 at
+// a time and counted as bed_gather_kernel counts them.  counts[(c m_tot + j) 2 + e]:
+// e = 0 alt-allele count, 1 missing count.
+__global__ void __launch_bounds__(kThreads)
+    bed_count_cohorts_kernel(const uint8_t* __restrict__ bed, int64_t bpm, int64_t j0,
+                             const int32_t* __restrict__ sidx, const int64_t* __restrict__ offs,
+                             const int64_t* __restrict__ ns, int n_cohorts, int64_t m_tot,
+                             long long* __restrict__ counts) {
+  extern __shared__ __align__(16) uint8_t row_s[];
+  __shared__ long long red[2][kThreads / 32];
+  const int64_t j = j0 + blockIdx.x;
+  const uint8_t* src = stage_row(bed + 3 + j * bpm, bpm, row_s);
+  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int c = 0; c < n_cohorts; ++c) {
+    const int32_t* sc = sidx + offs[c];
+    const int64_t n = ns[c];
+    const bool vec = (reinterpret_cast<uintptr_t>(sc) & 15u) == 0;
+    long long alt = 0, miss = 0;
+    for (int64_t w = threadIdx.x; w < (n + 15) / 16; w += blockDim.x) {
+      const int64_t k0 = 16 * w;
+      const int kn = (n - k0) < 16 ? (int)(n - k0) : 16;
+      const uint32_t word = gather_word(src, sc + k0, kn, vec && kn == 16);
+      const uint32_t keep = kn >= 16 ? 0xFFFFFFFFu : ((1u << (2 * kn)) - 1u);
+      count_word(word, keep & 0x55555555u, alt, miss);
+    }
+    alt = warp_sum_ll(alt);
+    miss = warp_sum_ll(miss);
+    if (lane == 0) {
+      red[0][wid] = alt;
+      red[1][wid] = miss;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      long long a = 0, mm = 0;
+      for (int k = 0; k < kThreads / 32; ++k) {
+        a += red[0][k];
+        mm += red[1][k];
+      }
+      counts[2 * ((int64_t)c * m_tot + j)] = a;
+      counts[2 * ((int64_t)c * m_tot + j) + 1] = mm;
+    }
+    __syncthreads();  // red is reused by the next cohort
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_bed_count_cohorts(const uint8_t* bed, int64_t bpm, int64_t j0, int64_t n_rows,
+                                     const int32_t* sidx, const int64_t* offs, const int64_t* ns,
+                                     int n_cohorts, int64_t m_tot, long long* counts,
+                                     cudaStream_t st) {
+  if (n_rows <= 0) return cudaSuccess;
+  if (bpm > kSmemRowMax) return cudaErrorInvalidValue;  // rows must fit in shared memory
+  const size_t smem = (size_t)round_up(bpm + 16, 16);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(bed_count_cohorts_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  bed_count_cohorts_kernel<<<(unsigned)n_rows, kThreads, smem, st>>>(bed, bpm, j0, sidx, offs, ns,
+                                                                    n_cohorts, m_tot, counts);
+  count_launches(1);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_bed_gather(const uint8_t* bed, int64_t bpm, const int64_t* src_rows,
                               int64_t n_rows, const int32_t* sample_idx, int64_t n,

@@ -303,6 +303,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
     // Ring positions advance incrementally: no division in the loop.
     const uint32_t idesc = i8_idesc(a.ng);
     int t = 0, s = 0, ab = 0;  // sub-stage within the load stage, load slot, operand slot
+    // (lane 0) the last load stage and sub-stage whose LDONE / ADONE was committed
+    int j_done = -1, k_done = -1;
     // One named-barrier handoff per batch of hb sub-stages (slots ab .. ab + hb - 1,
     // barrier 1 + ab / hb): the warp waits once, then lane 0 issues the whole batch.
     for (int k = 0; k < a.nk;) {
@@ -337,8 +339,14 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
             mma_i8_ts(tmem_g, ag + 8u * kk, bg + 2u * kk, idesc, acc);
             mma_i8_ts(tmem_m, am + 8u * kk, bm + 2u * kk, idesc, acc);
           }
-          if (!kMerged) mma_commit(P.ADONE(ab));
-          if (t == a.sub - 1 || k == a.nk - 1) mma_commit(P.LDONE(s));
+          if (!kMerged) {
+            mma_commit(P.ADONE(ab));
+            k_done = k;
+          }
+          if (t == a.sub - 1 || k == a.nk - 1) {
+            mma_commit(P.LDONE(s));
+            j_done = k / a.sub;
+          }
         }
         if (++t == a.sub) {
           t = 0;
@@ -349,7 +357,25 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
       __syncwarp();
       if (lane == 1) trace_mark(a, k_batch, 5);  // MMAs issued
     }
-    if (lane == 0) mma_commit(P.ACCF());
+    if (lane == 0) {
+      mma_commit(P.ACCF());
+      // A commit's mbarrier arrival is performed when its MMAs complete, in no set order
+      // with the other commits: the epilogue's wait on ACCF does not cover the last
+      // LDONE / ADONE arrivals, and one still in flight when the CTA exits would land in
+      // the shared memory of the next CTA on this SM.  So wait for the last committed
+      // phase of every such barrier (bounded) before the CTA can finish.
+      for (int ls = 0; ls < a.sl; ++ls) {
+        if (j_done < ls) continue;  // slot never committed
+        const int j = j_done - (j_done - ls) % a.sl;
+        mbar_wait_drain(P.LDONE(ls), (uint32_t)((j / a.sl) & 1), a.err);
+      }
+      if (!kMerged)
+        for (int as = 0; as < a.sa; ++as) {
+          if (k_done < as) continue;
+          const int kk2 = k_done - (k_done - as) % a.sa;
+          mbar_wait_drain(P.ADONE(as), (uint32_t)((kk2 / a.sa) & 1), a.err);
+        }
+    }
   } else {
     // ---------------- unpack (warps 2-9) ----------------
     // group 0 (warps 2-5) takes even stages, group 1 (warps 6-9) odd stages;
@@ -381,13 +407,18 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
       for (int j = 0; j < hb; ++j) {
         const int k = kb + j;
         if (hb == 1 || k < a.nk) {
-          if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err, a.wait_cycles);
-          if (live && row == 0) trace_mark(a, k, 1);  // codes landed
-          // operand slot ab is free once the MMAs of its previous use (sub-stage k - sa)
+          // Operand slot ab is free once the MMAs of its previous use (sub-stage k - sa)
           // completed; merged: both slots of the batch once the MMAs of the batch two
           // before (this group's previous batch, load stage kb/2 - 2, in the slot two
-          // back; the ring has at least three stages, so that phase is the latest)
-          // completed
+          // back) completed.  This wait comes before the one on the codes: a group sees
+          // only every other phase of a load slot that the two groups share (an odd ring
+          // depth), so FULL(s) may still be a phase behind — its previous load in flight
+          // — and its parity would then already read as this load's.  Once the MMA warp
+          // has taken sub-stage k - sa (merged: batch kb/2 - 2), every load stage up to
+          // it was seen complete, which covers load stage k/sub - sl for every accepted
+          // ring shape ((sl - 1) sub + 1 >= sa; merged: sl >= 3), so the parity below is
+          // unambiguous.  The LDONE phase is the latest of its slot, since the next use
+          // of the slot, load stage kb/2 - 2 + sl, follows this batch.
           if (!kMerged) {
             if (live && k >= a.sa)
               live = mbar_wait_sleep(P.ADONE(ab), ph_a ^ 1u, abort_flag, a.err, a.wait_cycles);
@@ -396,6 +427,8 @@ __global__ void __launch_bounds__(kThreads, 1) tc_grm_kernel(TcArgs a) {
             const uint32_t ph2 = s >= 2 ? ph_l : (ph_l ^ 1u);
             live = mbar_wait_sleep(P.LDONE(s2), ph2, abort_flag, a.err, a.wait_cycles);
           }
+          if (live) live = mbar_wait_sleep(P.FULL(s), ph_l, abort_flag, a.err, a.wait_cycles);
+          if (live && row == 0) trace_mark(a, k, 1);  // codes landed
           live = __all_sync(0xffffffffu, live);  // warp-uniform: the barrier calls below must agree
           if (live) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -958,6 +991,13 @@ struct Rings {
 // stages as fit (at most kMaxSL); as many TMEM operand slots as the
 // accumulators leave room for (at most kMaxSA, even, so that each unpack group
 // owns its slots and named barriers).
+// Operand slots (even) that a ring of sl load stages of sub sub-stages accepts: at
+// most (sl - 1) sub + 1, so that the slot-reuse wait of an unpack group implies its
+// load slot's previous load landed.
+int slots_for_ring(int slots, int sl, int sub) {
+  return std::min(slots, (sl - 1) * sub + 1) & ~1;
+}
+
 Rings tc_rings(int ng, bool pass_b) {
   Rings g;
   const size_t room = kSmemBudget - tc_fixed_bytes();
@@ -979,7 +1019,8 @@ Rings tc_rings(int ng, bool pass_b) {
   g.sub = 4;
   while (g.sub > 1 && room / plan_l_stage(ng, pass_b, g.sub) < 4) g.sub >>= 1;
   g.sl = (int)std::min<size_t>(kMaxSL, room / plan_l_stage(ng, pass_b, g.sub));
-  g.sa = std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols)) & ~1;
+  g.sa = slots_for_ring(std::min<int>(kMaxSA, (int)((kTmemCols - tmem_a0(ng)) / kSlotCols)),
+                        g.sl, g.sub);
   // one sub-stage per handoff (two, a tuner candidate, measured 1-5 % slower)
   g.hb = 1;
   return g;
@@ -1064,7 +1105,10 @@ static Status tc_plan_new(TcPlan** out) {
   if (p->tracing) {
     Status ts = p->trace.reserve((size_t)kTraceStages * kTraceSlots * 8);
     if (!ts.ok()) return bail(ts);
+    // (tracing only) cleared on the legacy stream and waited for, since the handle's
+    // non-blocking stream would not order itself after it
     cudaError_t e = cudaMemset(p->trace.ptr, 0, (size_t)kTraceStages * kTraceSlots * 8);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return bail(fail(SAIGE_ECUDA, "cudaMemset: %s", cudaGetErrorString(e)));
   }
   *out = p;
@@ -1152,6 +1196,9 @@ static cudaError_t launch_tc(unsigned grid, const TcArgs& args, cudaStream_t st)
     return cudaErrorInvalidValue;
   if (a.merged && !(a.hb == 2 && a.sub == 2 && a.sa == 4 && a.sl >= 3))
     return cudaErrorInvalidValue;
+  // an unpack group may wait on a load slot's codes only once the slot's previous load
+  // is known to have landed (see the unpack loop): (sl - 1) sub + 1 >= sa
+  if (!a.merged && (a.sl - 1) * a.sub + 1 < a.sa) return cudaErrorInvalidValue;
   const size_t smem = tc_fixed_bytes() + (size_t)a.sl * plan_l_stage(a.ng, kPassB, a.sub);
   if (smem > kSmemBudget) return cudaErrorInvalidValue;
   if (a.merged)
@@ -1233,8 +1280,9 @@ std::vector<Rings> tc_candidates(int ng, bool pass_b) {
     Rings g;
     g.sub = sub;
     g.sl = (int)std::min<size_t>(kMaxSL, room / ls);
-    g.sa = slots;
+    g.sa = slots_for_ring(slots, g.sl, sub);
     g.hb = 1;
+    if (g.sa < 2) continue;
     out.push_back(g);
     if (g.sa >= 4) {  // the same ring with two sub-stages per handoff (four slots)
       g.hb = 2;

@@ -292,6 +292,8 @@ __global__ void __launch_bounds__(kLayerThreads, 1) mlp_layer_kernel(LayerArgs a
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     int S = 0;
     uint32_t ph = 0;
+    // (lane 0) the last A half and the last tile whose AEMPTY / DFULL was committed
+    int64_t j_done = -1, i_done = -1;
     for (int64_t i = 0; i < n_my && ok; ++i) {
       const int d = (int)(i & 1);
       if (i >= 2) {
@@ -318,14 +320,34 @@ __global__ void __launch_bounds__(kLayerThreads, 1) mlp_layer_kernel(LayerArgs a
                           (h | pp | kk) != 0 ? 1u : 0u);
           }
           mma_commit(AEMPTY(S));
+          j_done = 2 * i + h;
         }
         if (++S == kASlots) { S = 0; ph ^= 1u; }
       }
       if (!ok) break;
-      if (lane == 0) mma_commit(DFULL(d));
+      if (lane == 0) {
+        mma_commit(DFULL(d));
+        i_done = i;
+      }
     }
     __syncwarp();
-    if (lane == 0) mma_commit(FIN);
+    if (lane == 0) {
+      mma_commit(FIN);
+      // A commit's arrival is performed when its MMAs complete, in no set order with the
+      // other commits: wait for the last committed phase of every slot and accumulator
+      // barrier, so that none lands in the shared memory of the next CTA on this SM.
+      mbar_wait_drain(FIN, 0u, a.err);
+      for (int sl = 0; sl < kASlots; ++sl) {
+        if (j_done < sl) continue;
+        const int64_t j = j_done - (j_done - sl) % kASlots;
+        mbar_wait_drain(AEMPTY(sl), (uint32_t)((j / kASlots) & 1), a.err);
+      }
+      for (int dd = 0; dd < 2; ++dd) {
+        if (i_done < dd) continue;
+        const int64_t ii = i_done - (i_done - dd) % 2;
+        mbar_wait_drain(DFULL(dd), (uint32_t)((ii >> 1) & 1), a.err);
+      }
+    }
   } else {
     // ---------------- epilogue ----------------
     const int ew = warp - 2, lg = warp & 3, ch = ew >> 2;

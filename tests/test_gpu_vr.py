@@ -194,16 +194,46 @@ def test_sub_cohort_fits_equal_their_own_fits(concurrent, tune, monkeypatch):
     y, x = cs.gen_pheno(spec)
     rng = np.random.default_rng(5)
     cohorts = []
-    for size in (700, 1300, 2200):
+    for size in (700, 1300, 2203):
         idx = np.sort(rng.choice(n, size, replace=False))
         cohorts.append((idx, y[idx], x[idx]))
+    # every sample, in shuffled order (the concurrent path counts all cohorts in one
+    # launch per marker chunk: unsorted indices and a ragged last word included)
+    idx = rng.permutation(n)
+    cohorts.append((idx, y[idx], x[idx]))
     cfg = cs.AiRemlConfig(max_iter=6, precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
                           warm_start=cs.WARM_RECYCLED)
     res, wall = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg,
                                     concurrent=concurrent)
-    assert wall > 0 and len(res) == 3
+    assert wall > 0 and len(res) == 4
     for (idx, yc, xc), r in zip(cohorts, res):
         one = cs.fit_null_from_bed(bed, n, m, yc, xc, cs.TraitType.Binary, cfg, sample_idx=idx)
         assert r.m_grm == one.m_grm
         assert np.array_equal(r.tau, one.ai_reml.tau)
         assert np.array_equal(r.alpha, one.ai_reml.alpha)
+
+
+def test_concurrent_sub_cohort_fits_are_bit_identical_to_sequential():
+    # Eight mid-size cohorts fitted concurrently (their tensor-core launches share the
+    # SMs with each other's vector kernels, which changes the pipeline timing) must give
+    # exactly the sequential fits: every product is an exact integer sum, so any
+    # difference is a pipeline race.  Block PCG from zero starts runs the most
+    # 42-column products (pass B on a three-stage load ring).
+    n, m = 60_000, 40_000
+    spec = cs.CohortSpec(n=n, m=m, seed=91, missing_rate=0.01, prevalence=0.1, h2=0.2, n_covar=4)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    rng = np.random.default_rng(17)
+    cohorts = []
+    for size in (8_000, 11_000, 15_000, 19_000, 23_000, 27_000, 31_000, 36_000):
+        idx = np.sort(rng.choice(n, size, replace=False))
+        cohorts.append((idx, y[idx], x[idx]))
+    cfg = cs.AiRemlConfig(max_iter=8, tol=1e-5, precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
+                          warm_start=cs.WARM_ZERO)
+    seq, _ = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg, concurrent=False)
+    for _ in range(3):
+        con, _ = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg, concurrent=True)
+        for a, b in zip(seq, con):
+            assert a.m_grm == b.m_grm
+            assert np.array_equal(a.tau, b.tau)
+            assert np.array_equal(a.alpha, b.alpha)

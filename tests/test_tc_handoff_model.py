@@ -174,3 +174,116 @@ def test_merged_batches_wait_on_the_commit_of_their_previous_batch(sl):
                 # that phase is still the barrier's latest when the wait runs: the next use
                 # of the slot is load stage b - 2 + sl > b, whose MMAs follow batch b's
                 assert b - 2 + sl > b
+
+
+def mma_commit_log(nk, sub, sl, sa, merged, abort_at):
+    """The MMA warp's commits (barrier, slot, phase) in issue order, with no further MMA or
+    commit from sub-stage abort_at on, and the (barrier, slot, parity) waits of its exit
+    drain, computed as the kernel does from the last committed load and sub-stage."""
+    log, phases = [], {}
+    t = s = ab = 0
+    j_done = k_done = -1
+    for k in range(nk):
+        if k < abort_at:
+            if not merged:
+                log.append(("ADONE", ab, phases.setdefault(("A", ab), [0])[0]))
+                phases[("A", ab)][0] += 1
+                k_done = k
+            if t == sub - 1 or k == nk - 1:
+                log.append(("LDONE", s, phases.setdefault(("L", s), [0])[0]))
+                phases[("L", s)][0] += 1
+                j_done = k // sub
+        t += 1
+        if t == sub:
+            t, s = 0, (s + 1) % sl
+        ab = (ab + 1) % sa
+    drain = []
+    for ls in range(sl):
+        if j_done >= ls:
+            j = j_done - (j_done - ls) % sl
+            drain.append(("LDONE", ls, (j // sl) & 1))
+    if not merged:
+        for a_s in range(sa):
+            if k_done >= a_s:
+                kk2 = k_done - (k_done - a_s) % sa
+                drain.append(("ADONE", a_s, (kk2 // sa) & 1))
+    return log, drain
+
+
+@pytest.mark.parametrize("shape", [(1, 2, 2, False), (2, 5, 4, False), (4, 3, 6, False),
+                                   (1, 24, 2, False), (2, 3, 4, True), (2, 5, 4, True),
+                                   (2, 24, 4, True)])
+def test_exit_drain_waits_on_the_last_commit_of_every_barrier(shape):
+    # a commit's mbarrier arrival lands when its MMAs complete, in no set order with the
+    # final ACCF commit: the exit drain must wait on the newest phase of every barrier
+    # that received a commit, so that no arrival is still in flight when the CTA exits
+    sub, sl, sa, merged = shape
+    for nk in list(range(1, 30)) + [141, 1164, 1565]:
+        for abort_at in sorted({0, 1, 2, nk // 2, nk - 1, nk}):
+            log, drain = mma_commit_log(nk, sub, sl, sa, merged, abort_at)
+            last = {}
+            for bar, slot, phase in log:
+                last[(bar, slot)] = phase
+            assert sorted((b, sl_, p) for b, sl_, p in drain) == \
+                sorted((b, sl_, ph & 1) for (b, sl_), ph in last.items())
+
+
+def full_waits(nk, sub, sl, sa, hb, merged, grp, slot_wait_first=True):
+    """For each sub-stage k of unpack group grp: (k, load stage J, the load stages known
+    to have landed when the group waits on FULL(J % sl)).  Known: the group's own earlier
+    loads, and — once its slot-reuse wait returned — every load up to the last sub-stage
+    the MMA warp has taken (it takes a sub-stage only after its group saw the codes
+    land).  With slot_wait_first=False the wait on the codes comes first, as it did before
+    (then only the previous batch's slot wait counts)."""
+    out, own = [], set()
+    kb = grp * hb
+    last_taken = -1
+    while kb < nk:
+        for j in range(hb):
+            k = kb + j
+            if k >= nk:
+                break
+            if merged:
+                taken = 2 * (kb // 2 - 2) + 1 if (j == 0 and kb >= 2 * hb) else None
+            else:
+                taken = k - sa if k >= sa else None
+            if slot_wait_first and taken is not None:
+                last_taken = max(last_taken, taken)
+            known = own | {x // sub for x in range(last_taken + 1)}
+            out.append((k, k // sub, known))
+            own.add(k // sub)
+            if not slot_wait_first and taken is not None:
+                last_taken = max(last_taken, taken)
+        kb += 2 * hb
+    return out
+
+
+def accepted_shapes():
+    for sub in (1, 2, 4):
+        for sl in (2, 3, 4, 5, 8, 24):
+            for sa in (2, 4, 6):
+                for hb in (1, 2):
+                    if sa % (2 * hb) == 0 and (sl - 1) * sub + 1 >= sa:  # launch_tc's rule
+                        yield sub, sl, sa, hb, False
+    for sl in (3, 4, 5, 24):
+        yield 2, sl, 4, 2, True
+
+
+def test_codes_wait_never_reads_a_parity_a_phase_early():
+    # A group waits on FULL(s) by parity; if the load slot's previous load (J - sl) were
+    # still landing, the barrier's parity would already read as load J's and the group
+    # would unpack codes that are still being written.  With the slot-reuse wait first,
+    # that previous load is always known to have landed, for every accepted shape.
+    for sub, sl, sa, hb, merged in accepted_shapes():
+        for nk in list(range(1, 48)) + [141, 1165, 1564]:
+            for grp in (0, 1):
+                for k, J, known in full_waits(nk, sub, sl, sa, hb, merged, grp):
+                    assert J - sl < 0 or (J - sl) in known, (sub, sl, sa, hb, merged, nk, k)
+
+
+def test_the_earlier_wait_order_could_read_a_phase_early():
+    # the merged batches with a three-stage ring (pass B at 42 columns): waiting on the
+    # codes before the slot left load stage b - 3 unknown at batch b
+    bad = [(k, J) for k, J, known in full_waits(64, 2, 3, 4, 2, True, 1, slot_wait_first=False)
+           if J - 3 >= 0 and (J - 3) not in known]
+    assert bad
