@@ -6,11 +6,13 @@
 // Sequential: each cohort in turn, every step its own (as fit_null::run per cohort).
 // Concurrent: the .bed streams in by marker chunks, and one launch per chunk counts
 // every cohort's alleles and missing calls of the chunk's markers (each raw row staged
-// once for all cohorts), all under the PCIe-bound transfer; then each cohort's marker
-// selection, GRM and fit run on its own host thread and stream, so that the launches of
-// small cohorts — whose sample-side pass fills a fraction of the GPU and whose PCG
-// steps are latency-bound — overlap with those of the others.  The counts are exact
-// integers either way, so both orders give the same fits.
+// once for all cohorts), all under the PCIe-bound transfer; each cohort's markers are
+// selected on the host, and one more pass over the .bed writes the packed rows of every
+// cohort's GRM (again each raw row staged once); then each cohort's fit runs on its own
+// host thread and stream, so that the launches of small cohorts — whose sample-side
+// pass fills a fraction of the GPU and whose PCG steps are latency-bound — overlap with
+// those of the others.  Counts and rows are exact either way, so both orders give the
+// same fits.
 #include <stdint.h>
 #include <string.h>
 
@@ -39,6 +41,10 @@ struct CohortJob {
   bool have_stats = false;
   std::vector<double> af, mac;
   std::vector<int64_t> nv;
+  // the cohort's GRM handle, when built beforehand (rows from the shared gather)
+  saige_grm* h = nullptr;
+  std::vector<int64_t> gidx;
+  std::vector<double> gaf;
   int64_t m_grm = 0;
   int32_t rc = SAIGE_OK;
   std::string err;
@@ -48,6 +54,15 @@ void run_cohort(int device, const uint8_t* d_bed, size_t bed_len, int64_t n_fam,
                 int32_t p, int32_t trait, double min_maf, double max_missing,
                 const saige_ai_reml_config* cfg, CohortJob& job) {
   cudaSetDevice(device);
+  if (job.h) {  // handle built beforehand: only the fit
+    int32_t rc = saige_fit_ai_reml(job.h, job.y, job.x, job.n, p, trait, cfg, job.out, job.alpha,
+                                   nullptr, nullptr, nullptr, nullptr);
+    if (rc != SAIGE_OK) job.err = saige_last_error();
+    grm_shell_destroy(job.h);
+    job.h = nullptr;
+    job.rc = rc;
+    return;
+  }
   int32_t rc = SAIGE_OK;
   if (!job.have_stats) {
     job.af.resize((size_t)m_tot);
@@ -78,12 +93,18 @@ void run_cohort(int device, const uint8_t* d_bed, size_t bed_len, int64_t n_fam,
   job.rc = rc;
 }
 
+// Every cohort's sample indices on the device, each list padded to 16 entries.
+struct SampleLists {
+  DevBuf d_sidx;
+  std::vector<int64_t> offs;
+};
+
 // Uploads the .bed into d_bed in marker chunks on a copy stream while, chunk by chunk,
 // one launch counts every cohort's alleles and missing calls of the chunk's markers;
-// fills each job's marker statistics.  Rows too long to stage in shared memory return
-// with have_stats false (each cohort then counts on its own).
+// fills each job's marker statistics and leaves the sample lists on the device.
+
 Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
-                        DevBuf& d_bed, std::vector<CohortJob>& jobs) {
+                        DevBuf& d_bed, std::vector<CohortJob>& jobs, SampleLists& lists) {
   const int64_t bpm = (n_fam + 3) / 4;
   const int k = (int)jobs.size();
   // every cohort's sample list, each padded to a multiple of 16 entries
@@ -104,7 +125,9 @@ Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64
   }
   cudaStream_t cp = nullptr, kst = nullptr;
   std::vector<cudaEvent_t> ev;
-  DevBuf d_sidx, d_offs, d_ns, d_cnt;
+  DevBuf& d_sidx = lists.d_sidx;
+  lists.offs = offs;
+  DevBuf d_offs, d_ns, d_cnt;
   std::vector<long long> cnt;
   auto body = [&]() -> Status {
     SG_CUDA(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking));
@@ -149,7 +172,6 @@ Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64
   if (kst) cudaStreamSynchronize(kst);
   {
     ReleaseScope idle(ReleaseMode::kIdle, nullptr);  // both streams have drained
-    d_sidx.release();
     d_offs.release();
     d_ns.release();
     d_cnt.release();
@@ -167,6 +189,82 @@ Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64
                       j.nv.data());
     j.have_stats = true;
   }
+  return Status();
+}
+
+// Every cohort's marker selection and GRM handle, with the packed rows of all of them
+// from one pass over the device .bed (each raw row staged once for all cohorts).
+Status build_handles(const uint8_t* d_bed, int64_t n_fam, int64_t m_tot, int dev, double min_maf,
+                     double max_missing, uint64_t seed, const SampleLists& lists,
+                     std::vector<CohortJob>& jobs) {
+  const int k = (int)jobs.size();
+  const int64_t bpm = (n_fam + 3) / 4;
+  PhaseTimer tm;
+  std::vector<int32_t> row_of((size_t)k * m_tot, -1);
+  // selection, handle and metadata of each cohort on its own host thread (a few ms of
+  // host work and uploads each)
+  auto prepare = [&](int c) {
+    CohortJob& j = jobs[(size_t)c];
+    cudaSetDevice(dev);
+    j.gidx.assign((size_t)m_tot, 0);
+    std::vector<int64_t> vidx((size_t)m_tot);
+    int64_t m_grm = 0, m_vr = 0;
+    j.rc = saige_select_grm_markers(j.af.data(), j.mac.data(), j.nv.data(), m_tot, j.n, min_maf,
+                                    max_missing, seed, j.gidx.data(), &m_grm, vidx.data(), &m_vr);
+    if (j.rc == SAIGE_OK) {
+      j.gidx.resize((size_t)m_grm);
+      j.m_grm = m_grm;
+      j.gaf.resize((size_t)m_grm);
+      for (int64_t r = 0; r < m_grm; ++r) {
+        j.gaf[(size_t)r] = j.af[(size_t)j.gidx[(size_t)r]];
+        row_of[(size_t)c * m_tot + (size_t)j.gidx[(size_t)r]] = (int32_t)r;
+      }
+      j.rc = grm_shell_create(dev, j.n, m_grm, j.gaf.data(), &j.h).code;
+    }
+    if (j.rc != SAIGE_OK) j.err = saige_last_error();
+  };
+  {
+    std::vector<std::thread> th;
+    for (int c = 0; c < k; ++c) th.emplace_back(prepare, c);
+    for (auto& t : th) t.join();
+  }
+  for (int c = 0; c < k; ++c)
+    if (jobs[(size_t)c].rc != SAIGE_OK)
+      return fail(jobs[(size_t)c].rc, "cohort %d: %s", c, jobs[(size_t)c].err.c_str());
+  tm.mark(" select+alloc");
+  cudaStream_t st = nullptr;
+  DevBuf d_rows, d_co;
+  auto body = [&]() -> Status {
+    SG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    SG_TRY(d_rows.reserve(row_of.size() * 4));
+    SG_TRY(d_co.reserve((size_t)k * sizeof(CohortRows)));
+    std::vector<CohortRows> co((size_t)k);
+    for (int c = 0; c < k; ++c) {
+      const saige_grm* h = jobs[(size_t)c].h;
+      co[(size_t)c] = CohortRows{h->geno, d_rows.as<int32_t>() + (size_t)c * m_tot, h->wpr, h->n,
+                                 lists.offs[(size_t)c]};
+    }
+    SG_CUDA(cudaMemcpyAsync(d_rows.ptr, row_of.data(), row_of.size() * 4, cudaMemcpyHostToDevice,
+                            st));
+    SG_CUDA(cudaMemcpyAsync(d_co.ptr, co.data(), co.size() * sizeof(CohortRows),
+                            cudaMemcpyHostToDevice, st));
+    SG_CUDA(launch_bed_gather_cohorts(d_bed, bpm, 0, m_tot, lists.d_sidx.as<int32_t>(),
+                                      d_co.as<CohortRows>(), k, st));
+    SG_CUDA(cudaStreamSynchronize(st));
+    return Status();
+  };
+  Status s = body();
+  if (st) cudaStreamSynchronize(st);
+  {
+    ReleaseScope idle(ReleaseMode::kIdle, nullptr);  // the stream has drained
+    d_rows.release();
+    d_co.release();
+  }
+  if (st) cudaStreamDestroy(st);
+  SG_TRY(s);
+  tm.mark(" gather");
+  for (int c = 0; c < k; ++c) SG_TRY(grm_shell_finish(jobs[(size_t)c].h, jobs[(size_t)c].gaf.data()));
+  tm.mark(" finish");
   return Status();
 }
 
@@ -209,9 +307,26 @@ SG_API int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_
     Status s = d_bed.reserve(bed_len);
     if (!s.ok()) return s.code;
     const int64_t bpm = (n_fam + 3) / 4;
+    SampleLists lists;
+    auto drop_handles = [&]() {
+      for (CohortJob& j : jobs)
+        if (j.h) {
+          grm_shell_destroy(j.h);
+          j.h = nullptr;
+        }
+    };
+    PhaseTimer tm;
     if (concurrent && bpm <= 200 * 1024) {
-      s = upload_and_count(bed, bed_len, n_fam, m_tot, d_bed, jobs);
-      if (!s.ok()) return s.code;
+      s = upload_and_count(bed, bed_len, n_fam, m_tot, d_bed, jobs, lists);
+      tm.mark("upload+counts");
+      if (s.ok())
+        s = build_handles(d_bed.as<uint8_t>(), n_fam, m_tot, dev, min_maf, max_missing, cf.seed,
+                          lists, jobs);
+      lists.d_sidx.release();
+      if (!s.ok()) {
+        drop_handles();
+        return s.code;
+      }
     } else if (cudaMemcpy(d_bed.ptr, bed, bed_len, cudaMemcpyHostToDevice) != cudaSuccess) {
       return fail(SAIGE_ECUDA, "bed upload failed: %s", cudaGetErrorString(cudaGetLastError())).code;
     }
@@ -223,6 +338,7 @@ SG_API int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_
         th.emplace_back(run_cohort, dev, db, bed_len, n_fam, m_tot, p, trait, min_maf, max_missing,
                         &cf, std::ref(jobs[(size_t)c]));
       for (auto& t : th) t.join();
+      tm.mark("fits");
     } else {
       for (int32_t c = 0; c < n_cohorts; ++c)
         run_cohort(dev, db, bed_len, n_fam, m_tot, p, trait, min_maf, max_missing, &cf,

@@ -1104,6 +1104,32 @@ SG_API int32_t saige_grm_create_from_bed(const uint8_t* bed, size_t bed_len, int
   SG_GUARD_END
 }
 
+namespace saige {
+
+Status grm_shell_create(int dev, int64_t n, int64_t m, const double* af, saige_grm** out) {
+  *out = nullptr;
+  saige_grm* h = new saige_grm();
+  h->device = dev;
+  Status s = grm_alloc(h, n, m);
+  if (s.ok() && m > 0) s = grm_upload_meta(h, af);
+  if (!s.ok()) {
+    grm_free(h);
+    return s;
+  }
+  *out = h;
+  return Status();
+}
+
+Status grm_shell_finish(saige_grm* h, const double* af) {
+  if (h->m > 0) SG_TRY(grm_blank_degenerate_rows(h, af));
+  SG_CUDA(cudaStreamSynchronize(h->stream));
+  return Status();
+}
+
+void grm_shell_destroy(saige_grm* h) { grm_free(h); }
+
+}  // namespace saige
+
 SG_API int32_t saige_grm_create_from_bed_dev(const uint8_t* bed_dev, size_t bed_len,
                                              int64_t n_fam, int64_t m_tot,
                                              const int64_t* sample_idx, int64_t n,

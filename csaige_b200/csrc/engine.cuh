@@ -140,6 +140,14 @@ struct saige_grm {
 
 namespace saige {
 
+// A handle for n samples and m marker rows (allele frequencies af) whose packed rows
+// the caller writes — rows [m, m_pad) are already coded 11 — then grm_shell_finish
+// recodes the zero-variance rows and drains the handle's stream.  For builds that fill
+// several handles from one pass over the .bed (the sub-cohorts).
+Status grm_shell_create(int dev, int64_t n, int64_t m, const double* af, saige_grm** out);
+Status grm_shell_finish(saige_grm* h, const double* af);
+void grm_shell_destroy(saige_grm* h);
+
 // Kv for q columns of v (ld = h->n_pad, padding rows zero) into kp.
 // active (host, length q, may be NULL) selects columns; others are skipped.
 Status grm_product(saige_grm* h, const double* v, double* kp, int q, const int32_t* active,

@@ -25,6 +25,22 @@ cudaError_t launch_bed_count_cohorts(const uint8_t* bed, int64_t bytes_per_marke
                                      const int64_t* ns, int n_cohorts, int64_t m_tot,
                                      long long* counts, cudaStream_t st);
 
+// One cohort's output of launch_bed_gather_cohorts: raw marker j goes to row
+// row_of[j] of geno (wpr words per row; -1: not kept), its n samples at
+// sidx[sidx_off ..] (sidx_off a multiple of 16).
+struct CohortRows {
+  uint32_t* geno;
+  const int32_t* row_of;
+  int64_t wpr;
+  int64_t n;
+  int64_t sidx_off;
+};
+// Gathers raw rows j0 .. j0 + n_rows into every cohort that keeps them (co: device
+// array of n_cohorts entries).  Rows of more than 200 KB are refused.
+cudaError_t launch_bed_gather_cohorts(const uint8_t* bed, int64_t bytes_per_marker, int64_t j0,
+                                      int64_t n_rows, const int32_t* sidx, const CohortRows* co,
+                                      int n_cohorts, cudaStream_t st);
+
 // ---- synthetic cohort ------------------------------------------------------
 struct CohortDev;
 cudaError_t launch_gen_bed(const void* layout, uint8_t* bed, int64_t bytes_per_marker,

@@ -210,7 +210,99 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// The packed rows of several sample subsets from one pass over the raw rows: block =
+// rpb consecutive raw markers from j0 + blockIdx.x rpb, staged once; for every cohort,
+// each thread loads the sample indices of a 16-sample word once and gathers that word
+// from each staged row the cohort keeps (row_of[j] >= 0), repacked and written exactly
+// as bed_gather_kernel writes it (padding samples coded 11).
+constexpr int kGatherRowsMax = 4;
+
+__global__ void __launch_bounds__(kThreads)
+    bed_gather_cohorts_kernel(const uint8_t* __restrict__ bed, int64_t bpm, int64_t j0,
+                              int64_t n_rows, int rpb, const int32_t* __restrict__ sidx,
+                              const CohortRows* __restrict__ co, int n_cohorts) {
+  extern __shared__ __align__(16) uint8_t row_s[];
+  const int64_t stride = (bpm + 31) / 16 * 16;  // round_up(bpm + 16, 16)
+  const int64_t jb = j0 + (int64_t)blockIdx.x * rpb;
+  const int64_t left = j0 + n_rows - jb;
+  const int nr = left < rpb ? (int)left : rpb;
+  const uint8_t* src[kGatherRowsMax];
+#pragma unroll
+  for (int q = 0; q < kGatherRowsMax; ++q)
+    src[q] = q < nr ? stage_row(bed + 3 + (jb + q) * bpm, bpm, row_s + q * stride) : nullptr;
+  for (int c = 0; c < n_cohorts; ++c) {
+    const CohortRows cr = co[c];
+    int32_t r[kGatherRowsMax];
+    bool any = false;
+#pragma unroll
+    for (int q = 0; q < kGatherRowsMax; ++q) {
+      r[q] = q < nr ? cr.row_of[jb + q] : -1;
+      any |= r[q] >= 0;
+    }
+    if (!any) continue;
+    const int32_t* sc = sidx + cr.sidx_off;
+    const bool vec = (reinterpret_cast<uintptr_t>(sc) & 15u) == 0;
+    const int64_t n_real = (cr.n + 15) / 16;
+    for (int64_t w = threadIdx.x; w < cr.wpr; w += blockDim.x) {
+      if (w >= n_real) {
+#pragma unroll
+        for (int q = 0; q < kGatherRowsMax; ++q)
+          if (r[q] >= 0) cr.geno[(int64_t)r[q] * cr.wpr + w] = 0xFFFFFFFFu;
+        continue;
+      }
+      const int64_t k0 = 16 * w;
+      const int kn = (cr.n - k0) < 16 ? (int)(cr.n - k0) : 16;
+      int32_t ss[16];
+      if (vec && kn == 16) {
+        const int4* s4 = reinterpret_cast<const int4*>(sc + k0);
+#pragma unroll
+        for (int g = 0; g < 4; ++g) {
+          const int4 v = __ldg(s4 + g);
+          ss[4 * g] = v.x;
+          ss[4 * g + 1] = v.y;
+          ss[4 * g + 2] = v.z;
+          ss[4 * g + 3] = v.w;
+        }
+      } else {
+#pragma unroll
+        for (int e = 0; e < 16; ++e) ss[e] = e < kn ? sc[k0 + e] : 0;
+      }
+      const uint32_t keep = kn >= 16 ? 0xFFFFFFFFu : ((1u << (2 * kn)) - 1u);
+#pragma unroll
+      for (int q = 0; q < kGatherRowsMax; ++q) {
+        if (r[q] < 0) continue;
+        uint32_t word = 0;
+#pragma unroll
+        for (int e = 0; e < 16; ++e)
+          word |= ((uint32_t)(src[q][ss[e] >> 2] >> ((ss[e] & 3) * 2)) & 3u) << (2 * e);
+        cr.geno[(int64_t)r[q] * cr.wpr + w] = to_device_layout((word & keep) | ~keep);
+      }
+    }
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_bed_gather_cohorts(const uint8_t* bed, int64_t bpm, int64_t j0, int64_t n_rows,
+                                      const int32_t* sidx, const CohortRows* co, int n_cohorts,
+                                      cudaStream_t st) {
+  if (n_rows <= 0) return cudaSuccess;
+  if (bpm > kSmemRowMax) return cudaErrorInvalidValue;
+  // as many rows per block as 200 KB of shared memory hold (each index load then serves
+  // all of them), at most kGatherRowsMax
+  const int64_t stride = round_up(bpm + 16, 16);
+  const int rpb = (int)std::max<int64_t>(1, std::min<int64_t>(kGatherRowsMax, kSmemRowMax / stride));
+  const size_t smem = (size_t)(stride * rpb);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(bed_gather_cohorts_kernel,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+  }
+  bed_gather_cohorts_kernel<<<(unsigned)ceil_div(n_rows, rpb), kThreads, smem, st>>>(
+      bed, bpm, j0, n_rows, rpb, sidx, co, n_cohorts);
+  count_launches(1);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_bed_count_cohorts(const uint8_t* bed, int64_t bpm, int64_t j0, int64_t n_rows,
                                      const int32_t* sidx, const int64_t* offs, const int64_t* ns,
