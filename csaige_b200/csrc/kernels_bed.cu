@@ -216,8 +216,9 @@ __global__ void __launch_bounds__(kThreads)
 // from each staged row the cohort keeps (row_of[j] >= 0), repacked and written exactly
 // as bed_gather_kernel writes it (padding samples coded 11).
 constexpr int kGatherRowsMax = 4;
+constexpr int kGatherThreads = 1024;  // one block of four staged rows per SM: 32 warps
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kGatherThreads)
     bed_gather_cohorts_kernel(const uint8_t* __restrict__ bed, int64_t bpm, int64_t j0,
                               int64_t n_rows, int rpb, const int32_t* __restrict__ sidx,
                               const CohortRows* __restrict__ co, int n_cohorts) {
@@ -298,7 +299,7 @@ cudaError_t launch_bed_gather_cohorts(const uint8_t* bed, int64_t bpm, int64_t j
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
   }
-  bed_gather_cohorts_kernel<<<(unsigned)ceil_div(n_rows, rpb), kThreads, smem, st>>>(
+  bed_gather_cohorts_kernel<<<(unsigned)ceil_div(n_rows, rpb), kGatherThreads, smem, st>>>(
       bed, bpm, j0, n_rows, rpb, sidx, co, n_cohorts);
   count_launches(1);
   return cudaGetLastError();
