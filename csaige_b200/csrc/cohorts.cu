@@ -16,6 +16,8 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <algorithm>
+#include <atomic>
 #include <chrono>
 #include <thread>
 #include <vector>
@@ -332,11 +334,24 @@ SG_API int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_
     }
     const uint8_t* db = d_bed.as<uint8_t>();
     if (concurrent) {
+      // a pool of host threads, each with its cohorts' streams: half the hardware threads
+      // (at least two; a fit's host thread spins on its stream's syncs, so one per
+      // cohort oversubscribed the cores and stalled whole runs), largest cohorts first
+      std::vector<int32_t> order((size_t)n_cohorts);
+      for (int32_t c = 0; c < n_cohorts; ++c) order[(size_t)c] = c;
+      std::stable_sort(order.begin(), order.end(),
+                       [&](int32_t a, int32_t b) { return jobs[(size_t)a].n > jobs[(size_t)b].n; });
+      const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+      const int32_t workers = std::min<int32_t>(n_cohorts, (int32_t)std::max(2u, hw / 2));
+      std::atomic<int32_t> next{0};
+      auto worker = [&]() {
+        for (int32_t i = next++; i < n_cohorts; i = next++)
+          run_cohort(dev, db, bed_len, n_fam, m_tot, p, trait, min_maf, max_missing, &cf,
+                     jobs[(size_t)order[(size_t)i]]);
+      };
       std::vector<std::thread> th;
-      th.reserve((size_t)n_cohorts);
-      for (int32_t c = 0; c < n_cohorts; ++c)
-        th.emplace_back(run_cohort, dev, db, bed_len, n_fam, m_tot, p, trait, min_maf, max_missing,
-                        &cf, std::ref(jobs[(size_t)c]));
+      th.reserve((size_t)workers);
+      for (int32_t w = 0; w < workers; ++w) th.emplace_back(worker);
       for (auto& t : th) t.join();
       tm.mark("fits");
     } else {
