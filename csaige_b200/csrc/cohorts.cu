@@ -16,9 +16,12 @@
 #include <stdint.h>
 #include <string.h>
 
+#include <math.h>
+
 #include <algorithm>
 #include <atomic>
 #include <chrono>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -194,6 +197,222 @@ Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64
   return Status();
 }
 
+// Host-mapped memory for the counts and row maps of a streamed cohort build (read and
+// written by kernels over PCIe: no copy queues behind the .bed's chunks on the copy
+// engine).  One block is kept for the process; a call that finds it in use by another
+// thread takes a block of its own.
+std::mutex g_cmap_mu;
+void* g_cmap = nullptr;
+size_t g_cmap_bytes = 0;
+bool g_cmap_busy = false;
+
+struct CohortMapped {
+  void* p = nullptr;
+  bool own = false;
+  ~CohortMapped() {
+    if (own) {
+      cudaFreeHost(p);
+    } else if (p) {
+      std::lock_guard<std::mutex> lk(g_cmap_mu);
+      g_cmap_busy = false;
+    }
+  }
+  Status take(size_t bytes) {
+    {
+      std::lock_guard<std::mutex> lk(g_cmap_mu);
+      if (!g_cmap_busy) {
+        if (g_cmap_bytes < bytes) {
+          // with headroom (pinning host memory costs milliseconds to a second): a small
+          // first call does not force a larger one to pin again
+          const size_t want = std::max<size_t>(bytes, (size_t)64 << 20);
+          if (g_cmap) cudaFreeHost(g_cmap);
+          g_cmap = nullptr;
+          g_cmap_bytes = 0;
+          SG_CUDA(cudaHostAlloc(&g_cmap, want, cudaHostAllocMapped));
+          g_cmap_bytes = want;
+        }
+        g_cmap_busy = true;
+        p = g_cmap;
+        return Status();
+      }
+    }
+    own = true;
+    SG_CUDA(cudaHostAlloc(&p, bytes, cudaHostAllocMapped));
+    return Status();
+  }
+};
+
+// The streamed build of every cohort's GRM (MIXED fits): the .bed streams in by marker
+// chunks on a copy stream; as each chunk lands, one launch counts every cohort's alleles
+// and missing calls of its markers (into host-mapped memory), the host applies each
+// cohort's marker QC (fit_null.rs:209-222) to them and writes where each passing marker
+// goes (the next row of that cohort), and one launch gathers the chunk's rows into every
+// cohort's handle — all under the PCIe-bound transfer.  Rows are then every QC-passing
+// marker in .bed order; grm_stream_rows_finish draws the variance-ratio candidates among
+// them and keeps them in place with zero metadata, so the tensor-core products are
+// bit-identical to those of a handle holding only the GRM markers (the sequential path).
+Status stream_cohorts(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot, int dev,
+                      double min_maf, double max_missing, uint64_t seed, DevBuf& d_bed,
+                      std::vector<CohortJob>& jobs) {
+  const int64_t bpm = (n_fam + 3) / 4;
+  const int k = (int)jobs.size();
+  PhaseTimer tm;
+  std::vector<int32_t> all;
+  std::vector<int64_t> offs((size_t)k), ns((size_t)k);
+  for (int c = 0; c < k; ++c) {
+    std::vector<int32_t> sv;
+    bool identity = true;
+    SG_TRY(check_subset(jobs[(size_t)c].sidx, jobs[(size_t)c].n, n_fam, sv, identity));
+    offs[(size_t)c] = (int64_t)all.size();
+    ns[(size_t)c] = jobs[(size_t)c].n;
+    all.insert(all.end(), sv.begin(), sv.end());
+    all.resize((size_t)round_up((int64_t)all.size(), 16), 0);
+  }
+  CohortMapped mp;
+  const size_t cnt_bytes = (size_t)k * m_tot * 2 * sizeof(long long);
+  SG_TRY(mp.take(cnt_bytes + (size_t)m_tot * k * sizeof(int32_t)));
+  long long* cnt_h = static_cast<long long*>(mp.p);
+  int32_t* map_h = reinterpret_cast<int32_t*>(static_cast<char*>(mp.p) + cnt_bytes);
+  void* mp_dev = nullptr;
+  SG_CUDA(cudaHostGetDevicePointer(&mp_dev, mp.p, 0));
+  long long* cnt_d = static_cast<long long*>(mp_dev);
+  const int32_t* map_d = reinterpret_cast<const int32_t*>(static_cast<char*>(mp_dev) + cnt_bytes);
+  std::vector<std::vector<int64_t>> pass((size_t)k);
+  cudaStream_t cp = nullptr, kst = nullptr;
+  std::vector<cudaEvent_t> ev;
+  cudaEvent_t counted = nullptr;
+  DevBuf d_sidx, d_offs, d_ns;
+  auto body = [&]() -> Status {
+    SG_CUDA(cudaStreamCreateWithFlags(&cp, cudaStreamNonBlocking));
+    SG_CUDA(cudaStreamCreateWithFlags(&kst, cudaStreamNonBlocking));
+    SG_CUDA(cudaEventCreateWithFlags(&counted, cudaEventDisableTiming));
+    SG_TRY(d_sidx.reserve(all.size() * 4));
+    SG_TRY(d_offs.reserve((size_t)k * 8));
+    SG_TRY(d_ns.reserve((size_t)k * 8));
+    // the sample lists ahead of the .bed on the copy engine
+    SG_CUDA(cudaMemcpyAsync(d_sidx.ptr, all.data(), all.size() * 4, cudaMemcpyHostToDevice, kst));
+    SG_CUDA(cudaMemcpyAsync(d_offs.ptr, offs.data(), (size_t)k * 8, cudaMemcpyHostToDevice, kst));
+    SG_CUDA(cudaMemcpyAsync(d_ns.ptr, ns.data(), (size_t)k * 8, cudaMemcpyHostToDevice, kst));
+    SG_CUDA(cudaStreamSynchronize(kst));
+    constexpr int kChunks = 32;
+    const int64_t per = std::max<int64_t>(1, ceil_div(m_tot, (int64_t)kChunks));
+    uint8_t* dst = d_bed.as<uint8_t>();
+    std::vector<std::pair<int64_t, int64_t>> spans;
+    for (int64_t j0 = 0; j0 < m_tot; j0 += per) {
+      const int64_t j1 = std::min(m_tot, j0 + per);
+      const size_t lo = j0 == 0 ? 0 : (size_t)(3 + j0 * bpm);
+      const size_t hi = j1 == m_tot ? bed_len : (size_t)(3 + j1 * bpm);
+      SG_CUDA(cudaMemcpyAsync(dst + lo, bed + lo, hi - lo, cudaMemcpyHostToDevice, cp));
+      cudaEvent_t e = nullptr;
+      SG_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+      ev.push_back(e);
+      SG_CUDA(cudaEventRecord(e, cp));
+      spans.emplace_back(j0, j1);
+    }
+    // the handles (room for every marker) while the first chunks land
+    {
+      std::vector<std::thread> th;
+      for (int c = 0; c < k; ++c)
+        th.emplace_back([&, c]() {
+          cudaSetDevice(dev);
+          CohortJob& j = jobs[(size_t)c];
+          j.rc = grm_shell_create_cap(dev, j.n, m_tot, &j.h).code;
+          if (j.rc != SAIGE_OK) j.err = saige_last_error();
+          j.af.resize((size_t)m_tot);
+          j.mac.resize((size_t)m_tot);
+          j.nv.resize((size_t)m_tot);
+          pass[(size_t)c].reserve((size_t)m_tot);
+        });
+      for (auto& t : th) t.join();
+    }
+    for (int c = 0; c < k; ++c)
+      if (jobs[(size_t)c].rc != SAIGE_OK)
+        return fail(jobs[(size_t)c].rc, "cohort %d: %s", c, jobs[(size_t)c].err.c_str());
+    tm.mark(" handles");
+    std::vector<std::pair<int, int64_t>> degenerate;
+    for (size_t i = 0; i < spans.size(); ++i) {
+      const int64_t j0 = spans[i].first, j1 = spans[i].second;
+      SG_CUDA(cudaStreamWaitEvent(kst, ev[i], 0));
+      SG_CUDA(launch_bed_count_cohorts(dst, bpm, j0, j1 - j0, d_sidx.as<int32_t>(),
+                                       d_offs.as<int64_t>(), d_ns.as<int64_t>(), k, m_tot, cnt_d,
+                                       kst));
+      SG_CUDA(cudaEventRecord(counted, kst));
+      SG_CUDA(cudaEventSynchronize(counted));
+      degenerate.clear();
+      for (int c = 0; c < k; ++c) {
+        CohortJob& jb = jobs[(size_t)c];
+        stats_from_counts(cnt_h + 2 * ((size_t)c * m_tot + j0), j1 - j0, jb.n, jb.af.data() + j0,
+                          jb.mac.data() + j0, jb.nv.data() + j0);
+        std::vector<int64_t>& ps = pass[(size_t)c];
+        for (int64_t j = j0; j < j1; ++j) {
+          int32_t r = -1;
+          if (marker_qc_pass(jb.af[(size_t)j], jb.nv[(size_t)j], jb.n, min_maf, max_missing)) {
+            r = (int32_t)ps.size();
+            ps.push_back(j);
+            const double pj = jb.af[(size_t)j];
+            if (!(sqrt(2.0 * pj * (1.0 - pj)) > 1e-10)) degenerate.emplace_back(c, (int64_t)r);
+          }
+          map_h[(size_t)j * k + c] = r;
+        }
+      }
+      for (int c0 = 0; c0 < k; c0 += kCohortsPerLaunch) {
+        CohortSet set{};
+        set.n = std::min(kCohortsPerLaunch, k - c0);
+        for (int q = 0; q < set.n; ++q) {
+          const saige_grm* h = jobs[(size_t)(c0 + q)].h;
+          set.c[q] = CohortRows{h->geno, map_d + (c0 + q), (int64_t)k, h->wpr, h->n,
+                                offs[(size_t)(c0 + q)]};
+        }
+        SG_CUDA(launch_bed_gather_cohorts(dst, bpm, j0, j1 - j0, d_sidx.as<int32_t>(), set, kst));
+      }
+      // a zero standardised column: codes 11, as grm_blank_degenerate_rows does
+      for (const auto& dg : degenerate) {
+        const saige_grm* h = jobs[(size_t)dg.first].h;
+        SG_CUDA(cudaMemsetAsync(h->geno + (size_t)dg.second * h->wpr, 0xFF, (size_t)h->wpr * 4, kst));
+      }
+    }
+    SG_CUDA(cudaStreamSynchronize(kst));
+    SG_CUDA(cudaStreamSynchronize(cp));
+    tm.mark(" upload+counts+gather");
+    return Status();
+  };
+  Status s = body();
+  if (cp) cudaStreamSynchronize(cp);
+  if (kst) cudaStreamSynchronize(kst);
+  {
+    ReleaseScope idle(ReleaseMode::kIdle, nullptr);  // both streams have drained
+    d_sidx.release();
+    d_offs.release();
+    d_ns.release();
+  }
+  for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  if (counted) cudaEventDestroy(counted);
+  if (cp) cudaStreamDestroy(cp);
+  if (kst) cudaStreamDestroy(kst);
+  SG_TRY(s);
+  // variance-ratio candidates, padding rows and metadata of each cohort (in parallel)
+  {
+    std::vector<std::thread> th;
+    for (int c = 0; c < k; ++c)
+      th.emplace_back([&, c]() {
+        cudaSetDevice(dev);
+        CohortJob& j = jobs[(size_t)c];
+        std::vector<int64_t> vidx;
+        j.rc = grm_stream_rows_finish(j.h, pass[(size_t)c], j.af.data(), j.mac.data(), seed, vidx)
+                   .code;
+        if (j.rc != SAIGE_OK) j.err = saige_last_error();
+        j.m_grm = j.h->m_eff;
+        j.have_stats = true;
+      });
+    for (auto& t : th) t.join();
+  }
+  for (int c = 0; c < k; ++c)
+    if (jobs[(size_t)c].rc != SAIGE_OK)
+      return fail(jobs[(size_t)c].rc, "cohort %d: %s", c, jobs[(size_t)c].err.c_str());
+  tm.mark(" finish");
+  return Status();
+}
+
 // Every cohort's marker selection and GRM handle, with the packed rows of all of them
 // from one pass over the device .bed (each raw row staged once for all cohorts).
 Status build_handles(const uint8_t* d_bed, int64_t n_fam, int64_t m_tot, int dev, double min_maf,
@@ -235,23 +454,22 @@ Status build_handles(const uint8_t* d_bed, int64_t n_fam, int64_t m_tot, int dev
       return fail(jobs[(size_t)c].rc, "cohort %d: %s", c, jobs[(size_t)c].err.c_str());
   tm.mark(" select+alloc");
   cudaStream_t st = nullptr;
-  DevBuf d_rows, d_co;
+  DevBuf d_rows;
   auto body = [&]() -> Status {
     SG_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     SG_TRY(d_rows.reserve(row_of.size() * 4));
-    SG_TRY(d_co.reserve((size_t)k * sizeof(CohortRows)));
-    std::vector<CohortRows> co((size_t)k);
-    for (int c = 0; c < k; ++c) {
-      const saige_grm* h = jobs[(size_t)c].h;
-      co[(size_t)c] = CohortRows{h->geno, d_rows.as<int32_t>() + (size_t)c * m_tot, h->wpr, h->n,
-                                 lists.offs[(size_t)c]};
-    }
     SG_CUDA(cudaMemcpyAsync(d_rows.ptr, row_of.data(), row_of.size() * 4, cudaMemcpyHostToDevice,
                             st));
-    SG_CUDA(cudaMemcpyAsync(d_co.ptr, co.data(), co.size() * sizeof(CohortRows),
-                            cudaMemcpyHostToDevice, st));
-    SG_CUDA(launch_bed_gather_cohorts(d_bed, bpm, 0, m_tot, lists.d_sidx.as<int32_t>(),
-                                      d_co.as<CohortRows>(), k, st));
+    for (int c0 = 0; c0 < k; c0 += kCohortsPerLaunch) {
+      CohortSet set{};
+      set.n = std::min(kCohortsPerLaunch, k - c0);
+      for (int i = 0; i < set.n; ++i) {
+        const saige_grm* h = jobs[(size_t)(c0 + i)].h;
+        set.c[i] = CohortRows{h->geno, d_rows.as<int32_t>() + (size_t)(c0 + i) * m_tot, 1,
+                              h->wpr, h->n, lists.offs[(size_t)(c0 + i)]};
+      }
+      SG_CUDA(launch_bed_gather_cohorts(d_bed, bpm, 0, m_tot, lists.d_sidx.as<int32_t>(), set, st));
+    }
     SG_CUDA(cudaStreamSynchronize(st));
     return Status();
   };
@@ -260,7 +478,6 @@ Status build_handles(const uint8_t* d_bed, int64_t n_fam, int64_t m_tot, int dev
   {
     ReleaseScope idle(ReleaseMode::kIdle, nullptr);  // the stream has drained
     d_rows.release();
-    d_co.release();
   }
   if (st) cudaStreamDestroy(st);
   SG_TRY(s);
@@ -318,7 +535,16 @@ SG_API int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_
         }
     };
     PhaseTimer tm;
-    if (concurrent && bpm <= 200 * 1024) {
+    if (concurrent && bpm <= 200 * 1024 && cf.precision == SAIGE_PREC_MIXED) {
+      s = stream_cohorts(bed, bed_len, n_fam, m_tot, dev, min_maf, max_missing, cf.seed, d_bed,
+                         jobs);
+      if (!s.ok()) {
+        drop_handles();
+        return s.code;
+      }
+    } else if (concurrent && bpm <= 200 * 1024) {
+      // FP32 fits: the rows must be the GRM markers only (an FP32 product's grouping of
+      // its sums follows the row count), so the selection waits for all the counts
       s = upload_and_count(bed, bed_len, n_fam, m_tot, d_bed, jobs, lists);
       tm.mark("upload+counts");
       if (s.ok())

@@ -869,6 +869,45 @@ static int32_t create_from_bed_impl(const uint8_t* bed, bool on_device, size_t b
   return SAIGE_OK;
 }
 
+namespace saige {
+
+Status grm_stream_rows_finish(saige_grm* h, const std::vector<int64_t>& pass, const double* af,
+                              const double* mac, uint64_t seed, std::vector<int64_t>& vidx) {
+  if (pass.empty())
+    return fail(SAIGE_EINVAL, "no marker passes QC (gen_range(0..0) in the reference)");
+  std::vector<uint8_t> flags;
+  vr_candidate_flags(pass, mac, seed, flags);
+  const int64_t rows = (int64_t)pass.size();
+  h->m = rows;
+  h->m_pad = round_up(rows, kMarkerPad);
+  // padding rows: all codes 11, 2p = 1/s = 0
+  SG_CUDA(cudaMemsetAsync(h->geno + (size_t)rows * h->wpr, 0xFF,
+                          (size_t)(h->m_pad - rows) * h->wpr * 4, h->stream));
+  std::vector<double> row_af((size_t)rows);
+  for (int64_t r = 0; r < rows; ++r) row_af[(size_t)r] = af[(size_t)pass[(size_t)r]];
+  std::vector<float4> zl;
+  std::vector<double> tp, is;
+  marker_meta(row_af.data(), rows, h->m_pad, zl, tp, is);
+  vidx.clear();
+  for (int64_t r = 0; r < rows; ++r) {
+    if (!flags[(size_t)r]) continue;
+    vidx.push_back(pass[(size_t)r]);
+    zl[(size_t)r] = make_float4(0.f, 0.f, 0.f, 0.f);
+    tp[(size_t)r] = 0.0;
+    is[(size_t)r] = 0.0;
+  }
+  SG_CUDA(cudaMemcpyAsync(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice,
+                          h->stream));
+  SG_CUDA(cudaMemcpyAsync(h->two_p, tp.data(), tp.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  SG_CUDA(cudaMemcpyAsync(h->inv_s, is.data(), is.size() * 8, cudaMemcpyHostToDevice, h->stream));
+  h->m_eff = rows - (int64_t)vidx.size();
+  h->n_splits = fp32_z_splits(h->n_pad, h->m_pad);
+  SG_CUDA(cudaStreamSynchronize(h->stream));  // the host vectors go out of scope
+  return Status();
+}
+
+}  // namespace saige
+
 // The fit-null GRM built while the .bed streams in from pinned host memory.  The
 // upload runs in marker chunks on a copy stream; as each chunk lands, the handle's
 // stream counts its alleles and missing calls (K1), the host applies the marker QC
@@ -1044,37 +1083,9 @@ Status stream_fit_null_grm(const uint8_t* bed, size_t bed_len, int64_t n_fam, in
       mt_done = mt_full;
     }
     tm.mark(" stream chunks");
-    if (pass.empty())
-      return fail(SAIGE_EINVAL, "no marker passes QC (gen_range(0..0) in the reference)");
-    std::vector<uint8_t> flags;
-    vr_candidate_flags(pass, mac.data(), seed, flags);
-    const int64_t rows = (int64_t)pass.size();
-    h->m = rows;
-    h->m_pad = round_up(rows, kMarkerPad);
-    // padding rows: all codes 11, 2p = 1/s = 0
-    SG_CUDA(cudaMemsetAsync(h->geno + (size_t)rows * h->wpr, 0xFF,
-                            (size_t)(h->m_pad - rows) * h->wpr * 4, h->stream));
+    SG_TRY(grm_stream_rows_finish(h, pass, af.data(), mac.data(), seed, vidx));
     SG_TRY(tc_stream_tiles(h, mt_done, h->m_pad / kMarkerPad, h->stream));
-    std::vector<double> row_af((size_t)rows);
-    for (int64_t r = 0; r < rows; ++r) row_af[(size_t)r] = af[(size_t)pass[(size_t)r]];
-    std::vector<float4> zl;
-    std::vector<double> tp, is;
-    marker_meta(row_af.data(), rows, h->m_pad, zl, tp, is);
-    vidx.clear();
-    for (int64_t r = 0; r < rows; ++r) {
-      if (!flags[(size_t)r]) continue;
-      vidx.push_back(pass[(size_t)r]);
-      zl[(size_t)r] = make_float4(0.f, 0.f, 0.f, 0.f);
-      tp[(size_t)r] = 0.0;
-      is[(size_t)r] = 0.0;
-    }
-    SG_CUDA(cudaMemcpyAsync(h->zlut, zl.data(), zl.size() * sizeof(float4), cudaMemcpyHostToDevice,
-                            h->stream));
-    SG_CUDA(cudaMemcpyAsync(h->two_p, tp.data(), tp.size() * 8, cudaMemcpyHostToDevice, h->stream));
-    SG_CUDA(cudaMemcpyAsync(h->inv_s, is.data(), is.size() * 8, cudaMemcpyHostToDevice, h->stream));
-    h->m_eff = rows - (int64_t)vidx.size();
     m_grm = h->m_eff;
-    h->n_splits = fp32_z_splits(h->n_pad, h->m_pad);
     SG_CUDA(cudaStreamSynchronize(h->stream));
     SG_CUDA(cudaStreamSynchronize(ss.c));
     tm.mark(" stream tail");
@@ -1127,6 +1138,23 @@ Status grm_shell_finish(saige_grm* h, const double* af) {
 }
 
 void grm_shell_destroy(saige_grm* h) { grm_free(h); }
+
+Status grm_shell_create_cap(int dev, int64_t n, int64_t rows_cap, saige_grm** out) {
+  *out = nullptr;
+  saige_grm* h = new saige_grm();
+  h->device = dev;
+  Status s = grm_alloc(h, n, rows_cap);
+  if (!s.ok()) {
+    grm_free(h);
+    return s;
+  }
+  *out = h;
+  return Status();
+}
+
+bool marker_qc_pass(double af, int64_t n_valid, int64_t n, double min_maf, double max_missing) {
+  return qc_pass(af, n_valid, n, min_maf, max_missing);
+}
 
 }  // namespace saige
 

@@ -147,6 +147,18 @@ namespace saige {
 Status grm_shell_create(int dev, int64_t n, int64_t m, const double* af, saige_grm** out);
 Status grm_shell_finish(saige_grm* h, const double* af);
 void grm_shell_destroy(saige_grm* h);
+// A handle with room for rows_cap marker rows and no metadata yet, for a streamed
+// build: the caller gathers the QC-passing markers into rows 0, 1, ... as the .bed
+// lands, then grm_stream_rows_finish(pass = their .bed indices, af and mac over all
+// markers) draws the variance-ratio candidates among them (kept in place with 2p = 1/s
+// = 0, so that integer products are those of a handle holding only the GRM markers),
+// codes the padding rows 11, uploads the metadata and sets m, m_pad, m_eff (the GRM's
+// M).  vidx receives the candidates' .bed indices.
+Status grm_shell_create_cap(int dev, int64_t n, int64_t rows_cap, saige_grm** out);
+Status grm_stream_rows_finish(saige_grm* h, const std::vector<int64_t>& pass, const double* af,
+                              const double* mac, uint64_t seed, std::vector<int64_t>& vidx);
+// fit_null.rs:209-222's marker QC over n samples (MAF and call rate).
+bool marker_qc_pass(double af, int64_t n_valid, int64_t n, double min_maf, double max_missing);
 
 // Kv for q columns of v (ld = h->n_pad, padding rows zero) into kp.
 // active (host, length q, may be NULL) selects columns; others are skipped.

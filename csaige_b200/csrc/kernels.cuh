@@ -26,20 +26,28 @@ cudaError_t launch_bed_count_cohorts(const uint8_t* bed, int64_t bytes_per_marke
                                      long long* counts, cudaStream_t st);
 
 // One cohort's output of launch_bed_gather_cohorts: raw marker j goes to row
-// row_of[j] of geno (wpr words per row; -1: not kept), its n samples at
-// sidx[sidx_off ..] (sidx_off a multiple of 16).
+// row_of[j * row_stride] of geno (wpr words per row; -1: not kept), its n samples at
+// sidx[sidx_off ..] (sidx_off a multiple of 16).  row_of may be host-mapped memory.
 struct CohortRows {
   uint32_t* geno;
   const int32_t* row_of;
+  int64_t row_stride;
   int64_t wpr;
   int64_t n;
   int64_t sidx_off;
 };
-// Gathers raw rows j0 .. j0 + n_rows into every cohort that keeps them (co: device
-// array of n_cohorts entries).  Rows of more than 200 KB are refused.
+// Up to kCohortsPerLaunch cohorts, passed by value in the launch's parameters (no copy
+// to queue behind other transfers).
+constexpr int kCohortsPerLaunch = 32;
+struct CohortSet {
+  CohortRows c[kCohortsPerLaunch];
+  int n;
+};
+// Gathers raw rows j0 .. j0 + n_rows into every cohort of the set that keeps them.  Rows
+// of more than 200 KB are refused.
 cudaError_t launch_bed_gather_cohorts(const uint8_t* bed, int64_t bytes_per_marker, int64_t j0,
-                                      int64_t n_rows, const int32_t* sidx, const CohortRows* co,
-                                      int n_cohorts, cudaStream_t st);
+                                      int64_t n_rows, const int32_t* sidx, const CohortSet& set,
+                                      cudaStream_t st);
 
 // ---- synthetic cohort ------------------------------------------------------
 struct CohortDev;

@@ -221,7 +221,7 @@ constexpr int kGatherThreads = 1024;  // one block of four staged rows per SM: 3
 __global__ void __launch_bounds__(kGatherThreads)
     bed_gather_cohorts_kernel(const uint8_t* __restrict__ bed, int64_t bpm, int64_t j0,
                               int64_t n_rows, int rpb, const int32_t* __restrict__ sidx,
-                              const CohortRows* __restrict__ co, int n_cohorts) {
+                              const CohortSet set) {
   extern __shared__ __align__(16) uint8_t row_s[];
   const int64_t stride = (bpm + 31) / 16 * 16;  // round_up(bpm + 16, 16)
   const int64_t jb = j0 + (int64_t)blockIdx.x * rpb;
@@ -231,13 +231,13 @@ __global__ void __launch_bounds__(kGatherThreads)
 #pragma unroll
   for (int q = 0; q < kGatherRowsMax; ++q)
     src[q] = q < nr ? stage_row(bed + 3 + (jb + q) * bpm, bpm, row_s + q * stride) : nullptr;
-  for (int c = 0; c < n_cohorts; ++c) {
-    const CohortRows cr = co[c];
+  for (int c = 0; c < set.n; ++c) {
+    const CohortRows& cr = set.c[c];
     int32_t r[kGatherRowsMax];
     bool any = false;
 #pragma unroll
     for (int q = 0; q < kGatherRowsMax; ++q) {
-      r[q] = q < nr ? cr.row_of[jb + q] : -1;
+      r[q] = q < nr ? cr.row_of[(jb + q) * cr.row_stride] : -1;
       any |= r[q] >= 0;
     }
     if (!any) continue;
@@ -285,9 +285,10 @@ __global__ void __launch_bounds__(kGatherThreads)
 }  // namespace
 
 cudaError_t launch_bed_gather_cohorts(const uint8_t* bed, int64_t bpm, int64_t j0, int64_t n_rows,
-                                      const int32_t* sidx, const CohortRows* co, int n_cohorts,
+                                      const int32_t* sidx, const CohortSet& set,
                                       cudaStream_t st) {
-  if (n_rows <= 0) return cudaSuccess;
+  if (n_rows <= 0 || set.n <= 0) return cudaSuccess;
+  if (set.n > kCohortsPerLaunch) return cudaErrorInvalidValue;
   if (bpm > kSmemRowMax) return cudaErrorInvalidValue;
   // as many rows per block as 200 KB of shared memory hold (each index load then serves
   // all of them), at most kGatherRowsMax
@@ -300,7 +301,7 @@ cudaError_t launch_bed_gather_cohorts(const uint8_t* bed, int64_t bpm, int64_t j
     if (e != cudaSuccess) return e;
   }
   bed_gather_cohorts_kernel<<<(unsigned)ceil_div(n_rows, rpb), kGatherThreads, smem, st>>>(
-      bed, bpm, j0, n_rows, rpb, sidx, co, n_cohorts);
+      bed, bpm, j0, n_rows, rpb, sidx, set);
   count_launches(1);
   return cudaGetLastError();
 }
