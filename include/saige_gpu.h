@@ -561,12 +561,12 @@ int32_t saige_write_sparse_grm(const saige_sparse_grm* g, const char* const* sam
  * without the variance ratio (counts, QC and VR/GRM split over the cohort's samples,
  * GRM, AI-REML) — fit_null::run per cohort (fit_null.rs:199-287).  The .bed is
  * uploaded once.  With concurrent != 0 the .bed streams in by marker chunks while one
- * launch per chunk counts every cohort's alleles and missing calls (pinned host
- * memory lets the counts run under the transfer), one pass over the device .bed
- * writes every cohort's GRM rows, and each cohort's fit runs on its own host thread
- * and stream, so that small cohorts' launches overlap; the results are bit-identical
- * to the sequential ones (concurrent == 0).  Rows of more than 200 KB (over 800,000
- * samples) take the per-cohort steps on the threads instead.  out[c], alpha[c] (p, may be
+ * launch per chunk counts every cohort's alleles and missing calls and (MIXED fits)
+ * one more gathers the chunk's QC-passing markers into every cohort's GRM (pinned host
+ * memory lets both run under the transfer; FP32 fits gather in one pass after it), and
+ * the fits run on a pool of host threads, each cohort on its own stream; the results
+ * are bit-identical to the sequential ones (concurrent == 0).  Rows of more than
+ * 200 KB (over 800,000 samples) take the per-cohort steps on the threads instead.  out[c], alpha[c] (p, may be
  * NULL), m_grm[c] (may be NULL); wall_seconds (may be NULL) = the whole call. */
 int32_t saige_fit_null_cohorts(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
                                int32_t n_cohorts, const int64_t* const* sample_idx,
