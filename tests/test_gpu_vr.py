@@ -181,8 +181,9 @@ def test_pinned_upload_path_gives_the_same_fit(subset, trait):
     assert a.variance_ratio.variance_ratio == b.variance_ratio.variance_ratio
 
 
-@pytest.mark.parametrize("concurrent,tune", [(True, False), (False, False), (True, True)])
-def test_sub_cohort_fits_equal_their_own_fits(concurrent, tune, monkeypatch):
+@pytest.mark.parametrize("concurrent,tune,prec", [(True, False, "mixed"), (False, False, "mixed"),
+                                                  (True, True, "mixed"), (True, False, "fp32")])
+def test_sub_cohort_fits_equal_their_own_fits(concurrent, tune, prec, monkeypatch):
     # fit_null::run per sub-cohort of one .bed, concurrently on threads and streams; with
     # tune, the ring-shape autotuner runs on every launch size, so the concurrent fits'
     # products share its per-key candidate state (results are the same for every shape)
@@ -201,8 +202,11 @@ def test_sub_cohort_fits_equal_their_own_fits(concurrent, tune, monkeypatch):
     # launch per marker chunk: unsorted indices and a ragged last word included)
     idx = rng.permutation(n)
     cohorts.append((idx, y[idx], x[idx]))
-    cfg = cs.AiRemlConfig(max_iter=6, precision=cs.PREC_MIXED, solve=cs.SOLVE_BLOCK,
-                          warm_start=cs.WARM_RECYCLED)
+    # MIXED: the concurrent call builds every cohort's rows under the streamed upload
+    # (all QC-passing markers, the variance-ratio ones kept in place with zero metadata);
+    # FP32: one shared gather of the GRM markers after all counts
+    cfg = cs.AiRemlConfig(max_iter=6, solve=cs.SOLVE_BLOCK, warm_start=cs.WARM_RECYCLED,
+                          precision=cs.PREC_MIXED if prec == "mixed" else cs.PREC_FP32)
     res, wall = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg,
                                     concurrent=concurrent)
     assert wall > 0 and len(res) == 4
