@@ -6,13 +6,15 @@
 // Sequential: each cohort in turn, every step its own (as fit_null::run per cohort).
 // Concurrent: the .bed streams in by marker chunks, and one launch per chunk counts
 // every cohort's alleles and missing calls of the chunk's markers (each raw row staged
-// once for all cohorts), all under the PCIe-bound transfer; each cohort's markers are
-// selected on the host, and one more pass over the .bed writes the packed rows of every
-// cohort's GRM (again each raw row staged once); then each cohort's fit runs on its own
-// host thread and stream, so that the launches of small cohorts — whose sample-side
-// pass fills a fraction of the GPU and whose PCG steps are latency-bound — overlap with
-// those of the others.  Counts and rows are exact either way, so both orders give the
-// same fits.
+// once for all cohorts), all under the PCIe-bound transfer.  For MIXED fits the host
+// applies each cohort's marker QC to every chunk as its counts arrive and one more
+// launch per chunk gathers the passing markers into every cohort's GRM, also under the
+// transfer (stream_cohorts); FP32 fits select their markers once all counts are in and
+// gather in one pass after the upload (build_handles).  The fits then run on a pool of
+// host threads, each cohort on its own stream, so that the launches of small cohorts —
+// whose sample-side pass fills a fraction of the GPU and whose PCG steps are
+// latency-bound — overlap with those of the others.  Counts and rows are exact either
+// way, so both orders give the same fits.
 #include <stdint.h>
 #include <string.h>
 
