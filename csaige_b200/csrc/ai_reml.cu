@@ -127,6 +127,11 @@ Status solve(Fit& f, const double* b, double* x, const double* x0, int q, const 
   run.max_iter = f.cfg->pcg_max_iter;
   run.precision = f.cfg->precision;
   run.x = x;
+  // A warm-started column takes at least one step even when its start meets the
+  // tolerance (the reference, starting from zero, always refines against the current
+  // operator).  Measured at N = 200k, M = 150k, τ tolerance 1e-5: without the step the fit
+  // launched 8 products instead of 10, but took 10 AI-REML iterations instead of 5 and
+  // ended 3.4e-4 away in tau1.
   run.force_step = x0 != nullptr;
   if (keep) {
     run.keep_p = keep->p;
