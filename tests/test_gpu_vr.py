@@ -241,3 +241,27 @@ def test_concurrent_sub_cohort_fits_are_bit_identical_to_sequential():
             assert a.m_grm == b.m_grm
             assert np.array_equal(a.tau, b.tau)
             assert np.array_equal(a.alpha, b.alpha)
+
+
+@pytest.mark.parametrize("prec", ["mixed", "fp32"])
+def test_more_cohorts_than_one_gather_launch_holds(prec):
+    # 35 cohorts: the concurrent call gathers their rows in launches of at most 32 cohorts
+    # (the cohorts' outputs ride in the launch parameters), so two launches per chunk
+    n, m = 3000, 1500
+    spec = cs.CohortSpec(n=n, m=m, seed=53, missing_rate=0.01, prevalence=0.3, h2=0.3, n_covar=2)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    rng = np.random.default_rng(9)
+    cohorts = []
+    for size in rng.integers(400, 900, 35):
+        idx = np.sort(rng.choice(n, int(size), replace=False))
+        cohorts.append((idx, y[idx], x[idx]))
+    cfg = cs.AiRemlConfig(max_iter=3, solve=cs.SOLVE_BLOCK, warm_start=cs.WARM_RECYCLED,
+                          precision=cs.PREC_MIXED if prec == "mixed" else cs.PREC_FP32)
+    seq, _ = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg, concurrent=False)
+    con, _ = cs.fit_null_cohorts(bed, n, m, cohorts, cs.TraitType.Binary, cfg, concurrent=True)
+    assert len(con) == 35
+    for a, b in zip(seq, con):
+        assert a.m_grm == b.m_grm
+        assert np.array_equal(a.tau, b.tau)
+        assert np.array_equal(a.alpha, b.alpha)
