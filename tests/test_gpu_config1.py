@@ -121,3 +121,46 @@ def test_block_solve_of_the_fit_rhs_to_pcg_tolerance(cohort, precision):
         resid = np.linalg.norm(b - sig @ r.x) / max(np.linalg.norm(b), 1.0)
         assert r.converged, col
         assert resid <= RESID_REL, (col, resid)
+
+
+@pytest.fixture(scope="module")
+def cohort_quant():
+    """The same CPU-scale cohort with a quantitative trait (4 N(0,1) covariates,
+    h2 = 0.3, Gaussian noise): tau0 is estimated too, with the W^-1 AI solve
+    (ai_reml.rs:281-306)."""
+    spec = cs.CohortSpec(trait=cs.TraitType.Quantitative, n_covar=4, h2=0.3)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = O.marker_stats(bed, spec.n, spec.m)
+    g, _ = O.select_markers(af, mac, nv, spec.n)
+    k = O.grm_explicit(O.standardize(O.dosages(bed, spec.n, g), af[g], 0))
+    oracle = {tol: O.fit_ai_reml(y, x, O.QUANTITATIVE, O.K_EXPLICIT, k, max_iter=30, tol=tol)
+              for tol in (0.02, 1e-5)}
+    return dict(spec=spec, bed=bed, y=y, x=x, af=af, g=g, k=k, oracle=oracle)
+
+
+@pytest.mark.parametrize("tol", [0.02, 1e-5])
+@pytest.mark.parametrize("name", list(CONFIGS))
+def test_quantitative_fit_matches_fp64_oracle(cohort_quant, name, tol, capsys):
+    c = cohort_quant
+    o = c["oracle"][tol]
+    kw = CONFIGS[name]
+    grm = _grm(c, kw["precision"])
+    r = cs.fit_ai_reml(c["y"], c["x"], grm, cs.TraitType.Quantitative,
+                       cs.AiRemlConfig(max_iter=30, tol=tol, **kw))
+    tau_rel = np.abs(r.tau - o["tau"]) / np.abs(o["tau"])
+    a_rel = np.abs(r.alpha - o["alpha"]).max() / np.abs(o["alpha"]).max()
+    sol = cs.PcgSolver(1e-5, 500).solve(grm, r.working_weights, r.tau, c["y"])
+    sig = _sigma(c, r.tau, r.working_weights)
+    resid = np.linalg.norm(c["y"] - sig @ sol.x) / np.linalg.norm(c["y"])
+    with capsys.disabled():
+        print(f"\n[config 1 quantitative {name} tol {tol:g}] tau {r.tau} oracle {o['tau']} "
+              f"rel {tau_rel.max():.2e}; alpha rel {a_rel:.2e}; AI-REML iterations "
+              f"{r.iterations} (oracle {o['iterations']}); residual {resid:.2e}; "
+              f"launches {r.n_kv_launches}")
+    assert r.converged and o["converged"]
+    assert np.all(tau_rel <= TAU_REL), tau_rel
+    assert a_rel <= ALPHA_REL, a_rel
+    assert sol.converged and resid <= RESID_REL, resid
+    if kw["warm_start"] == cs.WARM_ZERO:
+        assert r.iterations == o["iterations"]
