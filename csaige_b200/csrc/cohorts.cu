@@ -109,7 +109,6 @@ struct SampleLists {
 // Uploads the .bed into d_bed in marker chunks on a copy stream while, chunk by chunk,
 // one launch counts every cohort's alleles and missing calls of the chunk's markers;
 // fills each job's marker statistics and leaves the sample lists on the device.
-
 Status upload_and_count(const uint8_t* bed, size_t bed_len, int64_t n_fam, int64_t m_tot,
                         DevBuf& d_bed, std::vector<CohortJob>& jobs, SampleLists& lists) {
   const int64_t bpm = (n_fam + 3) / 4;
@@ -207,6 +206,19 @@ std::mutex g_cmap_mu;
 void* g_cmap = nullptr;
 size_t g_cmap_bytes = 0;
 bool g_cmap_busy = false;
+
+}  // namespace
+
+void saige::release_cohort_mapped() {
+  std::lock_guard<std::mutex> lk(g_cmap_mu);
+  if (g_cmap && !g_cmap_busy) {
+    cudaFreeHost(g_cmap);
+    g_cmap = nullptr;
+    g_cmap_bytes = 0;
+  }
+}
+
+namespace {
 
 struct CohortMapped {
   void* p = nullptr;

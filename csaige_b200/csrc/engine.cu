@@ -96,6 +96,8 @@ size_t cache_flush(int dev) {
 
 void release_cached_blocks() {
   cache_flush(-1);
+  // the sub-cohort build's host-mapped block, unless a build is using it
+  release_cohort_mapped();
   // the streamed build's host-mapped block, unless a build is using it
   std::lock_guard<std::mutex> lk(g_mapped_mu);
   if (g_mapped && !g_mapped_busy) {

@@ -47,6 +47,8 @@ struct DevBuf {
 };
 
 void release_cached_blocks();
+// Frees the sub-cohort build's host-mapped block unless a call is using it (cohorts.cu).
+void release_cohort_mapped();
 
 // Makes device d current for the scope and gives the caller's device back at the
 // end, on every return path.  ok is false when d could not be made current.
