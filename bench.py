@@ -143,6 +143,13 @@ class ClockSampler:
             self.thread.start()
         except FileNotFoundError:
             self.proc = None
+            return self
+        # nvidia-smi takes a moment to print its first sample: wait for it (up to 5 s) and
+        # drop it, so that a short timed region is still sampled and only under load
+        t0 = time.monotonic()
+        while not self.lines and self.proc.poll() is None and time.monotonic() - t0 < 5.0:
+            time.sleep(0.02)
+        self.lines.clear()
         return self
 
     def _read(self):
