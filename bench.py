@@ -645,8 +645,13 @@ def run_ours(args, world, rank, local):
     if st["sc_launches"]:
         # one-column products (dp4a on the CUDA cores): both passes read the codes once
         sc_avg = st["sc_ms"] / st["sc_launches"] * 1e-3
+        listed = st["missing_listed"]
         roof["single_column"] = {
-            "kernels": "sr_pass_a_kernel + sr_pass_b_kernel (+ quantisation)",
+            "kernels": ("sr_pass_a_kernel + sr_pass_b_kernel (+ quantisation)"
+                        + (", summing over the missing-call lists" if st["sc_list_launches"]
+                           else "")),
+            "missing_lists": {"products": st["sc_list_launches"], "calls": listed,
+                              "index_bytes_per_pass": 4 * listed if listed > 0 else 0},
             "products_per_step": st["sc_launches"] / args.steps, "avg_ms": sc_avg * 1e3,
             "achieved_gbs": 2 * bytes_launch / sc_avg / 1e9,
             "frac": 2 * bytes_launch / sc_avg / 1e9 / hbm,

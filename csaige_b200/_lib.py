@@ -162,6 +162,8 @@ class GrmStatsC(C.Structure):
         ("fp32_ms", C.c_double),
         ("sc_launches", C.c_int64),
         ("sc_ms", C.c_double),
+        ("sc_list_launches", C.c_int64),
+        ("missing_listed", C.c_int64),
     ]
 
 

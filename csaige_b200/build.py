@@ -35,6 +35,7 @@ SOURCES = [
     "warm.cu",
     "mlp.cu",
     "cohorts.cu",
+    "miss_lists.cu",
 ]
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -581,6 +581,7 @@ static Status fit_impl(saige_grm* h, const double* y, const double* x, int64_t n
     return fail(SAIGE_EINVAL, "unknown warm_start %d", cfg->warm_start);
   if (cfg->precond != SAIGE_PRECOND_UNIT && cfg->precond != SAIGE_PRECOND_DIAG_K)
     return fail(SAIGE_EINVAL, "unknown precond %d", cfg->precond);
+  h->n_fits += 1;
   PhaseTimer tm;
   tm.launches = &h->n_kv_launches;
   tm.l0 = h->n_kv_launches;

@@ -694,6 +694,7 @@ SG_API int32_t saige_grm_get_stats(const saige_grm* h, saige_grm_stats* out) {
   *out = h->stats;
   out->n_kv = h->n_kv;
   out->n_kv_launches = h->n_kv_launches;
+  out->missing_listed = tc_missing_listed(h);
   return SAIGE_OK;
 }
 

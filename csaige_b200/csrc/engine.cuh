@@ -136,6 +136,7 @@ struct saige_grm {
   saige::DevBuf excl;
   // statistics
   int64_t n_kv = 0, n_kv_launches = 0;
+  int64_t n_fits = 0;  // AI-REML fits started on the handle (the missing-call lists' trigger)
   bool profiling = false;
   saige_grm_stats stats{};
 };

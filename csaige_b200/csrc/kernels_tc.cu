@@ -51,6 +51,7 @@
 
 #include "kernels.cuh"
 #include "kernels_tc.cuh"
+#include "miss_lists.cuh"
 #include "tcgen05.cuh"
 
 namespace saige {
@@ -710,7 +711,9 @@ __global__ void __launch_bounds__(128)
 // These kernels form the same exact integer sums with dp4a — the limbs of q as
 // int8 planes, genotypes and missing flags expanded four at a time by byte
 // permutes — and apply the same FP64 epilogue, so their results are bit-identical
-// to the tensor-core path's.
+// to the tensor-core path's.  With the missing-call lists of the handle
+// (miss_lists.cuh) the flag sums give way to int64 sums over the ~1 % missing calls,
+// a third fewer instructions per entry for the same integers.
 // ---------------------------------------------------------------------------
 // prmt tables of the NEGATED genotype (codes 00, 01, 10, 11 -> -2, 0, -1, 0) and of
 // the missing flag (01 -> 1).  A selector nibble holds the code either in its bits
@@ -724,6 +727,20 @@ constexpr int kSrWarpMarkers = 8;                        // pass A: markers per 
 constexpr int kSrBlockMarkers = 8 * kSrWarpMarkers;      // pass A: markers per block
 constexpr int kSrWords = 1024;                           // pass A: sample words staged per round
 constexpr int kSrChunk = 2048;  // markers of limb planes staged per pass-B round
+// error word bit of a one-column product: a missing-call list entry out of range (the
+// entry is skipped; timeouts of the tensor-core pipeline set other bits)
+constexpr unsigned int kSrListErr = 1u << 30;
+// Missing-call entries of a pass-A segment staged at once in shared memory (a block's 64
+// markers x 16,384 samples: ~10,500 calls at 1 % missing); larger segments take several
+// pieces.  (Pass B reads its segments, ~5,200 calls per chunk, from global memory: staging
+// them cost it more resident blocks than the uncoalesced reads cost; 3.89 against 3.09 ms
+// per pass at 200,000 x 150,000.)
+constexpr int kPieceA = 12288;
+// dynamic shared memory of sr_pass_a_kernel: three planes of kSrWords 16-byte words, and
+// with the missing-call lists a piece of entries and one int64 counter per marker
+constexpr size_t sr_pass_a_smem(bool lists) {
+  return 3 * kSrWords * 16 + (lists ? kPieceA * 4 + kSrBlockMarkers * 8 : 0);
+}
 static_assert(kSamplePad % 256 == 0, "pass B of one column takes sample tiles in pairs");
 
 __device__ __forceinline__ uint32_t prmt(uint32_t x, uint32_t y, uint32_t sel) {
@@ -743,6 +760,70 @@ __device__ __forceinline__ void sr_expand(uint32_t w, int neg_g[4], int miss[4])
     neg_g[g] = (int)prmt(kNegGenoX, kNegGenoY, sel[g]);
     miss[g] = (int)prmt(kMissX, kMissY, sel[g]);
   }
+}
+
+// Asynchronous 4-byte copies global -> shared (cp.async), their commit, and the wait
+// for all of this thread's committed copies.
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_all;" ::: "memory");
+}
+
+// Entries [p0, p0 + n) of a list copied into buf (shared memory) by the block's nt
+// threads, asynchronously: complete after cp_async_wait_all and a barrier.
+__device__ __forceinline__ void stage_piece(uint32_t* buf, const uint32_t* __restrict__ ent,
+                                            int64_t p0, int n, int t, int nt) {
+  for (int i = t; i < n; i += nt) cp_async4(buf + i, ent + p0 + i);
+  cp_async_commit();
+}
+
+// One thread's share of a segment of missing-call entries (tag << bits | position),
+// ascending: the contiguous slice [e0 + t L, e0 + (t + 1) L) of [e0, e1) with L =
+// ceil((e1 - e0) / nt).  Consecutive entries mostly share a tag (a row or a sample), so
+// the thread sums value(position) per run of equal tags in int64 and adds each run to
+// counters[tag] with one shared-memory atomic.  An entry whose tag or position is out of
+// range (tag >= n_tags, position >= n_pos) sets kSrListErr in err and is skipped.
+template <class Value>
+__device__ __forceinline__ void add_slice(const uint32_t* ent, int64_t e0, int64_t e1,
+                                          int t, int nt, int bits, uint32_t n_tags, uint32_t n_pos,
+                                          unsigned long long* counters, unsigned int* err,
+                                          Value value) {
+  const int64_t len = (e1 - e0 + nt - 1) / nt;
+  const int64_t lo = e0 + (int64_t)t * len;
+  const int64_t hi = lo + len < e1 ? lo + len : e1;
+  const uint32_t pmask = (1u << bits) - 1u;
+  uint32_t tag = 0xFFFFFFFFu;
+  long long acc = 0;
+#pragma unroll 4
+  for (int64_t e = lo; e < hi; ++e) {
+    const uint32_t x = ent[e];
+    const uint32_t g = x >> bits, pos = x & pmask;
+    if (g >= n_tags || pos >= n_pos) {
+      atomicOr(err, kSrListErr);
+      continue;
+    }
+    if (g != tag) {
+      if (tag != 0xFFFFFFFFu) atomicAdd(&counters[tag], (unsigned long long)acc);
+      tag = g;
+      acc = 0;
+    }
+    acc += value(pos);
+  }
+  if (tag != 0xFFFFFFFFu) atomicAdd(&counters[tag], (unsigned long long)acc);
+}
+
+// The same groups as bytes of -g only (the missing sums come from the lists).
+__device__ __forceinline__ void sr_expand_g(uint32_t w, int neg_g[4]) {
+  const uint32_t hi = w >> 16;
+  const uint32_t sel[4] = {w & 0x3333u, w & 0xCCCCu, hi & 0x3333u, hi & 0xCCCCu};
+#pragma unroll
+  for (int g = 0; g < 4; ++g) neg_g[g] = (int)prmt(kNegGenoX, kNegGenoY, sel[g]);
 }
 
 // q = rint(x / scale) as in quant_v_kernel, into three int8 planes (l2, l1, l0) of
@@ -777,14 +858,15 @@ __global__ void __launch_bounds__(256)
 }
 
 // w = u inv_s, c = w 2p quantised as in quant_wc_kernel into planes (w: l2 l1 l0,
-// c: l2 l1 l0; length m_pad each), and sum qc.
+// c: l2 l1 l0; length m_pad each) and, when qc32 is given, qc as int32 (|qc| <= 127 *
+// 2^16); and sum qc.
 __global__ void __launch_bounds__(256)
     sr_quant_wc_kernel(const double* __restrict__ u, int64_t m_pad,
                        const double* __restrict__ inv_s, const double* __restrict__ two_p,
                        const unsigned long long* __restrict__ amax_w,
                        const unsigned long long* __restrict__ amax_c, double* __restrict__ scale_w,
                        double* __restrict__ scale_c, int8_t* __restrict__ planes,
-                       unsigned long long* __restrict__ sum_c) {
+                       int32_t* __restrict__ qc32, unsigned long long* __restrict__ sum_c) {
   __shared__ long long sh[8];
   const int64_t m = (int64_t)blockIdx.x * 256 + threadIdx.x;
   const double sw = scale_of(amax_w[0]), scc = scale_of(amax_c[0]);
@@ -803,6 +885,7 @@ __global__ void __launch_bounds__(256)
     planes[3 * m_pad + m] = (int8_t)l2;
     planes[4 * m_pad + m] = (int8_t)l1;
     planes[5 * m_pad + m] = (int8_t)l0;
+    if (qc32) qc32[m] = (int32_t)qc;
   }
   long long t = qc;
   for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
@@ -823,31 +906,56 @@ __global__ void __launch_bounds__(256)
 // limb planes of q are staged in shared memory kSrWords words (16 samples each) at a
 // time and shared by the block's warps; each lane keeps the six sums of its warp's 8
 // markers over its words, and the warp's sums are finished as in the tensor-core
-// epilogue.
+// epilogue.  With kLists the lanes keep the three genotype sums only: after each chunk
+// the block adds q (rebuilt from its staged limbs) over the missing calls of its markers
+// in the chunk — one segment of miss_ent, each entry (marker in block) << bits | (sample
+// in chunk) — into per-marker int64 counters: the same integer Mi the flag sums give.
+template <bool kLists>
 __global__ void __launch_bounds__(256, 2)
     sr_pass_a_kernel(const uint32_t* __restrict__ geno, int64_t wpr,
                      const int8_t* __restrict__ planes, int64_t n_pad,
                      const unsigned long long* __restrict__ sum_q,
                      const double* __restrict__ scale_v, const double* __restrict__ two_p,
-                     const double* __restrict__ inv_s, double* __restrict__ u) {
-  __shared__ uint4 sp[3][kSrWords];
+                     const double* __restrict__ inv_s, const uint32_t* __restrict__ miss_ent,
+                     const int64_t* __restrict__ miss_seg, int64_t nch, int bits,
+                     unsigned int* __restrict__ err, double* __restrict__ u) {
+  constexpr int kSums = kLists ? 3 : 6;
+  // dynamic shared memory (sr_pass_a_smem bytes): the three staged limb planes, then
+  // with kLists the per-marker missing sums and a piece of the chunk's entries
+  extern __shared__ uint4 sr_dyn[];
+  uint4(*sp)[kSrWords] = reinterpret_cast<uint4(*)[kSrWords]>(sr_dyn);
+  unsigned long long* mi_s = reinterpret_cast<unsigned long long*>(sr_dyn + 3 * kSrWords);
+  uint32_t* piece = reinterpret_cast<uint32_t*>(mi_s + kSrBlockMarkers);
+  if constexpr (kLists) {
+    if (threadIdx.x < kSrBlockMarkers) mi_s[threadIdx.x] = 0ull;
+  }
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t m0 = (int64_t)blockIdx.x * kSrBlockMarkers + warp * kSrWarpMarkers;
   const uint32_t* rows = geno + m0 * wpr;
-  int acc[kSrWarpMarkers][6];
+  int acc[kSrWarpMarkers][kSums];
 #pragma unroll
   for (int k = 0; k < kSrWarpMarkers; ++k)
 #pragma unroll
-    for (int j = 0; j < 6; ++j) acc[k][j] = 0;
+    for (int j = 0; j < kSums; ++j) acc[k][j] = 0;
   const int64_t n_words = n_pad / 16;
   for (int64_t c0 = 0; c0 < n_words; c0 += kSrWords) {
     const int cn = n_words - c0 < kSrWords ? (int)(n_words - c0) : kSrWords;
+    int64_t e0 = 0, e1 = 0;  // kLists: this chunk's segment
+    if constexpr (kLists) {
+      const int64_t* sg = miss_seg + (int64_t)blockIdx.x * nch + c0 / kSrWords;
+      e0 = sg[0];
+      e1 = sg[1];
+    }
     __syncthreads();
     for (int t = threadIdx.x; t < 3 * kSrWords; t += 256) {
       const int pl = t / kSrWords, k = t % kSrWords;
       sp[pl][k] = k < cn ? __ldg(reinterpret_cast<const uint4*>(planes + pl * n_pad) + c0 + k)
                          : make_uint4(0u, 0u, 0u, 0u);
     }
+    // kLists: the segment's first piece lands while the dense loop runs
+    if constexpr (kLists)
+      stage_piece(piece, miss_ent, e0, (int)(e1 - e0 < kPieceA ? e1 - e0 : kPieceA), threadIdx.x,
+                  256);
     __syncthreads();
 #pragma unroll 4
     for (int t = lane; t < cn; t += 32) {
@@ -860,34 +968,69 @@ __global__ void __launch_bounds__(256, 2)
       const int l0[4] = {(int)a0.x, (int)a0.y, (int)a0.z, (int)a0.w};
 #pragma unroll
       for (int k = 0; k < kSrWarpMarkers; ++k) {
-        int gbs[4], mbs[4];
-        sr_expand(w[k], gbs, mbs);
+        if constexpr (kLists) {
+          int gbs[4];
+          sr_expand_g(w[k], gbs);
 #pragma unroll
-        for (int g = 0; g < 4; ++g) {
-          const int gb = gbs[g], mb = mbs[g];
-          acc[k][0] = __dp4a(gb, l2[g], acc[k][0]);
-          acc[k][1] = __dp4a(gb, l1[g], acc[k][1]);
-          acc[k][2] = __dp4a(gb, l0[g], acc[k][2]);
-          acc[k][3] = __dp4a(mb, l2[g], acc[k][3]);
-          acc[k][4] = __dp4a(mb, l1[g], acc[k][4]);
-          acc[k][5] = __dp4a(mb, l0[g], acc[k][5]);
+          for (int g = 0; g < 4; ++g) {
+            acc[k][0] = __dp4a(gbs[g], l2[g], acc[k][0]);
+            acc[k][1] = __dp4a(gbs[g], l1[g], acc[k][1]);
+            acc[k][2] = __dp4a(gbs[g], l0[g], acc[k][2]);
+          }
+        } else {
+          int gbs[4], mbs[4];
+          sr_expand(w[k], gbs, mbs);
+#pragma unroll
+          for (int g = 0; g < 4; ++g) {
+            const int gb = gbs[g], mb = mbs[g];
+            acc[k][0] = __dp4a(gb, l2[g], acc[k][0]);
+            acc[k][1] = __dp4a(gb, l1[g], acc[k][1]);
+            acc[k][2] = __dp4a(gb, l0[g], acc[k][2]);
+            acc[k][3] = __dp4a(mb, l2[g], acc[k][3]);
+            acc[k][4] = __dp4a(mb, l1[g], acc[k][4]);
+            acc[k][5] = __dp4a(mb, l0[g], acc[k][5]);
+          }
         }
       }
     }
+    if constexpr (kLists) {
+      const int8_t* p2 = reinterpret_cast<const int8_t*>(sp[0]);
+      const int8_t* p1 = reinterpret_cast<const int8_t*>(sp[1]);
+      const int8_t* p0 = reinterpret_cast<const int8_t*>(sp[2]);
+      for (int64_t q0 = e0; q0 < e1; q0 += kPieceA) {  // uniform over the block
+        const int n = (int)(e1 - q0 < kPieceA ? e1 - q0 : kPieceA);
+        if (q0 != e0) {  // a later piece: after the last one's slices are done
+          __syncthreads();
+          stage_piece(piece, miss_ent, q0, n, threadIdx.x, 256);
+        }
+        cp_async_wait_all();
+        __syncthreads();
+        add_slice(piece, 0, n, threadIdx.x, 256, bits, kSrBlockMarkers, 16u * (uint32_t)cn, mi_s,
+                  err, [&](uint32_t s) {
+                    return 65536LL * p2[s] + 256LL * p1[s] + (long long)p0[s];
+                  });
+      }
+    }
   }
+  if constexpr (kLists) __syncthreads();
 #pragma unroll
   for (int k = 0; k < kSrWarpMarkers; ++k)
 #pragma unroll
-    for (int j = 0; j < 6; ++j)
+    for (int j = 0; j < kSums; ++j)
       for (int o = 16; o > 0; o >>= 1) acc[k][j] += __shfl_xor_sync(0xffffffffu, acc[k][j], o);
   const double S = (double)(long long)sum_q[0];
 #pragma unroll
   for (int k = 0; k < kSrWarpMarkers; ++k) {
     if (lane != k) continue;
     const int64_t m = m0 + k;
-    // the genotype sums were formed with -g
+    // the genotype sums were formed with -g; Mi is the same integer either way
     const double G = -(65536.0 * (double)acc[k][0] + 256.0 * (double)acc[k][1] + (double)acc[k][2]);
-    const double Mi = 65536.0 * (double)acc[k][3] + 256.0 * (double)acc[k][4] + (double)acc[k][5];
+    double Mi;
+    if constexpr (kLists)
+      Mi = (double)(long long)mi_s[warp * kSrWarpMarkers + k];
+    else
+      Mi = 65536.0 * (double)acc[k][kSums - 3] + 256.0 * (double)acc[k][kSums - 2] +
+           (double)acc[k][kSums - 1];
     const double tt = __dsub_rn(G, __dmul_rn(two_p[m], S - Mi));
     u[m] = __dmul_rn(inv_s[m], __dmul_rn(scale_v[0], tt));
   }
@@ -895,31 +1038,58 @@ __global__ void __launch_bounds__(256, 2)
 
 // Pass B of one column: block = two 128-sample tiles of tiles_s, thread = one sample of
 // each (the limb words it loads serve both).  The marker limb planes are staged in
-// shared memory kSrChunk markers at a time.
+// shared memory kSrChunk markers at a time.  With kLists the c planes give way to qc
+// itself (qc32), and after each chunk the block adds qc over the missing calls of its
+// 256 samples in the chunk — one segment of miss_ent, each entry (sample in block) <<
+// bits | (marker in chunk) — into per-sample int64 counters: the integer Mi the flag
+// sums give.
+template <bool kLists>
 __global__ void __launch_bounds__(128)
     sr_pass_b_kernel(const uint8_t* __restrict__ tiles_s, int64_t n_mt, int64_t s_ld,
                      const int8_t* __restrict__ planes, int64_t m_pad,
                      const unsigned long long* __restrict__ sum_c,
                      const double* __restrict__ scale_w, const double* __restrict__ scale_c,
-                     double out_scale, double* __restrict__ out) {
-  __shared__ __align__(16) int8_t sp[6][kSrChunk];
+                     const int32_t* __restrict__ qc32, const uint32_t* __restrict__ miss_ent,
+                     const int64_t* __restrict__ miss_seg, int64_t nch, int bits,
+                     unsigned int* __restrict__ err, double out_scale, double* __restrict__ out) {
+  constexpr int kPlanes = kLists ? 3 : 6;
+  __shared__ __align__(16) int8_t sp[kPlanes][kSrChunk];
+  __shared__ __align__(16) int32_t sq[kLists ? kSrChunk : 4];
   const int64_t st0 = 2 * (int64_t)blockIdx.x;
   const int r = threadIdx.x;
-  int acc[2][6];
+  int acc[2][kPlanes];
 #pragma unroll
   for (int h = 0; h < 2; ++h)
 #pragma unroll
-    for (int e = 0; e < 6; ++e) acc[h][e] = 0;
+    for (int e = 0; e < kPlanes; ++e) acc[h][e] = 0;
+  __shared__ unsigned long long mi_s[kLists ? 2 * kRows : 1];
+  if constexpr (kLists) {
+    mi_s[r] = 0ull;
+    mi_s[kRows + r] = 0ull;
+  }
   for (int64_t mt0 = 0; mt0 < n_mt; mt0 += kSrChunk / 128) {
     const int64_t base = mt0 * 128;
     const int64_t len = m_pad - base < kSrChunk ? m_pad - base : (int64_t)kSrChunk;
+    int64_t e0 = 0, e1 = 0;  // kLists: this chunk's segment
+    if constexpr (kLists) {
+      const int64_t* sg = miss_seg + (int64_t)blockIdx.x * nch + mt0 / (kSrChunk / 128);
+      e0 = sg[0];
+      e1 = sg[1];
+    }
     __syncthreads();
-    for (int t = threadIdx.x; t < 6 * (kSrChunk / 16); t += 128) {
+    for (int t = threadIdx.x; t < kPlanes * (kSrChunk / 16); t += 128) {
       const int pl = t / (kSrChunk / 16), k = t % (kSrChunk / 16);
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
       if (16 * k < len)
         v = __ldg(reinterpret_cast<const uint4*>(planes + (int64_t)pl * m_pad + base) + k);
       reinterpret_cast<uint4*>(sp[pl])[k] = v;
+    }
+    if constexpr (kLists) {
+      for (int t = threadIdx.x; t < kSrChunk / 4; t += 128) {
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (4 * t < len) v = __ldg(reinterpret_cast<const uint4*>(qc32 + base) + t);
+        reinterpret_cast<uint4*>(sq)[t] = v;
+      }
     }
     __syncthreads();
     const int64_t mt_end = mt0 + kSrChunk / 128 < n_mt ? mt0 + kSrChunk / 128 : n_mt;
@@ -941,39 +1111,63 @@ __global__ void __launch_bounds__(128)
         const uint4 w2 = *reinterpret_cast<const uint4*>(sp[0] + mk);
         const uint4 w1 = *reinterpret_cast<const uint4*>(sp[1] + mk);
         const uint4 w0 = *reinterpret_cast<const uint4*>(sp[2] + mk);
-        const uint4 c2 = *reinterpret_cast<const uint4*>(sp[3] + mk);
-        const uint4 c1 = *reinterpret_cast<const uint4*>(sp[4] + mk);
-        const uint4 c0 = *reinterpret_cast<const uint4*>(sp[5] + mk);
         const int W2[4] = {(int)w2.x, (int)w2.y, (int)w2.z, (int)w2.w};
         const int W1[4] = {(int)w1.x, (int)w1.y, (int)w1.z, (int)w1.w};
         const int W0[4] = {(int)w0.x, (int)w0.y, (int)w0.z, (int)w0.w};
-        const int C2[4] = {(int)c2.x, (int)c2.y, (int)c2.z, (int)c2.w};
-        const int C1[4] = {(int)c1.x, (int)c1.y, (int)c1.z, (int)c1.w};
-        const int C0[4] = {(int)c0.x, (int)c0.y, (int)c0.z, (int)c0.w};
+        if constexpr (kLists) {
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          int gbs[4], mbs[4];
-          sr_expand(words[h][j], gbs, mbs);
+          for (int h = 0; h < 2; ++h) {
+            int gbs[4];
+            sr_expand_g(words[h][j], gbs);
 #pragma unroll
-          for (int g = 0; g < 4; ++g) {
-            acc[h][0] = __dp4a(gbs[g], W2[g], acc[h][0]);
-            acc[h][1] = __dp4a(gbs[g], W1[g], acc[h][1]);
-            acc[h][2] = __dp4a(gbs[g], W0[g], acc[h][2]);
-            acc[h][3] = __dp4a(mbs[g], C2[g], acc[h][3]);
-            acc[h][4] = __dp4a(mbs[g], C1[g], acc[h][4]);
-            acc[h][5] = __dp4a(mbs[g], C0[g], acc[h][5]);
+            for (int g = 0; g < 4; ++g) {
+              acc[h][0] = __dp4a(gbs[g], W2[g], acc[h][0]);
+              acc[h][1] = __dp4a(gbs[g], W1[g], acc[h][1]);
+              acc[h][2] = __dp4a(gbs[g], W0[g], acc[h][2]);
+            }
+          }
+        } else {
+          const uint4 c2 = *reinterpret_cast<const uint4*>(sp[kPlanes - 3] + mk);
+          const uint4 c1 = *reinterpret_cast<const uint4*>(sp[kPlanes - 2] + mk);
+          const uint4 c0 = *reinterpret_cast<const uint4*>(sp[kPlanes - 1] + mk);
+          const int C2[4] = {(int)c2.x, (int)c2.y, (int)c2.z, (int)c2.w};
+          const int C1[4] = {(int)c1.x, (int)c1.y, (int)c1.z, (int)c1.w};
+          const int C0[4] = {(int)c0.x, (int)c0.y, (int)c0.z, (int)c0.w};
+#pragma unroll
+          for (int h = 0; h < 2; ++h) {
+            int gbs[4], mbs[4];
+            sr_expand(words[h][j], gbs, mbs);
+#pragma unroll
+            for (int g = 0; g < 4; ++g) {
+              acc[h][0] = __dp4a(gbs[g], W2[g], acc[h][0]);
+              acc[h][1] = __dp4a(gbs[g], W1[g], acc[h][1]);
+              acc[h][2] = __dp4a(gbs[g], W0[g], acc[h][2]);
+              acc[h][kPlanes - 3] = __dp4a(mbs[g], C2[g], acc[h][kPlanes - 3]);
+              acc[h][kPlanes - 2] = __dp4a(mbs[g], C1[g], acc[h][kPlanes - 2]);
+              acc[h][kPlanes - 1] = __dp4a(mbs[g], C0[g], acc[h][kPlanes - 1]);
+            }
           }
         }
       }
     }
+    if constexpr (kLists) {
+      add_slice(miss_ent, e0, e1, threadIdx.x, 128, bits, 2u * kRows, (uint32_t)len, mi_s, err,
+                [&](uint32_t mk) { return (long long)sq[mk]; });
+    }
   }
+  if constexpr (kLists) __syncthreads();
   const double S = (double)(long long)sum_c[0];
 #pragma unroll
   for (int h = 0; h < 2; ++h) {
-    // the genotype sums were formed with -g
+    // the genotype sums were formed with -g; Mi is the same integer either way
     const double G =
         -(65536.0 * (double)acc[h][0] + 256.0 * (double)acc[h][1] + (double)acc[h][2]);
-    const double Mi = 65536.0 * (double)acc[h][3] + 256.0 * (double)acc[h][4] + (double)acc[h][5];
+    double Mi;
+    if constexpr (kLists)
+      Mi = (double)(long long)mi_s[h * kRows + r];
+    else
+      Mi = 65536.0 * (double)acc[h][kPlanes - 3] + 256.0 * (double)acc[h][kPlanes - 2] +
+           (double)acc[h][kPlanes - 1];
     out[(st0 + h) * 128 + r] = __dmul_rn(
         out_scale, __dsub_rn(__dmul_rn(scale_w[0], G), __dmul_rn(scale_c[0], S - Mi)));
   }
@@ -1032,7 +1226,24 @@ struct TcPlan {
   DevBuf tiles_m, tiles_s, img_a, img_w, img_c, u, scal, cmap, trace;
   int64_t s_ld = 0;  // tiles_s: marker tiles per sample tile (>= m_pad / 128)
   bool tracing = false;
+  // one-column products: the missing-call lists and qc as int32 (m_pad) for pass B's
+  // sums over them
+  MissLists miss;
+  DevBuf sr_qc;
 };
+
+// The missing-call lists cost about two products' time to build (four passes over the
+// codes) and 8 bytes per missing call, while a fit runs four or five one-column products:
+// a handle builds them at the first one-column product of its second AI-REML fit, so a
+// single fit (with its variance ratio) keeps the dense flag sums and repeated fits on a
+// handle (refits, LOCO) take the lists.
+// SAIGE_SR_LISTS: 0 keeps the dense missing-flag sums, 2 builds the lists at a handle's
+// first one-column product, otherwise (default) in its second fit.
+static int sr_lists_mode() {
+  const char* e = getenv("SAIGE_SR_LISTS");
+  if (!e || !e[0]) return 1;
+  return e[0] == '0' ? 0 : (e[0] == '2' ? 2 : 1);
+}
 
 // Pipeline trace: with SAIGE_TC_TRACE=1 each tensor-core launch records, for
 // CTA 0 and its first stages, when loads were issued and landed, when the
@@ -1097,6 +1308,13 @@ static Status tc_plan_new(TcPlan** out) {
                     tc_grm_kernel<false, 2, true>, tc_grm_kernel<true, 2, true>}) {
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)kSmemBudget);
+    if (e != cudaSuccess)
+      return bail(fail(SAIGE_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e)));
+  }
+  for (bool lists : {false, true}) {
+    cudaError_t e = cudaFuncSetAttribute(
+        lists ? sr_pass_a_kernel<true> : sr_pass_a_kernel<false>,
+        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sr_pass_a_smem(lists));
     if (e != cudaSuccess)
       return bail(fail(SAIGE_ECUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(e)));
   }
@@ -1387,6 +1605,10 @@ static Status launch_tc_tuned(int dev, unsigned grid, TcArgs a, cudaStream_t st)
 
 int64_t tc_autotune_trials() { return g_tune_trials.load(); }
 
+int64_t tc_missing_listed(const saige_grm* h) {
+  return h->tc && h->tc->miss.state == 1 ? h->tc->miss.total : -1;
+}
+
 void tc_set_wait_budget(long long cycles) {
   g_tc_wait_cycles.store(cycles < 0 ? kWaitCycles : cycles, std::memory_order_relaxed);
 }
@@ -1438,6 +1660,17 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     int8_t* planes_a = p->img_a.as<int8_t>();  // 3 x n_pad limb planes of q
     int8_t* planes_b = p->img_w.as<int8_t>();  // 6 x m_pad limb planes of qw, qc
     double* u = p->u.as<double>();
+    const int lmode = sr_lists_mode();
+    if (p->miss.state == 0 && (lmode == 2 || (lmode == 1 && h->n_fits >= 2)))
+      SG_TRY(miss_lists_build(h, p->tiles_s.as<uint8_t>(), p->s_ld,
+                              MissShape{kSrBlockMarkers, kSrWords, 2 * kRows, kSrChunk}, &p->miss,
+                              st));
+    const bool lists = p->miss.state == 1 && lmode != 0;
+    int32_t* qc32 = nullptr;
+    if (lists) {
+      SG_TRY(p->sr_qc.reserve((size_t)h->m_pad * sizeof(int32_t)));
+      qc32 = p->sr_qc.as<int32_t>();
+    }
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     SG_TRY(mark(&t0));
     SG_CUDA(cudaMemsetAsync(p->scal.ptr, 0, 5 * kMaxR * 8, st));
@@ -1445,8 +1678,17 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     amax_v_kernel<<<g1a, 256, 0, st>>>(v, h->n_pad, h->n, p->cmap.as<int>(), sc.amax_v);
     sr_quant_v_kernel<<<(unsigned)ceil_div(h->n_pad, 256), 256, 0, st>>>(
         v + (int64_t)cols[0] * h->n_pad, h->n, h->n_pad, sc.amax_v, sc.scale_v, planes_a, sc.sum_v);
-    sr_pass_a_kernel<<<(unsigned)(h->m_pad / kSrBlockMarkers), 256, 0, st>>>(
-        h->geno, h->wpr, planes_a, h->n_pad, sc.sum_v, sc.scale_v, h->two_p, h->inv_s, u);
+    if (lists)
+      sr_pass_a_kernel<true><<<(unsigned)(h->m_pad / kSrBlockMarkers), 256, sr_pass_a_smem(true),
+                               st>>>(
+          h->geno, h->wpr, planes_a, h->n_pad, sc.sum_v, sc.scale_v, h->two_p, h->inv_s,
+          p->miss.a_ent.as<uint32_t>(), p->miss.a_seg.as<int64_t>(), p->miss.a_nch, p->miss.a_bits,
+          sc.err, u);
+    else
+      sr_pass_a_kernel<false><<<(unsigned)(h->m_pad / kSrBlockMarkers), 256, sr_pass_a_smem(false),
+                                st>>>(
+          h->geno, h->wpr, planes_a, h->n_pad, sc.sum_v, sc.scale_v, h->two_p, h->inv_s, nullptr,
+          nullptr, 0, 0, nullptr, u);
     SG_CHECK_LAUNCH();
     if (h->masked) SG_CUDA(mask_rows_f64(u, h->m_pad, 1, h->excl.as<uint8_t>(), h->m, st));
     const dim3 g1b((unsigned)std::min<int64_t>(ceil_div(h->m_pad, 256), 296), 1u);
@@ -1454,16 +1696,26 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
                                         sc.amax_c);
     sr_quant_wc_kernel<<<(unsigned)ceil_div(h->m_pad, 256), 256, 0, st>>>(
         u, h->m_pad, h->inv_s, h->two_p, sc.amax_w, sc.amax_c, sc.scale_w, sc.scale_c, planes_b,
-        sc.sum_c);
+        qc32, sc.sum_c);
     // two sample tiles per block (n_pad is a multiple of 512: an even tile count)
-    sr_pass_b_kernel<<<(unsigned)(h->n_pad / (2 * kRows)), kRows, 0, st>>>(
-        p->tiles_s.as<uint8_t>(), h->m_pad / kRows, p->s_ld, planes_b, h->m_pad, sc.sum_c, sc.scale_w,
-        sc.scale_c, 1.0 / (double)(h->masked ? h->m_active : h->m_eff), kp + (int64_t)cols[0] * h->n_pad);
+    const unsigned grid_b = (unsigned)(h->n_pad / (2 * kRows));
+    const double out_scale = 1.0 / (double)(h->masked ? h->m_active : h->m_eff);
+    double* out = kp + (int64_t)cols[0] * h->n_pad;
+    if (lists)
+      sr_pass_b_kernel<true><<<grid_b, kRows, 0, st>>>(
+          p->tiles_s.as<uint8_t>(), h->m_pad / kRows, p->s_ld, planes_b, h->m_pad, sc.sum_c,
+          sc.scale_w, sc.scale_c, qc32, p->miss.b_ent.as<uint32_t>(), p->miss.b_seg.as<int64_t>(),
+          p->miss.b_nch, p->miss.b_bits, sc.err, out_scale, out);
+    else
+      sr_pass_b_kernel<false><<<grid_b, kRows, 0, st>>>(
+          p->tiles_s.as<uint8_t>(), h->m_pad / kRows, p->s_ld, planes_b, h->m_pad, sc.sum_c,
+          sc.scale_w, sc.scale_c, nullptr, nullptr, nullptr, 0, 0, nullptr, out_scale, out);
     SG_CHECK_LAUNCH();
     count_launches(6);
     SG_TRY(mark(&t1));
     if (h->profiling) ev_s.emplace_back(t0, t1);
     h->stats.sc_launches += 1;
+    h->stats.sc_list_launches += lists ? 1 : 0;
     h->n_kv += 1;
   }
   for (size_t c0 = 0; c0 < (single ? 0 : cols.size()); c0 += kMaxR) {
@@ -1576,6 +1828,8 @@ Status tc_product(saige_grm* h, const double* v, double* kp, int q, const int32_
     h->stats.sc_ms += ms;
   }
   for (cudaEvent_t e : ev) cudaEventDestroy(e);
+  if (err & kSrListErr)
+    return fail(SAIGE_ECUDA, "one-column GRM product: a missing-call list entry out of range");
   if (err) return fail(SAIGE_TIMEOUT, "tensor-core GRM product: a pipeline wait timed out");
   return Status();
 }

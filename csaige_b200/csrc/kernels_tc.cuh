@@ -19,6 +19,8 @@ void tc_destroy(saige_grm* h);
 // tiles of marker tiles [mt0, mt1) from h->geno as those rows are complete.
 Status tc_stream_begin(saige_grm* h, int64_t rows_cap);
 Status tc_stream_tiles(saige_grm* h, int64_t mt0, int64_t mt1, cudaStream_t st);
+// Missing calls in the handle's lists for one-column products (-1: none built, or declined).
+int64_t tc_missing_listed(const saige_grm* h);
 // Trial launches the ring-shape autotuner has timed in this process.
 int64_t tc_autotune_trials();
 // Budget of every pipeline wait of the tensor-core product, in SM cycles (< 0: the

@@ -441,6 +441,16 @@ typedef struct {
   double fp32_ms;
   int64_t sc_launches;        /* MIXED single-column products on the CUDA    */
   double sc_ms;               /* cores (both passes; dp4a, same sums)        */
+  int64_t sc_list_launches;   /* of those, with the missing-call lists: sums */
+                              /* over the missing calls in place of dense    */
+                              /* flag sums, the same integers; built at the  */
+                              /* first such product of the handle's second   */
+                              /* fit (env SAIGE_SR_LISTS=2: its first        */
+                              /* product, =0: never)                         */
+  int64_t missing_listed;     /* missing calls in the handle's lists; -1     */
+                              /* while none are built or when declined       */
+                              /* (over 3 % of the calls missing, or too      */
+                              /* little free device memory)                  */
 } saige_grm_stats;
 
 /* Turn per-kernel CUDA-event timing on (1) or off (0) for a handle. */

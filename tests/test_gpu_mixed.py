@@ -142,22 +142,57 @@ def test_autotuned_ring_shapes_give_identical_products(monkeypatch):
     assert int(cs.api.LIB.saige_tc_autotune_trials()) > before
 
 
-@pytest.mark.parametrize("n,m,sub", [(1001, 300, False), (17000, 4300, False), (4500, 700, True)])
-def test_single_column_cuda_core_path_equals_tensor_core_path(monkeypatch, n, m, sub):
+@pytest.mark.parametrize("lists", ["2", "0"])
+@pytest.mark.parametrize("n,m,sub,miss", [(1001, 300, False, 0.02), (17000, 4300, False, 0.02),
+                                          (4500, 700, True, 0.02), (3000, 900, False, 0.0),
+                                          (3000, 900, False, 0.06)])
+def test_single_column_cuda_core_path_equals_tensor_core_path(monkeypatch, n, m, sub, miss, lists):
     # one active column runs both passes with dp4a on the CUDA cores: the same exact
     # integer sums and the same FP64 epilogue, so every bit agrees with the tensor-core
     # passes (SAIGE_SC=0) and with the CPU model; the sizes cross the staging chunks
-    # (1024 sample words in pass A, 2048 markers in pass B)
+    # (1024 sample words in pass A, 2048 markers in pass B, 8192 values of the lists' sums).
+    # With the lists (SAIGE_SR_LISTS=2: built at the handle's first one-column product)
+    # the sums over missing calls come from the per-block segments of missing calls; over
+    # 3 % missing the lists are declined and the dense flag sums stay, as they do with
+    # SAIGE_SR_LISTS=0.
+    monkeypatch.setenv("SAIGE_SR_LISTS", lists)
     rng = np.random.default_rng(n + m)
     sidx = rng.permutation(n)[: n - 37] if sub else None
-    grm, bed, keep, afs = _case(n, m, sidx=sidx, miss=0.02)
+    grm, bed, keep, afs = _case(n, m, sidx=sidx, miss=miss)
+    codes = MM.codes(bed, n, keep, sidx)
     v = rng.standard_normal((1, grm.n_samples))
-    before = grm.stats()["sc_launches"]
+    before = grm.stats()
     got = grm.mat_vec(v)
-    assert grm.stats()["sc_launches"] == before + 1
+    st = grm.stats()
+    assert st["sc_launches"] == before["sc_launches"] + 1
+    listed = lists == "2" and miss <= 0.02
+    assert st["sc_list_launches"] == before["sc_list_launches"] + int(listed)
+    assert st["missing_listed"] == (int((codes == 1).sum()) if listed else -1)
     monkeypatch.setenv("SAIGE_SC", "0")
     tc = grm.mat_vec(v)
-    assert grm.stats()["sc_launches"] == before + 1
+    assert grm.stats()["sc_launches"] == before["sc_launches"] + 1
     assert np.array_equal(got, tc)
-    want = MM.kv(MM.codes(bed, n, keep, sidx), afs, v.T).T
+    want = MM.kv(codes, afs, v.T).T
     assert np.array_equal(got, want)
+
+
+def test_missing_lists_built_in_a_handles_second_fit(monkeypatch):
+    # by default a handle's first AI-REML fit keeps the dense flag sums and its second fit
+    # builds the missing-call lists at its first one-column product: the products are the
+    # same integers, so the two fits agree to the bit
+    monkeypatch.delenv("SAIGE_SR_LISTS", raising=False)
+    spec = cs.CohortSpec(n=3000, m=1500, seed=31)
+    bed = cs.gen_bed(spec)
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = cs.bed_marker_stats(bed, spec.n, spec.m)
+    g, _ = cs.select_grm_markers(af, mac, nv, spec.n)
+    grm = cs.OnTheFlyGrm.from_bed(bed, spec.n, spec.m, g, af[g], precision=MIXED)
+    cfg = cs.AiRemlConfig(max_iter=30, tol=1e-5, precision=MIXED, solve=cs.SOLVE_BLOCK,
+                          warm_start=cs.WARM_RECYCLED)
+    r1 = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg)
+    st = grm.stats()
+    assert st["sc_launches"] > 0 and st["missing_listed"] == -1 and st["sc_list_launches"] == 0
+    r2 = cs.fit_ai_reml(y, x, grm, cs.TraitType.Binary, cfg)
+    st = grm.stats()
+    assert st["missing_listed"] > 0 and st["sc_list_launches"] > 0
+    assert np.array_equal(r1.tau, r2.tau) and np.array_equal(r1.alpha, r2.alpha)
