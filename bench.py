@@ -182,6 +182,36 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def single_column_modes(grm, n: int, reps: int = 4) -> dict:
+    """Device ms per one-column product on the bench's handle (after its timed fits) with
+    the dense missing-flag sums (SAIGE_SR_LISTS=0) and with the missing-call lists the
+    handle built in its second warm-up fit: the same products to the bit."""
+    import numpy as np
+
+    v = np.random.default_rng(3).standard_normal((1, n))
+    prev = os.environ.get("SAIGE_SR_LISTS")
+    out = {}
+    grm.set_profiling(True)
+    try:
+        for mode, key in (("0", "flags"), ("1", "lists")):
+            os.environ["SAIGE_SR_LISTS"] = mode
+            grm.mat_vec(v)
+            grm.reset_stats()
+            for _ in range(reps):
+                grm.mat_vec(v)
+            s = grm.stats()
+            out[key + "_ms"] = s["sc_ms"] / max(s["sc_launches"], 1)
+            out[key + "_list_products"] = s["sc_list_launches"]
+    finally:
+        if prev is None:
+            os.environ.pop("SAIGE_SR_LISTS", None)
+        else:
+            os.environ["SAIGE_SR_LISTS"] = prev
+        grm.set_profiling(False)
+    out["products"] = reps
+    return out
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -656,6 +686,8 @@ def run_ours(args, world, rank, local):
             "achieved_gbs": 2 * bytes_launch / sc_avg / 1e9,
             "frac": 2 * bytes_launch / sc_avg / 1e9 / hbm,
             "share_of_step": st["sc_ms"] / 1e3 / (step_s * args.steps)}
+        if world == 1:
+            roof["single_column"]["flags_vs_lists"] = single_column_modes(grm, args.n)
 
     line = {
         "metric": METRIC, "value": whole_job_seconds_per_fit(step_s, world), "unit": "s",
