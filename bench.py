@@ -99,6 +99,8 @@ def parse_args():
                     help="skip the zero / recycled / learned start comparison (N=400k, M=100k)")
     ap.add_argument("--no-config1", action="store_true",
                     help="skip the plain CPU-scale cohort (GPU fits, oracle, measured CPU fit)")
+    ap.add_argument("--no-plain-scale", action="store_true",
+                    help="skip the plain method at GPU scale (N=50k, M=100k, quantitative)")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the product and solve errors against the FP64 oracle")
     ap.add_argument("--no-explicit-grm", action="store_true",
@@ -481,6 +483,63 @@ def accuracy_block(cs) -> dict:
     return out
 
 
+def plain_scale_block(cs) -> dict:
+    """The plain method at GPU scale (N = 50,000, M = 100,000, a quantitative trait with
+    h2 = 0.3, 4 N(0,1) covariates, Gaussian noise, 30 probes, tolerance 1e-5): the
+    reference's strategy (FP32 products, one PCG per right-hand side, zero starts) and
+    the fast configuration on the same cohort, each with seconds, iterations, tau, and
+    the true residual of Sigma^-1 y with the oracle's FP64 products at its own tau and W;
+    plus the FP32 product's error against the FP64 product."""
+    sys.path.insert(0, str(ROOT / "tests"))
+    import numpy as np
+    import torch
+
+    import oracle_ffi as O
+
+    n, m = ACCURACY["n"], ACCURACY["m"]
+    spec = cs.CohortSpec(n=n, m=m, seed=WORKLOAD["seed"] + 1, sib_frac=WORKLOAD["sib_frac"],
+                         cousin_frac=WORKLOAD["cousin_frac"], missing_rate=WORKLOAD["missing_rate"],
+                         trait=cs.TraitType.Quantitative, n_covar=4, h2=0.3)
+    bed_dev = torch.empty(spec.bed_len, dtype=torch.uint8, device="cuda")
+    cs.gen_bed_dev(spec, bed_dev.data_ptr())
+    bed = bed_dev.cpu().numpy()
+    y, x = cs.gen_pheno(spec)
+    af, mac, nv = cs.api.bed_marker_stats_dev(bed_dev.data_ptr(), spec.bed_len, n, m)
+    g, _ = cs.select_grm_markers(af, mac, nv, n)
+    out = {"workload": f"quantitative h2 0.3, N={n}, M={m} bed markers ({len(g)} in the GRM), "
+                       f"4 covariates, 30 probes, tol 1e-5"}
+    fits = {}
+    for name, prec, solve, warm in (("plain", cs.PREC_FP32, cs.SOLVE_SINGLE, cs.WARM_ZERO),
+                                    ("fast", cs.PREC_MIXED, cs.SOLVE_BLOCK, cs.WARM_RECYCLED)):
+        grm = cs.OnTheFlyGrm.from_bed_dev(bed_dev.data_ptr(), spec.bed_len, n, m, g, af[g],
+                                          precision=prec)
+        if name == "plain":
+            v = np.random.default_rng(7).standard_normal(n)
+            want = O.grm_matmul_f64_packed(bed, n, g, af[g], v[None, :])[0]
+            got = grm.mat_vec(v, precision=cs.PREC_FP32)
+            out["kv_fp32_max_rel"] = float(np.abs(got - want).max() / np.abs(want).max())
+        cfg = cs.AiRemlConfig(precision=prec, solve=solve, warm_start=warm, tol=CLI_TOL,
+                              max_iter=30)
+        r = cs.fit_ai_reml(y, x, grm, cs.TraitType.Quantitative, cfg)
+        fits[name] = r
+        sol = cs.PcgSolver(1e-5, 500).solve(grm, r.working_weights, r.tau, y, precision=prec)
+        kx = O.grm_matmul_f64_packed(bed, n, g, af[g], sol.x[None, :])[0]
+        sig_x = r.tau[0] * sol.x / np.maximum(r.working_weights, 1e-30) + r.tau[1] * kx
+        out[f"{name}_fit"] = {
+            "seconds": r.seconds, "ai_reml_iterations": int(r.iterations),
+            "n_kv": int(r.n_kv), "n_kv_launches": int(r.n_kv_launches),
+            "pcg_iters": int(r.pcg_iters), "tau": [float(r.tau[0]), float(r.tau[1])],
+            "sigma_inv_y_true_residual": float(np.linalg.norm(y - sig_x) / np.linalg.norm(y))}
+        grm.close()
+    del bed_dev
+    torch.cuda.empty_cache()
+    out["tau_rel_diff_fast_vs_plain"] = float(max(
+        abs(fits["fast"].tau[k] - fits["plain"].tau[k]) / abs(fits["plain"].tau[k])
+        for k in (0, 1)))
+    out["speedup_fast_vs_plain"] = fits["plain"].seconds / fits["fast"].seconds
+    return out
+
+
 def starts_block(cs) -> dict:
     """The learned-start cohort (N = 400,000, M = 100,000, binary at 1 %, 10
     covariates): twelve AI-REML iterations of the fast configuration (MIXED, block PCG
@@ -853,6 +912,11 @@ def run_ours(args, world, rank, local):
     if rank == 0 and world == 1 and not args.no_accuracy:
         del grm
         line["accuracy"] = accuracy_block(cs)
+    if rank == 0 and world == 1 and not args.no_plain_scale:
+        try:
+            line["plain_gpu_scale"] = plain_scale_block(cs)
+        except Exception as e:  # a side block: its failure must not cost the bench line
+            line["plain_gpu_scale"] = {"error": repr(e)[:300]}
     if rank == 0 and world == 1 and not args.no_learned:
         line["config5_starts"] = starts_block(cs)
     if rank == 0 and world == 1 and not args.no_explicit_grm:
